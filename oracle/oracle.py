@@ -1,0 +1,175 @@
+"""ctypes front end of the CPU restatement in af_oracle.cpp.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline / reference legs, never by the product package.
+
+``OracleOperator`` mirrors the reference's ``EULEROperator`` surface
+(euler_operator.h:24-67): set_dt / set_Mach / set_Froude / set_HYPERBOLIC_stage /
+set_NS_stage / set_rho_for_fixed / set_pres_fixed / set_u_fixed / vmult_rhs_rho_update /
+vmult_rhs_pressure / vmult_rhs_velocity_fixed / vmult / vmult_pressure / vmult_enthalpy /
+compute_diagonal, with numpy vectors in the deal.II DoF layout.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libaf_oracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp,
+                                 ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_int]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_set_params.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_set_stages.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_set_fixed.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+        L.orc_rhs.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, ctypes.POINTER(dp), ctypes.c_int]
+        L.orc_vmult.restype = ctypes.c_int
+        L.orc_vmult.argtypes = [ctypes.c_void_p, dp, dp]
+        L.orc_vmult_pressure.argtypes = [ctypes.c_void_p, dp, dp]
+        L.orc_vmult_enthalpy.argtypes = [ctypes.c_void_p, dp, dp]
+        L.orc_inverse_diagonal.argtypes = [ctypes.c_void_p, dp]
+        L.orc_tables.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp]
+        L.orc_set_num_threads.argtypes = [ctypes.c_int]
+        L.orc_get_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def set_num_threads(n: int):
+    lib().orc_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return lib().orc_get_num_threads()
+
+
+def tables(P, NQ):
+    nodes = np.zeros(P + 1); qp = np.zeros(NQ); qw = np.zeros(NQ)
+    S = np.zeros(NQ * (P + 1)); D = np.zeros(NQ * (P + 1))
+    lib().orc_tables(P, NQ, _p(nodes), _p(qp), _p(qw), _p(S), _p(D))
+    return nodes, qp, qw, S.reshape(NQ, P + 1), D.reshape(NQ, P + 1)
+
+
+class OracleOperator:
+    """CPU EULEROperator restatement; all vectors are float64 numpy arrays."""
+
+    def __init__(self, mesh, degree, Ma, Fr, dt, n_q_1d=None, long_double=False):
+        self.mesh = mesh
+        self.P = degree
+        self.NQ = n_q_1d if n_q_1d is not None else 2 * degree + 1
+        self._vtx = _c(mesh.vertices)
+        self.Ma, self.Fr, self.dt = Ma, Fr, dt
+        self._h = lib().orc_create(self.P, self.NQ, mesh.nx, mesh.nz, int(mesh.periodic_x), _p(self._vtx),
+                                   int(mesh.gravity), float(mesh.radial_a), Ma, Fr, dt, int(long_double))
+        self.hyperbolic_stage = 1
+        self.ns_stage = 1
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    @property
+    def n_scalar(self):
+        return self.mesh.n_cells * (self.P + 1) ** 2
+
+    # --- setters (euler_operator.h:243-339) ---
+    def _push(self):
+        lib().orc_set_params(self._h, self.Ma, self.Fr, self.dt)
+        lib().orc_set_stages(self._h, self.hyperbolic_stage, self.ns_stage)
+
+    def set_dt(self, dt):
+        self.dt = dt; self._push()
+
+    def set_Mach(self, Ma):
+        self.Ma = Ma; self._push()
+
+    def set_Froude(self, Fr):
+        self.Fr = Fr; self._push()
+
+    def set_HYPERBOLIC_stage(self, s):
+        assert 1 <= s <= 3
+        self.hyperbolic_stage = s; self._push()
+
+    def set_NS_stage(self, s):
+        assert 1 <= s <= 6
+        self.ns_stage = s; self._push()
+
+    def set_rho_for_fixed(self, v):
+        lib().orc_set_fixed(self._h, 0, _p(_c(v)))
+
+    def set_pres_fixed(self, v):
+        lib().orc_set_fixed(self._h, 1, _p(_c(v)))
+
+    def set_u_fixed(self, v):
+        lib().orc_set_fixed(self._h, 2, _p(_c(v)))
+
+    # --- explicit right-hand sides ---
+    def _rhs(self, kind, src):
+        src = [_c(s) for s in src]
+        arr = (ctypes.POINTER(ctypes.c_double) * len(src))(*[_p(s) for s in src])
+        n = self.n_scalar * (2 if kind == 2 else 1)
+        dst = np.zeros(n)
+        lib().orc_rhs(self._h, kind, _p(dst), arr, len(src))
+        return dst
+
+    def vmult_rhs_rho_update(self, src):
+        return self._rhs(0, src)
+
+    def vmult_rhs_pressure(self, src):
+        return self._rhs(1, src)
+
+    def vmult_rhs_velocity_fixed(self, src):
+        return self._rhs(2, src)
+
+    # --- implicit operators ---
+    def vmult(self, src):
+        ns = self.ns_stage
+        n = self.n_scalar * (2 if ns in (3, 5) else 1)
+        dst = np.zeros(n)
+        self.last_inner_iterations = lib().orc_vmult(self._h, _p(dst), _p(_c(src)))
+        return dst
+
+    def vmult_pressure(self, src):
+        dst = np.zeros(2 * self.n_scalar)
+        lib().orc_vmult_pressure(self._h, _p(dst), _p(_c(src)))
+        return dst
+
+    def vmult_enthalpy(self, src):
+        dst = np.zeros(self.n_scalar)
+        lib().orc_vmult_enthalpy(self._h, _p(dst), _p(_c(src)))
+        return dst
+
+    def inverse_diagonal(self):
+        ns = self.ns_stage
+        n = self.n_scalar * (2 if ns in (3, 5) else 1)
+        dst = np.zeros(n)
+        lib().orc_inverse_diagonal(self._h, _p(dst))
+        return dst
