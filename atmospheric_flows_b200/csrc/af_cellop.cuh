@@ -1,0 +1,545 @@
+// af_cellop.cuh -- generic cell-centric, sum-factorised DG operator kernel for sm_100a.
+//
+// One CTA owns CB consecutive cells (deal.II active-cell order = DoF order) and NQ
+// threads per cell ("members").  Every operator of the reference's EULEROperator is a
+// sum over "groups" of input fields of (cell integral) + (face integral) terms, so a
+// Phys policy describes, per group, the input arrays, the pointwise integrand and the
+// numerical flux; this kernel does the data movement and the tensor-product algebra:
+//
+//   per group:  global -> smem (coalesced, 16-byte loads, odd-padded per cell)
+//               X pass : rows (i, P-i) combined even/odd, contracted along x  -> smem
+//               Z pass : member = quadrature column qx; points (qz, NQ-1-qz) in pairs,
+//                        integrand, then test-function contraction along z accumulated
+//                        in registers (even/odd split, constant-memory coefficients)
+//               faces  : member = face quadrature point; own trace and the neighbour's
+//                        trace (GLL nodes on the face), numerical flux, weighted and
+//                        accumulated per (face, output, point) in smem
+//   then:       XT pass: contraction along x of the accumulated rows, plus the face
+//                        terms on the face nodes -> smem -> coalesced global stores.
+//
+// Faces are evaluated from both sides (cell-centric): no atomics, deterministic, and the
+// flux seen by the two cells of a face is the exact negation of each other because the
+// normals come from the same two vertices.  Boundary faces call Phys::boundary.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <type_traits>
+#include <utility>
+
+#include "af_tables.cuh"
+
+namespace af {
+
+struct MeshDev {
+  const double2* vtx;  // (nz+1)*(nx+1) vertices, row-major in (j, i)
+  int nx, nz, periodic_x, gravity;
+  double radial_a;
+};
+
+struct PointGeo {
+  double X[2];  // physical position (valid when Phys::NEED_X)
+};
+
+template <int N, class F, int... I>
+__device__ __forceinline__ void sfor_impl(F& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void sfor(F&& f) {
+  sfor_impl<N>(f, std::make_integer_sequence<int, N>{});
+}
+
+template <int P>
+__device__ __forceinline__ const Tab<P>& tab();
+
+// Asynchronous global -> shared copies (all of a group in flight, one wait).
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+constexpr int odd(int n) { return n | 1; }
+
+// Cells per CTA and the CTAs-per-SM hint of __launch_bounds__, per degree.  Measured on
+// B200 for the fused stage-1 right-hand side at 512x256 cells, degree 4 (CB, MINB):
+// (16,1) 904 us, (16,2) 574 us, (32,1) 632 us, (8,3) 668 us, (24,1) 682 us.
+template <int P>
+constexpr int cells_per_block() {
+  return P <= 1 ? 64 : (P == 2 ? 32 : (P == 3 ? 32 : (P == 4 ? 16 : (P == 5 ? 16 : 8))));
+}
+template <int P>
+constexpr int min_blocks_per_sm() {
+  return P == 3 ? 1 : 2;
+}
+
+template <int MAXARR, int MAXOUT>
+struct ArgPtrs {
+  const double* in[MAXARR];
+  double* out[MAXOUT];
+};
+
+// ----------------------------------------------------------------------------------
+// compile-time helpers over a Phys policy
+// ----------------------------------------------------------------------------------
+template <class Phys, int G>
+struct GroupInfo {
+  static constexpr int NARR = Phys::template Grp<G>::NARR;
+  static constexpr int arr_base() {
+    int b = 0;
+    for (int g = 0; g < G; ++g) b += Phys::narr_of(g);
+    return b;
+  }
+  static constexpr int NF = [] {
+    int n = 0;
+    for (int a = 0; a < NARR; ++a) n += Phys::template Grp<G>::ncomp(a);
+    return n;
+  }();
+  static constexpr int NF_CELL = [] {  // fields used by cell integrals (face-only ones last)
+    int n = 0;
+    for (int a = 0; a < NARR; ++a)
+      if (!Phys::template Grp<G>::face_only(a)) n += Phys::template Grp<G>::ncomp(a);
+    return n;
+  }();
+};
+
+template <class Phys>
+struct PhysInfo {
+  static constexpr int NFMAX = [] {
+    int m = 0;
+    for (int g = 0; g < Phys::NG; ++g) m = m > Phys::nf_of(g) ? m : Phys::nf_of(g);
+    return m;
+  }();
+  static constexpr int NARR_TOTAL = [] {
+    int n = 0;
+    for (int g = 0; g < Phys::NG; ++g) n += Phys::narr_of(g);
+    return n;
+  }();
+};
+
+template <int P, class Phys, int CB_ = cells_per_block<P>()>
+struct Layout {
+  using T = Tab<P>;
+  static constexpr int P1 = T::P1, NQ = T::NQ, ND = P1 * P1;
+  static constexpr int CB = CB_;
+  static constexpr int NT = CB * NQ;
+  static constexpr int NDP = odd(ND);
+  static constexpr int P1P = odd(P1);
+  static constexpr int EOS = odd(P1 * NQ);
+  static constexpr int NF = PhysInfo<Phys>::NFMAX;
+  static constexpr int NOUT = Phys::NOUT;
+  static constexpr int R_IN = NF * CB * NDP;
+  static constexpr int R_NB = Phys::FACES ? 4 * NF * CB * P1P : 0;
+  static constexpr int R_EO = NF * CB * EOS;
+  static constexpr int R_ACC = NOUT * 2 * CB * EOS;
+  static constexpr int R0 = (R_IN + R_NB + R_EO) > R_ACC ? (R_IN + R_NB + R_EO) : R_ACC;
+  static constexpr int R_FLUX = Phys::FACES ? 4 * NOUT * CB * NQ : 0;
+  static constexpr int R_OUT = NOUT * CB * NDP;
+  static constexpr int R_GEO = CB * 24;  // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb
+  static constexpr int R_S = NQ * P1 + NQ;
+  static constexpr int TOTAL = R0 + R_FLUX + R_OUT + R_GEO + R_S;
+  static constexpr size_t BYTES = sizeof(double) * TOTAL;
+};
+
+// even/odd contraction of a P1-vector r along one direction to NQ values
+template <int P>
+__device__ __forceinline__ void contract_eo(const double* r, double* y) {
+  using T = Tab<P>;
+  const Tab<P>& t = tab<P>();
+  double re[T::H > 0 ? T::H : 1], ro[T::H > 0 ? T::H : 1];
+#pragma unroll
+  for (int i = 0; i < T::H; ++i) {
+    re[i] = r[i] + r[P - i];
+    ro[i] = r[i] - r[P - i];
+  }
+  const double rm = T::MIDN ? r[P / 2] : 0.0;
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    double e = 0.0, o = 0.0;
+#pragma unroll
+    for (int i = 0; i < T::H; ++i) {
+      e = fma(t.Se[k][i], re[i], e);
+      o = fma(t.So[k][i], ro[i], o);
+    }
+    if (T::MIDN) e = fma(t.Sm[k], rm, e);
+    y[k] = e + o;
+    y[T::NQ - 1 - k] = e - o;
+  }
+  double e = 0.0;
+#pragma unroll
+  for (int i = 0; i < T::H; ++i) e = fma(t.Se[P][i], re[i], e);
+  if (T::MIDN) e = fma(t.Sm[P], rm, e);
+  y[P] = e;
+}
+
+// ----------------------------------------------------------------------------------
+// the kernel
+// ----------------------------------------------------------------------------------
+template <int P, class Phys, int CB_ = cells_per_block<P>(), int MINB = min_blocks_per_sm<P>()>
+__global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
+    k_cellop(const MeshDev mesh, const ArgPtrs<PhysInfo<Phys>::NARR_TOTAL, Phys::NOUT_ARR> ptr,
+             const typename Phys::Params prm, const int ncell) {
+  using L = Layout<P, Phys, CB_>;
+  using T = Tab<P>;
+  constexpr int P1 = L::P1, NQ = L::NQ, ND = L::ND, CB = L::CB, NT = L::NT;
+  constexpr int H = T::H;
+  constexpr bool MIDN = T::MIDN;
+  constexpr int NOUT = Phys::NOUT;
+  const Tab<P>& tb = tab<P>();
+
+  extern __shared__ double smem[];
+  double* s_in = smem;
+  double* s_nb = s_in + L::R_IN;
+  double* s_eo = s_nb + L::R_NB;
+  double* s_acc = smem;  // aliases the group buffers after the last group
+  double* s_flux = smem + L::R0;
+  double* s_out = s_flux + L::R_FLUX;
+  double* s_geo = s_out + L::R_OUT;
+  double* s_S = s_geo + L::R_GEO;
+  double* s_w = s_S + NQ * P1;
+
+  const int tid = threadIdx.x;
+  const int m = tid / CB;   // member: row / column / face point
+  const int cl = tid % CB;  // cell within the block
+  const int c0 = blockIdx.x * CB;
+  const int ncb = min(CB, ncell - c0);  // valid cells in this block
+  const int c = c0 + (cl < ncb ? cl : ncb - 1);
+
+  // ---- per-cell geometry and neighbours (member 0), basis copy for runtime indexing
+  for (int k = tid; k < NQ * P1; k += NT) s_S[k] = tb.S[k / P1][k % P1];
+  for (int k = tid; k < NQ; k += NT) s_w[k] = tb.w[k];
+  if (m == 0) {
+    const int i = c % mesh.nx, j = c / mesh.nx, W = mesh.nx + 1;
+    const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
+    const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
+    double* g = s_geo + cl * 24;
+    g[0] = v1.x - v0.x; g[1] = v1.y - v0.y;                        // A = x_xi at eta = 0
+    g[2] = v3.x - v2.x - v1.x + v0.x; g[3] = v3.y - v2.y - v1.y + v0.y;  // B (bilinear term)
+    g[4] = v2.x - v0.x; g[5] = v2.y - v0.y;                        // C = x_eta at xi = 0
+    g[6] = v0.x; g[7] = v0.y;
+    // faces: 0 (xi=0, edge v0->v2), 1 (xi=1, v1->v3), 2 (eta=0, v0->v1), 3 (eta=1, v2->v3)
+    double tx, tz, len;
+    tx = v2.x - v0.x; tz = v2.y - v0.y; len = sqrt(tx * tx + tz * tz);
+    g[8] = -tz / len; g[9] = tx / len; g[10] = len;
+    tx = v3.x - v1.x; tz = v3.y - v1.y; len = sqrt(tx * tx + tz * tz);
+    g[11] = tz / len; g[12] = -tx / len; g[13] = len;
+    tx = v1.x - v0.x; tz = v1.y - v0.y; len = sqrt(tx * tx + tz * tz);
+    g[14] = tz / len; g[15] = -tx / len; g[16] = len;
+    tx = v3.x - v2.x; tz = v3.y - v2.y; len = sqrt(tx * tx + tz * tz);
+    g[17] = -tz / len; g[18] = tx / len; g[19] = len;
+    int nb0 = i > 0 ? c - 1 : (mesh.periodic_x ? c + mesh.nx - 1 : -1);
+    int nb1 = i < mesh.nx - 1 ? c + 1 : (mesh.periodic_x ? c - mesh.nx + 1 : -1);
+    int nb2 = j > 0 ? c - mesh.nx : -1;
+    int nb3 = j < mesh.nz - 1 ? c + mesh.nx : -1;
+    g[20] = (double)nb0; g[21] = (double)nb1; g[22] = (double)nb2; g[23] = (double)nb3;
+  }
+
+  // accumulators of the z-contraction (per output, per node row iz):
+  //   a = sum_qz S[qz][iz] (value JxW) + D[qz][iz] (eta-gradient),  b = sum_qz S[qz][iz] (xi-gradient)
+  double acc_a[NOUT][P1], acc_b[NOUT][P1];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+    for (int i = 0; i < P1; ++i) acc_a[o][i] = acc_b[o][i] = 0.0;
+  if (Phys::FACES) {
+    for (int k = tid; k < L::R_FLUX; k += NT) s_flux[k] = 0.0;
+  }
+
+  sfor<Phys::NG>([&](auto gc) {
+    constexpr int G = decltype(gc)::value;
+    using Gi = GroupInfo<Phys, G>;
+    using Gr = typename Phys::template Grp<G>;
+    constexpr int NF = Gi::NF, NFC = Gi::NF_CELL;
+    constexpr bool GFACE = Phys::FACES && Gr::FACE;
+
+    __syncthreads();  // previous group done with the smem buffers
+    // ---- load the group's arrays and the neighbours' face nodes: asynchronous copies,
+    //      all in flight, one wait (own cells: contiguous chunk per array, coalesced)
+    {
+      sfor<Gi::NARR>([&](auto ac) {
+        constexpr int A = decltype(ac)::value;
+        constexpr int NC = Gr::ncomp(A);
+        constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+        const double* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+        for (int e = tid; e < ncb * NC * ND; e += NT) {
+          const int cc = e / (NC * ND), r = e % (NC * ND);
+          cp_async8(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
+        }
+      });
+    }
+    // neighbour face nodes (L2-resident), ordered along the face parameter
+    if constexpr (GFACE) {
+      constexpr int TOT = 4 * NF * CB * P1;
+      for (int k = tid; k < TOT; k += NT) {
+        const int i = k % P1;
+        const int cc = (k / P1) % CB;
+        const int fi = (k / (P1 * CB)) % NF;
+        const int f = k / (P1 * CB * NF);
+        const int nb = (int)s_geo[cc * 24 + 20 + f];
+        double* dst = &s_nb[((f * NF + fi) * CB + cc) * L::P1P + i];
+        if (nb >= 0 && cc < ncb) {
+          const int kk = f == 0 ? i * P1 + P : (f == 1 ? i * P1 : (f == 2 ? P * P1 + i : i));
+          int a = 0, comp = fi;
+#pragma unroll
+          for (int aa = 0; aa < Gi::NARR; ++aa)
+            if (a == aa && comp >= Gr::ncomp(aa)) { comp -= Gr::ncomp(aa); ++a; }
+          const int nc = Gr::ncomp(a);
+          const double* base = nullptr;  // select with compile-time indices (no param copy)
+#pragma unroll
+          for (int aa = 0; aa < Gi::NARR; ++aa)
+            if (aa == a) base = ptr.in[Gi::arr_base() + aa];
+          cp_async8(dst, base + (size_t)nb * nc * ND + comp * ND + kk);
+        } else {
+          *dst = 0.0;
+        }
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // ---- X pass: rows (k, P-k) even/odd, contracted along x, for the cell fields
+    {
+      constexpr int NPR = H + (MIDN ? 1 : 0);
+      for (int task = m; task < NFC * NPR; task += NQ) {
+        const int fi = task / NPR, k = task % NPR;
+        const double* cell = s_in + (fi * CB + cl) * L::NDP;
+        double* eo = s_eo + (fi * CB + cl) * L::EOS;
+        double r[P1], y[NQ];
+        if (k < H) {
+#pragma unroll
+          for (int ix = 0; ix < P1; ++ix) r[ix] = cell[k * P1 + ix] + cell[(P - k) * P1 + ix];
+          contract_eo<P>(r, y);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) eo[k * NQ + q] = y[q];
+#pragma unroll
+          for (int ix = 0; ix < P1; ++ix) r[ix] = cell[k * P1 + ix] - cell[(P - k) * P1 + ix];
+          contract_eo<P>(r, y);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) eo[(H + k) * NQ + q] = y[q];
+        } else {
+#pragma unroll
+          for (int ix = 0; ix < P1; ++ix) r[ix] = cell[(P / 2) * P1 + ix];
+          contract_eo<P>(r, y);
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) eo[(2 * H) * NQ + q] = y[q];
+        }
+      }
+    }
+    __syncthreads();
+    // ---- Z pass: member = quadrature column qx.  Points are evaluated in mirror pairs
+    //      (qz, NQ-1-qz) from the even/odd rows (read from smem), and each point's
+    //      integrand is contracted into the per-row accumulators right away.
+    if constexpr (NFC > 0) {
+      const int qx = m;
+      const double* g = s_geo + cl * 24;
+      const double xi = tb.x[qx];
+      const double wx = s_w[qx];
+      const double J01 = fma(g[2], xi, g[4]);  // x_eta (x component)
+      const double J11 = fma(g[3], xi, g[5]);  // x_eta (z component)
+      auto point = [&](const double* v, const int qz) {
+        const double eta = tb.x[qz];
+        const double J00 = fma(g[2], eta, g[0]);
+        const double J10 = fma(g[3], eta, g[1]);
+        const double w = wx * tb.w[qz];
+        const double det = J00 * J11 - J01 * J10;
+        PointGeo pg;
+        if (Phys::NEED_X) {
+          pg.X[0] = g[6] + g[0] * xi + g[4] * eta + g[2] * xi * eta;
+          pg.X[1] = g[7] + g[1] * xi + g[5] * eta + g[3] * xi * eta;
+        }
+        double val[NOUT], gr[NOUT][2];
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) { val[o] = 0.0; gr[o][0] = gr[o][1] = 0.0; }
+        Phys::template point<G>(prm, v, pg, val, gr);
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) {
+          const bool hv = Phys::has_val(o), hg = Phys::has_grad(o);
+          const double fv = val[o] * det * w;
+          const double fx = (J11 * gr[o][0] - J01 * gr[o][1]) * w;  // adj(J) g, xi row
+          const double fe = (J00 * gr[o][1] - J10 * gr[o][0]) * w;  // adj(J) g, eta row
+#pragma unroll
+          for (int iz = 0; iz < P1; ++iz) {
+            if (hv) acc_a[o][iz] = fma(tb.S[qz][iz], fv, acc_a[o][iz]);
+            if (hg) {
+              acc_a[o][iz] = fma(tb.D[qz][iz], fe, acc_a[o][iz]);
+              acc_b[o][iz] = fma(tb.S[qz][iz], fx, acc_b[o][iz]);
+            }
+          }
+        }
+      };
+#pragma unroll
+      for (int k = 0; k <= P; ++k) {
+        const bool pair = k < P;
+        double v1[NF > 0 ? NF : 1], v2[NF > 0 ? NF : 1];
+#pragma unroll
+        for (int fi = 0; fi < NFC; ++fi) {
+          const double* eo = s_eo + (fi * CB + cl) * L::EOS + qx;
+          double e = 0.0, o = 0.0;
+#pragma unroll
+          for (int i = 0; i < H; ++i) {
+            e = fma(tb.Se[k][i], eo[i * NQ], e);
+            if (pair) o = fma(tb.So[k][i], eo[(H + i) * NQ], o);
+          }
+          if (MIDN) e = fma(tb.Sm[k], eo[(2 * H) * NQ], e);
+          v1[fi] = e + o;
+          v2[fi] = e - o;
+        }
+        point(v1, k);
+        if (pair) point(v2, NQ - 1 - k);
+      }
+    }
+    // ---- faces: member = face quadrature point
+    if constexpr (GFACE) {
+      const int q = m;
+      double sq[P1];
+#pragma unroll
+      for (int i = 0; i < P1; ++i) sq[i] = s_S[q * P1 + i];
+      const double wq = s_w[q];
+      const double* g = s_geo + cl * 24;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const int nb = (int)g[20 + f];
+        double vp[NF], vm[NF];
+#pragma unroll
+        for (int fi = 0; fi < NF; ++fi) {
+          const double* cell = s_in + (fi * CB + cl) * L::NDP;
+          const double* nbv = s_nb + ((f * NF + fi) * CB + cl) * L::P1P;
+          double a = 0.0, b = 0.0;
+#pragma unroll
+          for (int i = 0; i < P1; ++i) {
+            const int kk = f == 0 ? i * P1 : (f == 1 ? i * P1 + P : (f == 2 ? i : P * P1 + i));
+            a = fma(sq[i], cell[kk], a);
+            b = fma(sq[i], nbv[i], b);
+          }
+          vp[fi] = a;
+          vm[fi] = b;
+        }
+        const double n[2] = {g[8 + 3 * f], g[9 + 3 * f]};
+        const double jxw = g[10 + 3 * f] * wq;
+        double flux[NOUT];
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) flux[o] = 0.0;
+        if (nb >= 0) Phys::template face<G>(prm, vp, vm, n, flux);
+        else Phys::template boundary<G>(prm, vp, n, flux);
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) s_flux[((f * NOUT + o) * CB + cl) * NQ + q] += flux[o] * jxw;
+      }
+    }
+  });
+
+  __syncthreads();  // all groups done: reuse the group buffers for the accumulators
+  {
+    const int qx = m;
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      double* A = s_acc + ((o * 2 + 0) * CB + cl) * L::EOS;
+      double* B = s_acc + ((o * 2 + 1) * CB + cl) * L::EOS;
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) {
+        A[iz * NQ + qx] = acc_a[o][iz];
+        B[iz * NQ + qx] = acc_b[o][iz];
+      }
+    }
+  }
+  __syncthreads();
+  // ---- XT pass: task (output, row iz) -> P1 outputs, plus face terms on face nodes
+  for (int task = m; task < NOUT * P1; task += NQ) {
+    const int o = task / P1, iz = task % P1;
+    const double* A = s_acc + ((o * 2 + 0) * CB + cl) * L::EOS + iz * NQ;
+    const double* B = s_acc + ((o * 2 + 1) * CB + cl) * L::EOS + iz * NQ;
+    double oE[H > 0 ? H : 1], oO[H > 0 ? H : 1], oM = 0.0;
+#pragma unroll
+    for (int i = 0; i < H; ++i) oE[i] = oO[i] = 0.0;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      const double a1 = A[k], a2 = A[NQ - 1 - k], b1 = B[k], b2 = B[NQ - 1 - k];
+      const double As = a1 + a2, Ad = a1 - a2, Bs = b1 + b2, Bd = b1 - b2;
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        oE[i] = fma(tb.Se[k][i], As, oE[i]);
+        oE[i] = fma(tb.De[k][i], Bd, oE[i]);
+        oO[i] = fma(tb.So[k][i], Ad, oO[i]);
+        oO[i] = fma(tb.Do[k][i], Bs, oO[i]);
+      }
+      if (MIDN) { oM = fma(tb.Sm[k], As, oM); oM = fma(tb.Dm[k], Bd, oM); }
+    }
+    {
+      const double am = A[P], bm = B[P];
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        oE[i] = fma(tb.Se[P][i], am, oE[i]);
+        oO[i] = fma(tb.Do[P][i], bm, oO[i]);
+      }
+      if (MIDN) oM = fma(tb.Sm[P], am, oM);
+    }
+    double out[P1];
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      out[i] = oE[i] + oO[i];
+      out[P - i] = oE[i] - oO[i];
+    }
+    if (MIDN) out[P / 2] = oM;
+    if (Phys::FACES) {
+      const double* F0 = s_flux + ((0 * NOUT + o) * CB + cl) * NQ;
+      const double* F1 = s_flux + ((1 * NOUT + o) * CB + cl) * NQ;
+      double l = 0.0, r = 0.0;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const double s = s_S[q * P1 + iz];
+        l = fma(s, F0[q], l);
+        r = fma(s, F1[q], r);
+      }
+      out[0] += l;
+      out[P] += r;
+      if (iz == 0 || iz == P) {
+        const double* F = s_flux + (((iz == 0 ? 2 : 3) * NOUT + o) * CB + cl) * NQ;
+#pragma unroll
+        for (int ix = 0; ix < P1; ++ix) {
+          double s = 0.0;
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) s = fma(tb.S[q][ix], F[q], s);
+          out[ix] += s;
+        }
+      }
+    }
+    double* dst = s_out + (o * CB + cl) * L::NDP + iz * P1;
+#pragma unroll
+    for (int ix = 0; ix < P1; ++ix) dst[ix] = out[ix];
+  }
+  __syncthreads();
+  // ---- store (coalesced)
+  {
+    int obase = 0;
+    sfor<Phys::NOUT_ARR>([&](auto oc) {
+      constexpr int OA = decltype(oc)::value;
+      constexpr int NC = Phys::out_ncomp(OA);
+      constexpr int ob = [] { int b = 0; for (int a = 0; a < OA; ++a) b += Phys::out_ncomp(a); return b; }();
+      double* dst = ptr.out[OA] + (size_t)c0 * NC * ND;
+      for (int e = tid; e < ncb * NC * ND; e += NT) {
+        const int cc = e / (NC * ND), r = e % (NC * ND);
+        const double v = s_out[((ob + r / ND) * CB + cc) * L::NDP + r % ND];
+        if (Phys::ACCUMULATE) dst[e] += v;
+        else dst[e] = v;
+      }
+      (void)obase;
+    });
+  }
+}
+
+template <int P, class Phys, int CB_ = cells_per_block<P>(), int MINB = min_blocks_per_sm<P>()>
+cudaError_t launch_cellop(const MeshDev& mesh, const ArgPtrs<PhysInfo<Phys>::NARR_TOTAL, Phys::NOUT_ARR>& ptr,
+                          const typename Phys::Params& prm, int ncell, cudaStream_t stream) {
+  using L = Layout<P, Phys, CB_>;
+  static bool configured = false;  // per instantiation; the attribute is per device function
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_cellop<P, Phys, CB_, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)L::BYTES);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int nblk = (ncell + L::CB - 1) / L::CB;
+  k_cellop<P, Phys, CB_, MINB><<<nblk, L::NT, L::BYTES, stream>>>(mesh, ptr, prm, ncell);
+  return cudaGetLastError();
+}
+
+}  // namespace af

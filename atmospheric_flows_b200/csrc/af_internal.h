@@ -1,0 +1,45 @@
+// af_internal.h -- host-side declarations shared by the C ABI and the per-degree kernel
+// translation units (af_kern.cu is compiled once per polynomial degree 1..6).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "af_cellop.cuh"
+#include "af_physics.cuh"
+
+namespace af {
+
+// Sources of an explicit right-hand side in the reference's positional order of
+// vmult_rhs_pressure (the superset list, Atmospheric_Flow.cc:555-556, 562-564, 796-799):
+//   stage 1: rho0 u0 p0 rho2 u_fixed
+//   stage 2: rho0 u0 p0 rho2 u2 p2 rho3 u_fixed
+//   stage 3: rho0 u0 p0 rho2 u2 p2 rho3 u3 p3 rho_curr u_curr
+// Unused slots may be null.
+struct RhsSources {
+  const double* rho[3];
+  const double* u[3];
+  const double* p[3];
+  const double* rho_c;  // rho_tmp_2 / rho_tmp_3 / rho_curr
+  const double* u_fix;  // u_fixed / u_curr
+};
+
+struct DegreeOps {
+  cudaError_t (*upload_tables)();
+  cudaError_t (*rhs)(const MeshDev&, int stage, int mask, const RhsSources&, const RhsParams&, double* out_rho,
+                     double* out_u, double* out_p, int ncell, cudaStream_t);
+  // dst = scale * M src (ncomp 1 or 2), or M_rho src with a density weight
+  cudaError_t (*mass)(const MeshDev&, int ncomp, const double* src, const double* weight, double scale, double* dst,
+                      int ncell, cudaStream_t);
+  cudaError_t (*op_B)(const MeshDev&, const double* p, double c, double* u, int ncell, cudaStream_t);
+  // dst = C w (sign +1), or dst = D p - C w when p != null
+  cudaError_t (*op_C)(const MeshDev&, const double* w, const double* pf, const double* p, const CParams&, double* dst,
+                      int ncell, cudaStream_t);
+  // inverse of the diagonal of scale*M (weight null) or of M_rho (ncomp copies)
+  cudaError_t (*inv_diag)(const MeshDev&, int ncomp, const double* weight, double scale, double* dst, int ncell,
+                          cudaStream_t);
+  int cells_per_block;
+};
+
+const DegreeOps* degree_ops(int P);  // null if the degree was not compiled
+
+}  // namespace af

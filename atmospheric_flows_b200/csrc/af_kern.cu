@@ -1,0 +1,200 @@
+// af_kern.cu -- per-degree kernel instantiations.  Compiled once per polynomial degree
+// with -DAF_P=<p>; each object registers its entry points in the degree table used by
+// the C ABI (af_capi.cu).
+#include <cstdio>
+
+#include "af_internal.h"
+
+#ifndef AF_P
+#error "compile with -DAF_P=<degree>"
+#endif
+
+namespace af {
+
+static __constant__ Tab<AF_P> c_tab;
+
+template <>
+__device__ __forceinline__ const Tab<AF_P>& tab<AF_P>() {
+  return c_tab;
+}
+
+namespace {
+
+constexpr int P = AF_P;
+
+cudaError_t upload_tables() {
+  static const Tab<P> t = host::make_tab<P>();
+  return cudaMemcpyToSymbol(c_tab, &t, sizeof(t));
+}
+
+template <int STAGE, int MASK>
+cudaError_t rhs_mask(const MeshDev& mesh, const RhsSources& s, const RhsParams& prm, double* o_rho, double* o_u,
+                     double* o_p, int ncell, cudaStream_t st) {
+  using Ph = RhsPhys<STAGE, MASK>;
+  ArgPtrs<PhysInfo<Ph>::NARR_TOTAL, Ph::NOUT_ARR> a{};
+  int k = 0;
+  for (int j = 0; j < STAGE; ++j) {
+    a.in[k++] = s.rho[j];
+    a.in[k++] = s.u[j];
+    if (Ph::VEL || Ph::PRES) a.in[k++] = s.p[j];
+    if (Ph::quirk_group(j)) a.in[k++] = s.u[0];
+  }
+  if (Ph::HAS_I) {
+    a.in[k++] = s.rho_c;
+    if (Ph::PRES) a.in[k++] = s.u_fix;
+  }
+  int o = 0;
+  if (Ph::RHO) a.out[o++] = o_rho;
+  if (Ph::VEL) a.out[o++] = o_u;
+  if (Ph::PRES) a.out[o++] = o_p;
+  for (int i = 0; i < k; ++i)
+    if (!a.in[i]) return cudaErrorInvalidValue;
+  for (int i = 0; i < o; ++i)
+    if (!a.out[i]) return cudaErrorInvalidValue;
+  return launch_cellop<P, Ph>(mesh, a, prm, ncell, st);
+}
+
+template <int STAGE>
+cudaError_t rhs_stage(const MeshDev& mesh, int mask, const RhsSources& s, const RhsParams& prm, double* o_rho,
+                      double* o_u, double* o_p, int ncell, cudaStream_t st) {
+  switch (mask) {
+    case 1: return rhs_mask<STAGE, 1>(mesh, s, prm, o_rho, o_u, o_p, ncell, st);
+    case 2: return rhs_mask<STAGE, 2>(mesh, s, prm, o_rho, o_u, o_p, ncell, st);
+    case 4: return rhs_mask<STAGE, 4>(mesh, s, prm, o_rho, o_u, o_p, ncell, st);
+    case 6: return rhs_mask<STAGE, 6>(mesh, s, prm, o_rho, o_u, o_p, ncell, st);
+    case 7: return rhs_mask<STAGE, 7>(mesh, s, prm, o_rho, o_u, o_p, ncell, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t rhs(const MeshDev& mesh, int stage, int mask, const RhsSources& s, const RhsParams& prm, double* o_rho,
+                double* o_u, double* o_p, int ncell, cudaStream_t st) {
+  switch (stage) {
+    case 1: return rhs_stage<1>(mesh, mask, s, prm, o_rho, o_u, o_p, ncell, st);
+    case 2: return rhs_stage<2>(mesh, mask, s, prm, o_rho, o_u, o_p, ncell, st);
+    case 3: return rhs_stage<3>(mesh, mask, s, prm, o_rho, o_u, o_p, ncell, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t mass(const MeshDev& mesh, int ncomp, const double* src, const double* weight, double scale, double* dst,
+                 int ncell, cudaStream_t st) {
+  MassParams prm{scale};
+  if (weight) {
+    if (ncomp == 2) {
+      ArgPtrs<2, 1> a{{src, weight}, {dst}};
+      return launch_cellop<P, MassPhys<2, true>>(mesh, a, prm, ncell, st);
+    }
+    ArgPtrs<2, 1> a{{src, weight}, {dst}};
+    return launch_cellop<P, MassPhys<1, true>>(mesh, a, prm, ncell, st);
+  }
+  if (ncomp == 2) {
+    ArgPtrs<1, 1> a{{src}, {dst}};
+    return launch_cellop<P, MassPhys<2, false>>(mesh, a, prm, ncell, st);
+  }
+  ArgPtrs<1, 1> a{{src}, {dst}};
+  return launch_cellop<P, MassPhys<1, false>>(mesh, a, prm, ncell, st);
+}
+
+cudaError_t op_B(const MeshDev& mesh, const double* p, double c, double* u, int ncell, cudaStream_t st) {
+  ArgPtrs<1, 1> a{{p}, {u}};
+  return launch_cellop<P, BPhys>(mesh, a, BParams{c}, ncell, st);
+}
+
+cudaError_t op_C(const MeshDev& mesh, const double* w, const double* pf, const double* p, const CParams& prm,
+                 double* dst, int ncell, cudaStream_t st) {
+  if (p) {
+    ArgPtrs<3, 1> a{{p, w, pf}, {dst}};
+    return launch_cellop<P, CPhys<true, -1>>(mesh, a, prm, ncell, st);
+  }
+  ArgPtrs<2, 1> a{{w, pf}, {dst}};
+  return launch_cellop<P, CPhys<false, 1>>(mesh, a, prm, ncell, st);
+}
+
+// Diagonal of the (weighted) mass matrix, inverted:
+//   diag_i = sum_q l_i(x_q)^2 l_j(z_q)^2 w(q) JxW(q)   (what the reference's unit-vector
+//   probing in assemble_diagonal_cell_term_* computes, euler_operator.h:2458-2586)
+__global__ void k_inv_diag(const MeshDev mesh, const double* __restrict__ weight, const double scale,
+                           double* __restrict__ dst, const int ncomp, const int ncell) {
+  using T = Tab<P>;
+  constexpr int P1 = T::P1, NQ = T::NQ, ND = P1 * P1;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const Tab<P>& tb = c_tab;
+  const int i = c % mesh.nx, j = c / mesh.nx, W = mesh.nx + 1;
+  const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
+  const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
+  const double Ax = v1.x - v0.x, Az = v1.y - v0.y, Cx = v2.x - v0.x, Cz = v2.y - v0.y;
+  const double Bx = v3.x - v2.x - v1.x + v0.x, Bz = v3.y - v2.y - v1.y + v0.y;
+  double wn[ND];
+  if (weight) {
+#pragma unroll
+    for (int k = 0; k < ND; ++k) wn[k] = weight[(size_t)c * ND + k];
+  }
+  double dz[P1][NQ];
+#pragma unroll
+  for (int iz = 0; iz < P1; ++iz)
+#pragma unroll
+    for (int qx = 0; qx < NQ; ++qx) dz[iz][qx] = 0.0;
+  for (int qx = 0; qx < NQ; ++qx) {
+    double tx[P1];
+    if (weight) {
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) {
+        double s = 0.0;
+#pragma unroll
+        for (int ix = 0; ix < P1; ++ix) s = fma(tb.S[qx][ix], wn[iz * P1 + ix], s);
+        tx[iz] = s;
+      }
+    }
+    const double xi = tb.x[qx];
+    const double J01 = fma(Bx, xi, Cx), J11 = fma(Bz, xi, Cz);
+#pragma unroll
+    for (int qz = 0; qz < NQ; ++qz) {
+      const double eta = tb.x[qz];
+      const double J00 = fma(Bx, eta, Ax), J10 = fma(Bz, eta, Az);
+      double f = (J00 * J11 - J01 * J10) * tb.w[qx] * tb.w[qz];
+      if (weight) {
+        double wv = 0.0;
+#pragma unroll
+        for (int iz = 0; iz < P1; ++iz) wv = fma(tb.S[qz][iz], tx[iz], wv);
+        f *= wv;
+      } else {
+        f *= scale;
+      }
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) dz[iz][qx] = fma(tb.S[qz][iz] * tb.S[qz][iz], f, dz[iz][qx]);
+    }
+  }
+#pragma unroll
+  for (int iz = 0; iz < P1; ++iz)
+#pragma unroll
+    for (int ix = 0; ix < P1; ++ix) {
+      double s = 0.0;
+#pragma unroll
+      for (int qx = 0; qx < NQ; ++qx) s = fma(tb.S[qx][ix] * tb.S[qx][ix], dz[iz][qx], s);
+      const double inv = 1.0 / s;
+      for (int d = 0; d < ncomp; ++d) dst[((size_t)c * ncomp + d) * ND + iz * P1 + ix] = inv;
+    }
+}
+
+cudaError_t inv_diag(const MeshDev& mesh, int ncomp, const double* weight, double scale, double* dst, int ncell,
+                     cudaStream_t st) {
+  const int bs = 128;
+  k_inv_diag<<<(ncell + bs - 1) / bs, bs, 0, st>>>(mesh, weight, scale, dst, ncomp, ncell);
+  return cudaGetLastError();
+}
+
+const DegreeOps kOps = {upload_tables, rhs, mass, op_B, op_C, inv_diag, cells_per_block<P>()};
+
+}  // namespace
+
+void register_degree(int p, const DegreeOps* ops);
+
+namespace {
+struct Registrar {
+  Registrar() { register_degree(P, &kOps); }
+} registrar;
+}  // namespace
+
+}  // namespace af

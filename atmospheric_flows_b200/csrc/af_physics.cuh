@@ -1,0 +1,331 @@
+// af_physics.cuh -- pointwise integrands and numerical fluxes of the reference's operators,
+// as policies for the generic kernel in af_cellop.cuh.
+//
+// Each policy restates, per group of input fields, one family of EULEROperator integrals
+// (file:line in the reference's euler_operator.h):
+//   RhsPhys<STAGE, MASK>  assemble_rhs_{cell,face,boundary}_term_{rho_update,pressure,
+//                         velocity_fixed} for HYPERBOLIC_stage = STAGE, fused over the
+//                         equations selected by MASK (1 density, 2 velocity, 4 pressure):
+//                         :344-692, :745-1361, :1622-2305
+//   BPhys                 assemble_{cell,face,boundary}_term_pressure (matrix B) :1512-1617
+//   CPhys<WITH_D, SIGN>   assemble_{cell,face}_term_enthalpy (matrix C) :1413-1507, with
+//                         the internal-energy mass D (:1386-1408) fused for the Schur
+//                         complement output D p - C w (:2374-2408)
+//   MassPhys<NC, W>       assemble_cell_term_{rho_update,internal_energy,velocity_fixed}
+//                         (:715-740, :1386-1408, :2330-2357)
+//
+// Conventions of the cell-centric kernel: the calling cell is always the "+" side, n its
+// outward unit normal, and the returned flux is the integrand tested against the cell's
+// own basis functions on that face (already carrying the reference's phi_p sign).
+// Integrands are algebraically equal to the reference's (e.g. rho*(p/((g-1) rho)) is
+// formed as p/(g-1)); the oracle keeps the literal forms and parity is checked at 1e-12.
+#pragma once
+
+#include "af_cellop.cuh"
+
+namespace af {
+
+struct RhsParams {
+  double dt, Ma2, invMa2, invFr2, Ma2Fr2, a2;
+  double g1, gg;          // 1/(gamma-1), gamma/(gamma-1)
+  double ca[3], ct[3];    // explicit weights a_j and a~_j of the stage's explicit terms
+  double cg[3], cgI;      // gravity weights of the explicit terms and of the implicit one
+  int radial;             // 0: e_z, |g| const; 1: e_r = X/|X|, factor a^2/|X|^2
+};
+
+__device__ __forceinline__ void gravity_dir(const RhsParams& prm, const PointGeo& pg, double& e0, double& e1,
+                                            double& fac) {
+  if (prm.radial) {
+    const double r2 = pg.X[0] * pg.X[0] + pg.X[1] * pg.X[1];
+    const double ir = 1.0 / sqrt(r2);
+    e0 = pg.X[0] * ir;
+    e1 = pg.X[1] * ir;
+    fac = prm.a2 / r2;
+  } else {
+    e0 = 0.0;
+    e1 = 1.0;
+    fac = 1.0;
+  }
+}
+
+template <int STAGE, int MASK>
+struct RhsPhys {
+  static constexpr bool RHO = (MASK & 1) != 0, VEL = (MASK & 2) != 0, PRES = (MASK & 4) != 0;
+  static constexpr bool HAS_I = STAGE < 3 ? (VEL || PRES) : PRES;
+  static constexpr int NG = STAGE + (HAS_I ? 1 : 0);
+  static constexpr bool FACES = true, NEED_X = true, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = (RHO ? 1 : 0) + (VEL ? 1 : 0) + (PRES ? 1 : 0);
+  static constexpr int NOUT = (RHO ? 1 : 0) + (VEL ? 2 : 0) + (PRES ? 1 : 0);
+  static constexpr int O_RHO = 0, O_U = RHO ? 1 : 0, O_P = (RHO ? 1 : 0) + (VEL ? 2 : 0);
+  using Params = RhsParams;
+
+  static constexpr int out_ncomp(int a) {
+    // output arrays in the order rho, u, p (present ones only)
+    return (VEL && a == (RHO ? 1 : 0)) ? 2 : 1;
+  }
+  static constexpr bool has_val(int) { return true; }
+  static constexpr bool has_grad(int) { return true; }
+
+  static constexpr bool quirk_group(int g) { return STAGE == 2 && PRES && g == 1; }
+  static constexpr int narr_of(int g) {
+    if (g < STAGE) return 2 + ((VEL || PRES) ? 1 : 0) + (quirk_group(g) ? 1 : 0);
+    return STAGE < 3 ? (1 + (PRES ? 1 : 0)) : 2;
+  }
+  static constexpr int nf_of(int g) {
+    if (g < STAGE) return 3 + ((VEL || PRES) ? 1 : 0) + (quirk_group(g) ? 2 : 0);
+    return STAGE < 3 ? (1 + (PRES ? 2 : 0)) : 3;
+  }
+
+  template <int G>
+  struct Grp {
+    static constexpr bool EXPL = G < STAGE;
+    static constexpr int NARR = narr_of(G);
+    static constexpr bool FACE = EXPL;
+    // explicit: rho_j, u_j, [p_j], [u_0 face-only];  implicit: rho_c, [u_fixed]
+    static constexpr int ncomp(int a) { return a == 1 ? 2 : (EXPL && a == 3 ? 2 : 1); }
+    static constexpr bool face_only(int a) { return EXPL && a == 3; }
+  };
+
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo& pg,
+                                               double* val, double (*gr)[2]) {
+    double e0, e1, fac;
+    gravity_dir(prm, pg, e0, e1, fac);
+    if constexpr (G < STAGE) {
+      const double rho = v[0], ux = v[1], uz = v[2];
+      const double ca = prm.ca[G] * prm.dt, cg = prm.cg[G] * prm.dt;
+      if constexpr (RHO) {  // euler_operator.h:378-380 (and stage 2/3 analogues)
+        if (G == 0) val[O_RHO] += rho;
+        gr[O_RHO][0] += ca * rho * ux;
+        gr[O_RHO][1] += ca * rho * uz;
+      }
+      if constexpr (VEL || PRES) {
+        const double p = v[3];
+        const double ct = prm.ct[G] * prm.dt;
+        if constexpr (VEL) {  // :1686-1691
+          if (G == 0) { val[O_U] += rho * ux; val[O_U + 1] += rho * uz; }
+          const double gfac = cg * prm.invFr2 * rho * fac;
+          val[O_U] -= gfac * e0;
+          val[O_U + 1] -= gfac * e1;
+          const double cr = ca * rho, pt = ct * prm.invMa2 * p;
+          gr[O_U][0] += cr * ux * ux + pt;
+          gr[O_U][1] += cr * ux * uz;
+          gr[O_U + 1][0] += cr * uz * ux;
+          gr[O_U + 1][1] += cr * uz * uz + pt;
+        }
+        if constexpr (PRES) {  // :806-813: rho E = p/(g-1) + Ma^2 rho |u|^2 / 2
+          const double uu = ux * ux + uz * uz;
+          if (G == 0) val[O_P] += p * prm.g1 + 0.5 * prm.Ma2 * rho * uu;
+          val[O_P] -= cg * prm.Ma2Fr2 * rho * (ux * e0 + uz * e1) * fac;
+          const double s = 0.5 * ca * prm.Ma2 * uu * rho + ct * prm.gg * p;
+          gr[O_P][0] += s * ux;
+          gr[O_P][1] += s * uz;
+        }
+      }
+    } else {
+      const double rc = v[0];
+      const double cgI = prm.cgI * prm.dt;
+      if constexpr (VEL && STAGE < 3) {
+        const double gfac = cgI * prm.invFr2 * rc * fac;
+        val[O_U] -= gfac * e0;
+        val[O_U + 1] -= gfac * e1;
+      }
+      if constexpr (PRES) {
+        const double fx = v[1], fz = v[2];
+        val[O_P] -= 0.5 * rc * prm.Ma2 * (fx * fx + fz * fz);
+        if (STAGE < 3) val[O_P] -= cgI * prm.Ma2Fr2 * rc * (fx * e0 + fz * e1) * fac;
+      }
+    }
+  }
+
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    if constexpr (G < STAGE) {
+      const double rp = vp[0], upx = vp[1], upz = vp[2];
+      const double rm = vm[0], umx = vm[1], umz = vm[2];
+      const double unp = upx * n[0] + upz * n[1], unm = umx * n[0] + umz * n[1];
+      const double lam = fmax(fabs(unp), fabs(unm));
+      const double ca = prm.ca[G] * prm.dt;
+      if constexpr (RHO) {  // :519-526
+        const double F = ca * (0.5 * (rp * unp + rm * unm) + 0.5 * lam * (rp - rm));
+        flux[O_RHO] = -F;
+      }
+      if constexpr (VEL || PRES) {
+        const double pp = vp[3], pm = vm[3];
+        const double ct = prm.ct[G] * prm.dt;
+        if constexpr (VEL) {  // :1938-1950
+          const double pa = ct * prm.invMa2 * 0.5 * (pp + pm);
+          const double Fx = ca * 0.5 * (rp * upx * unp + rm * umx * unm) + pa * n[0] + ca * 0.5 * lam * (rp * upx - rm * umx);
+          const double Fz = ca * 0.5 * (rp * upz * unp + rm * umz * unm) + pa * n[1] + ca * 0.5 * lam * (rp * upz - rm * umz);
+          flux[O_U] = -Fx;
+          flux[O_U + 1] = -Fz;
+        }
+        if constexpr (PRES) {  // :1057-1079 (stage 1), :1141-1194 (2), :1275-1355 (3)
+          const double uup = upx * upx + upz * upz, uum = umx * umx + umz * umz;
+          const double kin = 0.5 * (0.5 * uup * rp * unp + 0.5 * uum * rm * unm);
+          const double ent = 0.5 * prm.gg * (pp * unp + pm * unm);
+          double F;
+          if constexpr (STAGE < 3) {
+            double jk;
+            if constexpr (quirk_group(G)) {  // :1182-1183 uses u_tmp_2 . u_old
+              jk = rp * 0.5 * (upx * vp[4] + upz * vp[5]) - rm * 0.5 * (umx * vm[4] + umz * vm[5]);
+            } else {
+              jk = rp * 0.5 * uup - rm * 0.5 * uum;
+            }
+            const double je = prm.g1 * (pp - pm);
+            F = ca * prm.Ma2 * (kin + 0.5 * lam * jk) + ct * (ent + 0.5 * lam * je);
+          } else {
+            const double jE = prm.g1 * (pp - pm) + 0.5 * prm.Ma2 * (rp * uup - rm * uum);
+            F = ca * prm.Ma2 * kin + ca * ent + ca * 0.5 * lam * jE;
+          }
+          flux[O_P] = -F;
+        }
+      }
+    }
+  }
+
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
+                                                  double* flux) {
+    if constexpr (G < STAGE && VEL) {  // :2189-2305, p_D = p
+      const double pp = vp[3];
+      const double s = prm.ct[G] * prm.dt * prm.invMa2 * (0.5 * (pp + pp));
+      flux[O_U] = -s * n[0];
+      flux[O_U + 1] = -s * n[1];
+    }
+  }
+};
+
+// ---------------------------------------------------------------- B: p -> u
+struct BParams {
+  double c;  // coeff * dt / Ma^2, coeff = a~22 (stage 1) or a~33
+};
+
+struct BPhys {
+  static constexpr int NG = 1;
+  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = 2;
+  using Params = BParams;
+  static constexpr int out_ncomp(int) { return 2; }
+  static constexpr bool has_val(int) { return false; }
+  static constexpr bool has_grad(int) { return true; }
+  static constexpr int narr_of(int) { return 1; }
+  static constexpr int nf_of(int) { return 1; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = 1;
+    static constexpr bool FACE = true;
+    static constexpr int ncomp(int) { return 1; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo&, double*,
+                                               double (*gr)[2]) {
+    const double s = -prm.c * v[0];  // submit_divergence (:1536)
+    gr[0][0] += s;
+    gr[1][1] += s;
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    const double a = prm.c * 0.5 * (vp[0] + vm[0]);  // :1574-1577
+    flux[0] = a * n[0];
+    flux[1] = a * n[1];
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
+                                                  double* flux) {
+    const double a = prm.c * 0.5 * (vp[0] + vp[0]);  // :1611-1613
+    flux[0] = a * n[0];
+    flux[1] = a * n[1];
+  }
+};
+
+// ------------------------------------------- C (u -> p), optionally D p - C w (Schur)
+struct CParams {
+  double cdt;     // coeff * dt
+  double g1, gg;  // 1/(gamma-1), gamma/(gamma-1)
+};
+
+template <bool WITH_D, int SIGN>
+struct CPhys {
+  static constexpr int NG = WITH_D ? 2 : 1;
+  static constexpr int GW = WITH_D ? 1 : 0;  // group of (w, p_fixed)
+  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = 1;
+  using Params = CParams;
+  static constexpr int out_ncomp(int) { return 1; }
+  static constexpr bool has_val(int) { return WITH_D; }
+  static constexpr bool has_grad(int) { return true; }
+  static constexpr int narr_of(int g) { return g == GW ? 2 : 1; }
+  static constexpr int nf_of(int g) { return g == GW ? 3 : 1; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = G == GW ? 2 : 1;
+    static constexpr bool FACE = G == GW;
+    static constexpr int ncomp(int a) { return (G == GW && a == 0) ? 2 : 1; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo&, double* val,
+                                               double (*gr)[2]) {
+    if constexpr (G == GW) {  // :1444
+      const double s = -SIGN * prm.cdt * prm.gg * v[2];
+      gr[0][0] += s * v[0];
+      gr[0][1] += s * v[1];
+    } else {                  // :1403
+      val[0] += prm.g1 * v[0];
+    }
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    if constexpr (G == GW) {  // :1494-1502
+      const double wnp = vp[0] * n[0] + vp[1] * n[1], wnm = vm[0] * n[0] + vm[1] * n[1];
+      const double lam = fmax(fabs(wnp), fabs(wnm));
+      const double F = prm.cdt * (0.5 * prm.gg * (vp[2] * wnp + vm[2] * wnm) + 0.5 * lam * (prm.g1 * (vp[2] - vm[2])));
+      flux[0] = SIGN * F;
+    }
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
+};
+
+// ---------------------------------------------------------------- mass-type operators
+struct MassParams {
+  double scale;
+};
+
+template <int NC, bool WEIGHTED>
+struct MassPhys {
+  static constexpr int NG = 1;
+  static constexpr bool FACES = false, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = NC;
+  using Params = MassParams;
+  static constexpr int out_ncomp(int) { return NC; }
+  static constexpr bool has_val(int) { return true; }
+  static constexpr bool has_grad(int) { return false; }
+  static constexpr int narr_of(int) { return WEIGHTED ? 2 : 1; }
+  static constexpr int nf_of(int) { return NC + (WEIGHTED ? 1 : 0); }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = WEIGHTED ? 2 : 1;
+    static constexpr bool FACE = false;
+    static constexpr int ncomp(int a) { return a == 0 ? NC : 1; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo&, double* val,
+                                               double (*)[2]) {
+#pragma unroll
+    for (int d = 0; d < NC; ++d) val[d] += (WEIGHTED ? v[NC] : prm.scale) * v[d];
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params&, const double*, const double*, const double*,
+                                              double*) {}
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
+};
+
+}  // namespace af

@@ -164,6 +164,18 @@ def hydrostatic_background(z, theta0=300.0, N=0.01, p0=1.0e5, sc: Scaling = Scal
     return rho / sc.rho_ref, p / sc.p_ref
 
 
+def _harmonics(theta, modes):
+    """cos(k theta), sin(k theta) for k = 1..modes by the angle-addition recurrence."""
+    c1, s1 = np.cos(theta), np.sin(theta)
+    C = np.empty((theta.size, modes), order="F")  # column k contiguous
+    S = np.empty((theta.size, modes), order="F")
+    C[:, 0], S[:, 0] = c1, s1
+    for k in range(1, modes):
+        C[:, k] = C[:, k - 1] * c1 - S[:, k - 1] * s1
+        S[:, k] = S[:, k - 1] * c1 + C[:, k - 1] * s1
+    return C, S
+
+
 def fourier_perturbation(xz, seed, modes=16, amplitude=1e-3, box=None):
     """Smooth seeded field: sum_{k,l<=modes} a_kl/(k^2+l^2) cos(2pi k x^ + phi) cos(pi l z^ + psi),
     a_kl ~ N(0,1), scaled to max |.| = amplitude over the given points."""
@@ -176,12 +188,21 @@ def fourier_perturbation(xz, seed, modes=16, amplitude=1e-3, box=None):
     a = rng.standard_normal((modes, modes))
     ph = rng.uniform(0, 2 * np.pi, (modes, modes))
     ps = rng.uniform(0, 2 * np.pi, (modes, modes))
-    f = np.zeros_like(x)
     k = np.arange(1, modes + 1)
-    cx = [np.cos(2 * np.pi * kk * xh[..., None] + ph[kk - 1][None, :]) for kk in k]
-    for ki, kk in enumerate(k):
-        for li, ll in enumerate(k):
-            f += a[ki, li] / (kk * kk + ll * ll) * cx[ki][..., li] * np.cos(np.pi * ll * zh + ps[ki, li])
+    c = a / (k[:, None] ** 2 + k[None, :] ** 2)
+    # cos(kX + phi) cos(lZ + psi) expanded so the double sum becomes four matrix products;
+    # evaluated in cache-sized chunks of points
+    Mcc, Mcs = c * np.cos(ph) * np.cos(ps), c * np.cos(ph) * np.sin(ps)
+    Msc, Mss = c * np.sin(ph) * np.cos(ps), c * np.sin(ph) * np.sin(ps)
+    xr, zr = xh.reshape(-1), zh.reshape(-1)
+    f = np.empty(xr.size)
+    chunk = 1 << 15
+    for b in range(0, xr.size, chunk):
+        CX, SX = _harmonics(2 * np.pi * xr[b:b + chunk], modes)
+        CZ, SZ = _harmonics(np.pi * zr[b:b + chunk], modes)
+        f[b:b + chunk] = (((CX @ Mcc) * CZ).sum(1) - ((CX @ Mcs) * SZ).sum(1)
+                          - ((SX @ Msc) * CZ).sum(1) + ((SX @ Mss) * SZ).sum(1))
+    f = f.reshape(x.shape)
     m = np.abs(f).max()
     return f * (amplitude / m if m > 0 else 0.0)
 

@@ -1,0 +1,352 @@
+"""Benchmark: GDoF/s of the Euler operator explicit apply (fused stage-1 right-hand side
+triple: density, velocity, pressure) on the 2D terrain-following 512x256 mesh, degree 4, FP64.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-sweep]
+
+One step = one fused apply over the whole mesh with inputs resident in HBM (`value`);
+`e2e` is the same apply through the host-buffer C-ABI call (pinned host inputs copied in,
+all four outputs copied back, every step).  The inputs (7 scalar FP64 fields, 183 MB) and
+outputs (105 MB) exceed the 126 MB L2, so no L2 flush is needed between steps.
+N > 1: one process per GPU (torchrun), independent replicas ("replicas only": the
+operator apply has no cross-GPU exchange in this library), max time over ranks.
+--impl reference: the CPU restatement of the reference operators (the reference itself
+needs deal.II, which is not installable here) on the host cores, same metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NZ, DEGREE, STAGE = 512, 256, 4, 1
+SEED = 20261203
+METRIC = "GDoF/s per Euler operator apply"
+PROFILE = os.path.join(ROOT, "profiles", "rhs_fused_stage1_p4_512x256.md")
+
+
+def workload(P=DEGREE, nx=NX, nz=NZ, modes=16):
+    """Stage-1 sources: rho0, u0, p0 from the seeded 16x16-mode state; rho_tmp_2 and
+    u_fixed from an independent 4x4-mode state (distinct arrays, so nothing aliases)."""
+    from atmospheric_flows_b200 import mesh as M
+    m = M.hill_mesh(nx, nz)
+    st = M.hill_state(m, P, seed=SEED, modes=modes)
+    st2 = M.hill_state(m, P, seed=SEED + 1, modes=4)
+    src = [st.rho, st.u, st.p, st2.rho, st2.u]
+    return m, src
+
+
+def config(P=DEGREE):
+    nd = NX * NZ * (P + 1) ** 2
+    return {
+        "workload": f"EulerOperator explicit apply: stage-1 rhs triple (density+velocity+pressure, one fused "
+                    f"launch) on the 2D terrain-following hill mesh {NX}x{NZ}, degree {P}, QGauss({2 * P + 1}), FP64",
+        "mesh": f"{NX}x{NZ} cells, Witch of Agnesi h0=400 m a=1 km, x in [-20,20] km, top 16 km, walls",
+        "degree": P, "dofs_per_apply": 4 * nd,
+        "inputs": "rho0, u0 (2), p0, rho_tmp_2, u_fixed (2): 7 scalar fields, 183 MB > L2 (no flush needed)",
+        "state": f"hydrostatic background (theta0=300 K, N=0.01/s) + 16x16-mode Fourier perturbation 1e-3, seed {SEED}",
+        "parallelism": "replicas",
+    }
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_numbers():
+    """traffic / executed FP64 flops per launch from the committed ncu summary."""
+    out = {}
+    if os.path.exists(PROFILE):
+        for line in open(PROFILE):
+            for key in ("traffic_bytes_per_launch", "fp64_flops_per_launch"):
+                if line.strip().startswith(key + ":"):
+                    out[key] = float(line.split(":", 1)[1].strip().split()[0])
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_oracle(rows, repeats, threads):
+    """The oracle (CPU restatement) on a horizontal strip of the workload mesh."""
+    from oracle.oracle import OracleOperator, set_num_threads
+    from atmospheric_flows_b200 import mesh as M
+    set_num_threads(threads)
+    m = M.hill_mesh(NX, rows, top=16000.0 * rows / NZ)
+    st = M.hill_state(m, DEGREE, seed=SEED)
+    st2 = M.hill_state(m, DEGREE, seed=SEED + 1)
+    sc = M.Scaling()
+    o = OracleOperator(m, DEGREE, sc.Ma, sc.Fr, 2.0)
+    o.set_HYPERBOLIC_stage(STAGE)
+    src = [st.rho, st.u, st.p, st2.rho, st2.u]
+
+    def one():
+        o.vmult_rhs_rho_update(src[:2])
+        o.vmult_rhs_velocity_fixed(src[:4])
+        o.vmult_rhs_pressure(src)
+
+    one()
+    best = 1e30
+    for _ in range(repeats):
+        t = time.perf_counter()
+        one()
+        best = min(best, time.perf_counter() - t)
+    dofs = 4 * m.n_cells * (DEGREE + 1) ** 2
+    return dofs / best / 1e9, m
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from oracle.oracle import OracleOperator, set_num_threads
+    from atmospheric_flows_b200 import mesh as M
+    set_num_threads(threads)
+    rows = 16
+    m = M.hill_mesh(NX, rows, top=16000.0 * rows / NZ)
+    st = M.hill_state(m, DEGREE, seed=SEED)
+    st2 = M.hill_state(m, DEGREE, seed=SEED + 1)
+    sc = M.Scaling()
+    o = OracleOperator(m, DEGREE, sc.Ma, sc.Fr, 2.0)
+    o.set_HYPERBOLIC_stage(STAGE)
+    src = [st.rho, st.u, st.p, st2.rho, st2.u]
+    for _ in range(args.warmup):
+        o.vmult_rhs_rho_update(src[:2]); o.vmult_rhs_velocity_fixed(src[:4]); o.vmult_rhs_pressure(src)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        o.vmult_rhs_rho_update(src[:2]); o.vmult_rhs_velocity_fixed(src[:4]); o.vmult_rhs_pressure(src)
+    dt = (time.perf_counter() - t) / args.steps
+    dofs = 4 * m.n_cells * (DEGREE + 1) ** 2
+    v = dofs / dt / 1e9
+    sample = f"{NX}x{rows} strip of the {NX}x{NZ} mesh (1/{NZ // rows} of the workload) per step"
+    line = {"metric": METRIC, "value": v, "unit": "GDoF/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(),
+            "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": threads, "kind": "port", "sample": sample,
+                             "note": "CPU restatement of euler_operator.h (oracle/af_oracle.cpp); the reference "
+                                     "needs deal.II >= 9.3 + MPI + p4est, unavailable here"},
+            "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def time_device(op, bufs, src, stream, K, W):
+    import torch
+    for _ in range(W):
+        op.vmult_rhs_fused(*bufs, src)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        op.vmult_rhs_fused(*bufs, src)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / K
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from atmospheric_flows_b200 import mesh as M
+    from atmospheric_flows_b200.operator import EULEROperator, lib
+    import ctypes
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sc = M.Scaling()
+    m, src_h = workload()
+    P = DEGREE
+    ns = m.n_cells * (P + 1) ** 2
+    stream = torch.cuda.Stream(device=dev)
+    op = EULEROperator(m, P, sc.Ma, sc.Fr, 2.0, stream=stream)
+    op.set_HYPERBOLIC_stage(STAGE)
+    src = [torch.from_numpy(a).to(dev) for a in src_h]
+    bufs = [torch.empty(k * ns, dtype=torch.float64, device=dev) for k in (1, 2, 1)]
+
+    # ---- device-resident throughput (value)
+    for _ in range(args.warmup):
+        op.vmult_rhs_fused(*bufs, src)
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = op.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            op.vmult_rhs_fused(*bufs, src)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_total = e0.elapsed_time(e1) * 1e-3
+    launches = op.launch_count() - launches0
+    if world > 1:
+        t = torch.tensor([t_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+    t_step = t_total / args.steps
+    dofs = 4 * ns
+    value = dofs * world / t_step / 1e9
+
+    # ---- end to end through the host-buffer C-ABI call (pinned host memory)
+    src_pin = [torch.from_numpy(a).pin_memory().numpy() for a in src_h]
+    out_pin = [torch.empty(k * ns, dtype=torch.float64).pin_memory().numpy() for k in (1, 2, 1)]
+    for _ in range(max(1, args.warmup // 2)):
+        op.vmult_rhs_fused_host(*out_pin, src_pin)
+    K2 = max(3, min(args.steps, 10))
+    if world > 1:
+        dist.barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(K2):
+        op.vmult_rhs_fused_host(*out_pin, src_pin)
+    e3.record(stream)
+    e3.synchronize()
+    t_e2e = e2.elapsed_time(e3) * 1e-3 / K2
+    if world > 1:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    h2d = sum(a.nbytes for a in src_pin)
+    d2h = sum(a.nbytes for a in out_pin)
+    # parity spot check of the e2e outputs against the device outputs
+    assert np.array_equal(out_pin[2], bufs[2].cpu().numpy())
+
+    # ---- roofline
+    peak, kind = measured_peaks()
+    alg_bytes = 8 * ns * 11  # 7 scalar fields in, 4 out
+    prof = profile_numbers()
+    fp64_peak = ctypes.c_double()
+    lib().af_measure_fp64_peak(ctypes.byref(fp64_peak))
+    roofline = {"bound": "hbm", "achieved": alg_bytes / t_step / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": alg_bytes / t_step / 1e9 / peak, "traffic": prof.get("traffic_bytes_per_launch"),
+                "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "fallback",
+                "alg_bytes_per_launch": alg_bytes}
+    if "fp64_flops_per_launch" in prof:
+        ach = prof["fp64_flops_per_launch"] / t_step / 1e12
+        roofline["fp64"] = {"achieved_tflops": ach, "peak_tflops": fp64_peak.value, "frac": ach / fp64_peak.value,
+                            "flops_per_launch": prof["fp64_flops_per_launch"],
+                            "note": "executed FP64 flops per launch from ncu; peak measured by af_measure_fp64_peak"}
+
+    line = None
+    if rank == 0:
+        # ---- degree sweep (same mesh), device-resident
+        sweep = {}
+        if not args.no_sweep:
+            for Pd in (2, 3, 4, 5, 6):
+                md, sh = workload(Pd, modes=4)
+                nsd = md.n_cells * (Pd + 1) ** 2
+                opd = EULEROperator(md, Pd, sc.Ma, sc.Fr, 2.0, stream=stream)
+                opd.set_HYPERBOLIC_stage(STAGE)
+                sd = [torch.from_numpy(a).to(dev) for a in sh]
+                bd = [torch.empty(k * nsd, dtype=torch.float64, device=dev) for k in (1, 2, 1)]
+                td = time_device(opd, bd, sd, stream, 10, 3)
+                sweep[str(Pd)] = {"gdofs": 4 * nsd / td / 1e9, "us_per_apply": td * 1e6,
+                                  "hbm_frac": 8 * nsd * 11 / td / 1e9 / peak}
+                del opd, sd, bd
+        threads = os.cpu_count() or 1
+        cpu_v, cpu_m = cpu_baseline_oracle(64, 3, threads)
+        line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (hydrostatic background + seeded Fourier perturbation)", "config": config(),
+                "e2e": {"value": dofs * world / t_e2e / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e * 1e3,
+                        "call": "af_vmult_rhs_fused_host (pinned host buffers)"},
+                "roofline": roofline, "gpu_launches": launches,
+                "clocks": clk.summary(),
+                "cpu_baseline": {"value": cpu_v, "unit": "GDoF/s", "cores": threads, "kind": "port",
+                                 "sample": f"{NX}x64 strip of the workload mesh, best of 3 (1/4 of the work)"},
+                "degree_sweep": sweep}
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-sweep", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,131 @@
+/*
+ * af_gpu.h -- C ABI of libaf_gpu.so, the B200 (sm_100a) implementation of the reference's
+ * matrix-free IMEX-DG operator class EULEROperator (euler_operator.h:24-211).
+ *
+ * Every function returns an int status (AF_OK on success).  Vectors are FP64 device
+ * pointers (16-byte aligned) in deal.II's DoF layout for the 2D structured meshes of this
+ * library: cell-major in active-cell order, FE_DGQ(p) Gauss-Lobatto nodes lexicographic
+ * (x fastest), velocity component-blocked inside each cell.  Work is queued on the
+ * handle's CUDA stream; results are visible after af_synchronize or stream ordering.
+ * A handle is not re-entrant (the reference's operator is not either: NS_stage is
+ * mutable and apply_add re-initializes the operator, euler_operator.h:91, 2383-2406).
+ *
+ * Spaces follow the reference's DoFHandler indices (Atmospheric_Flow.cc:334-336):
+ *   0 velocity (2 components), 1 pressure, 2 density.
+ */
+#ifndef AF_GPU_H
+#define AF_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  AF_OK = 0,
+  AF_BAD_ARG = 1,          /* invalid argument, stage or source count            */
+  AF_CUDA = 2,             /* CUDA runtime error (see af_last_error_message)      */
+  AF_NO_CONVERGENCE = 3,   /* SolverControl::NoConvergence of the reference       */
+  AF_NAN = 4,              /* NaN/Inf met in a Krylov recurrence                  */
+  AF_UNSUPPORTED = 5,      /* degree not compiled into this library               */
+  AF_NO_DEVICE = 6         /* no CUDA device available                            */
+};
+
+typedef struct af_operator af_operator;
+
+/* Mesh: nx x nz quadrilateral cells, cell (i, j) -> index j*nx + i, vertices
+ * vertices[(j*(nx+1) + i)*2 + {0,1}] = (x, z) on the HOST.  Bilinear geometry (deal.II
+ * MappingQ1).  Bottom and top are walls; lateral faces are walls or periodic.
+ * gravity 0: e_z with |g| = 1/Fr^2 constant; 1: the reference's radial gravity
+ * e_r |g| a^2/r^2 (euler_operator.h:790-811) with a = radial_a. */
+typedef struct {
+  int nx, nz;
+  int periodic_x;
+  const double* vertices;
+  int gravity;
+  double radial_a;
+} af_mesh_desc;
+
+/* EULEROperator(RunTimeParameters::Data_Storage&) + MatrixFree::reinit
+ * (euler_operator.h:229-240, Atmospheric_Flow.cc:325-348).  n_q_points_1d must be
+ * 2*degree+1 (QGauss(2*degree_u+1), Atmospheric_Flow.cc:345).  The handle creates its
+ * own CUDA stream on the current device. */
+int af_create(const af_mesh_desc* mesh, int degree, int n_q_points_1d, double Mach, double Froude, double dt,
+              af_operator** out);
+int af_destroy(af_operator* op);
+/* Use an external stream (cudaStream_t passed as void*); NULL restores the own stream. */
+int af_set_stream(af_operator* op, void* stream);
+int af_synchronize(af_operator* op);
+
+/* Setters: euler_operator.h:243-303 */
+int af_set_dt(af_operator* op, double dt);
+int af_set_Mach(af_operator* op, double Ma);
+int af_set_Froude(af_operator* op, double Fr);
+int af_set_HYPERBOLIC_stage(af_operator* op, int stage);  /* 1..3 */
+int af_set_NS_stage(af_operator* op, int stage);          /* 1..6 */
+
+/* Deep copies of the fixed-point fields: set_rho_for_fixed / set_pres_fixed /
+ * set_u_fixed, euler_operator.h:306-339.  Device pointers. */
+int af_set_rho_for_fixed(af_operator* op, const double* rho);
+int af_set_pres_fixed(af_operator* op, const double* p);
+int af_set_u_fixed(af_operator* op, const double* u);
+
+/* Explicit right-hand sides, src in the reference's positional order:
+ *  vmult_rhs_rho_update (euler_operator.h:697-712): {rho0,u0 [,rho2,u2 [,rho3,u3]]}
+ *  vmult_rhs_velocity_fixed (:2310-2325): st1 {rho0,u0,p0,rho2}; st2 {rho0,u0,p0,rho2,u2,p2,rho3};
+ *                                          st3 {rho0,u0,p0,rho2,u2,p2,rho3,u3,p3}
+ *  vmult_rhs_pressure (:1366-1381):        st1 {rho0,u0,p0,rho2,u_fixed};
+ *                                          st2 {rho0,u0,p0,rho2,u2,p2,rho3,u_fixed};
+ *                                          st3 {rho0,u0,p0,rho2,u2,p2,rho3,u3,p3,rho_curr,u_curr}
+ * The stage is the HYPERBOLIC_stage set on the handle.  dst is overwritten. */
+int af_vmult_rhs_rho_update(af_operator* op, double* dst, const double* const* src, int n_src);
+int af_vmult_rhs_velocity_fixed(af_operator* op, double* dst, const double* const* src, int n_src);
+int af_vmult_rhs_pressure(af_operator* op, double* dst, const double* const* src, int n_src);
+
+/* The three right-hand sides of one stage in a single fused launch (no counterpart in the
+ * reference, which runs three MatrixFree::loop calls).  src follows the vmult_rhs_pressure
+ * list of the stage; any of dst_rho / dst_u / dst_p may be NULL to skip that equation. */
+int af_vmult_rhs_fused(af_operator* op, double* dst_rho, double* dst_u, double* dst_p, const double* const* src,
+                       int n_src);
+/* Same with HOST buffers: copies in, computes, copies out, synchronizes.  This is the
+ * call a deal.II host-vector caller makes. */
+int af_vmult_rhs_fused_host(af_operator* op, double* dst_rho, double* dst_u, double* dst_p,
+                            const double* const* src, int n_src);
+
+/* MatrixFreeOperators::Base::vmult -> apply_add (euler_operator.h:2362-2417):
+ *  NS 1/4: density mass;  NS 3/5: rho_for_fixed-weighted velocity mass (A);
+ *  NS 6: internal-energy mass D = M/(gamma-1);
+ *  NS 2: Schur complement D p - C A^{-1} B p.  A^{-1} follows af_set_schur_mode. */
+int af_vmult(af_operator* op, double* dst, const double* src);
+/* B: pressure -> velocity space (vmult_pressure, :2422-2435) */
+int af_vmult_pressure(af_operator* op, double* dst, const double* src);
+/* C: velocity -> pressure space (vmult_enthalpy, :2440-2453), uses pres_fixed */
+int af_vmult_enthalpy(af_operator* op, double* dst, const double* src);
+/* compute_diagonal + get_matrix_diagonal_inverse (:2591-2626): writes the inverse
+ * diagonal of the operator selected by NS_stage into dst (its space). */
+int af_compute_diagonal(af_operator* op, double* inv_diag);
+
+/* A^{-1} inside the Schur apply: mode 0 = CG + Jacobi to rel_tol (the reference:
+ * SolverControl(10000, 1e-12 |B p|), euler_operator.h:2391-2397); the defaults are
+ * rel_tol 1e-12 and max_iter 10000. */
+int af_set_schur_mode(af_operator* op, int mode, double rel_tol, int max_iter);
+/* iterations of the last inner A^{-1} solve */
+int af_last_inner_iterations(const af_operator* op, int* its);
+
+/* Number of DoFs of a space (0 velocity, 1 pressure, 2 density): MatrixFree::initialize_dof_vector */
+int af_n_dofs(const af_operator* op, int space, long long* n);
+/* Number of kernels this library launched on the handle since creation. */
+int af_launch_count(const af_operator* op, long long* n);
+
+/* Measures the FP64 FMA throughput of the current device (TFLOP/s) with a short
+ * dependent-chain kernel; the denominator of the FP64 roofline the benchmark reports.
+ * No counterpart in the reference. */
+int af_measure_fp64_peak(double* tflops);
+
+const char* af_error_string(int status);
+const char* af_last_error_message(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AF_GPU_H */
