@@ -62,9 +62,16 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 constexpr int odd(int n) { return n | 1; }
 
+// Unroll factor of the z-pass loop over quadrature-point pairs (see the kernel).
+#ifndef AF_Z_UNROLL
+#define AF_Z_UNROLL 1
+#endif
+constexpr int kZUnroll = AF_Z_UNROLL;
+
 // Cells per CTA and the CTAs-per-SM hint of __launch_bounds__, per degree.  Measured on
 // B200 for the fused stage-1 right-hand side at 512x256 cells, degree 4 (CB, MINB):
-// (16,1) 904 us, (16,2) 574 us, (32,1) 632 us, (8,3) 668 us, (24,1) 682 us.
+// (16,1) 781 us, (16,2) 502 us, (32,1) 529 us, (8,3) 592 us, (8,4) 588 us (z loop not
+// unrolled; fully unrolled: 764 / 521 / 567 / 554 / 550 us).
 template <int P>
 constexpr int cells_per_block() {
   return P <= 1 ? 64 : (P == 2 ? 32 : (P == 3 ? 32 : (P == 4 ? 16 : (P == 5 ? 16 : 8))));
@@ -116,6 +123,17 @@ struct PhysInfo {
     for (int g = 0; g < Phys::NG; ++g) n += Phys::narr_of(g);
     return n;
   }();
+  // cell fields (all groups) evaluated together in the merged z pass
+  static constexpr int NFC_TOTAL = [] {
+    int n = 0;
+    for (int g = 0; g < Phys::NG; ++g) n += Phys::nfc_of(g);
+    return n;
+  }();
+  static constexpr int eo_offset(int G) {
+    int n = 0;
+    for (int g = 0; g < G; ++g) n += Phys::nfc_of(g);
+    return n;
+  }
 };
 
 template <int P, class Phys, int CB_ = cells_per_block<P>()>
@@ -128,17 +146,21 @@ struct Layout {
   static constexpr int P1P = odd(P1);
   static constexpr int EOS = odd(P1 * NQ);
   static constexpr int NF = PhysInfo<Phys>::NFMAX;
+  static constexpr int NFC = PhysInfo<Phys>::NFC_TOTAL;
   static constexpr int NOUT = Phys::NOUT;
+  // region A: x-contracted rows of every cell field, later the z-accumulators
+  static constexpr int R_EO = NFC * CB * EOS;
+  static constexpr int R_ACC = NOUT * 2 * CB * EOS;
+  static constexpr int RA = R_EO > R_ACC ? R_EO : R_ACC;
+  // region B: one group's nodal values and neighbour face nodes, later the outputs
   static constexpr int R_IN = NF * CB * NDP;
   static constexpr int R_NB = Phys::FACES ? 4 * NF * CB * P1P : 0;
-  static constexpr int R_EO = NF * CB * EOS;
-  static constexpr int R_ACC = NOUT * 2 * CB * EOS;
-  static constexpr int R0 = (R_IN + R_NB + R_EO) > R_ACC ? (R_IN + R_NB + R_EO) : R_ACC;
-  static constexpr int R_FLUX = Phys::FACES ? 4 * NOUT * CB * NQ : 0;
   static constexpr int R_OUT = NOUT * CB * NDP;
+  static constexpr int RB = (R_IN + R_NB) > R_OUT ? (R_IN + R_NB) : R_OUT;
+  static constexpr int R_FLUX = Phys::FACES ? 4 * NOUT * CB * NQ : 0;
   static constexpr int R_GEO = CB * 24;  // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb
   static constexpr int R_S = NQ * P1 + NQ;
-  static constexpr int TOTAL = R0 + R_FLUX + R_OUT + R_GEO + R_S;
+  static constexpr int TOTAL = RA + RB + R_FLUX + R_GEO + R_S;
   static constexpr size_t BYTES = sizeof(double) * TOTAL;
 };
 
@@ -186,16 +208,17 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   constexpr int H = T::H;
   constexpr bool MIDN = T::MIDN;
   constexpr int NOUT = Phys::NOUT;
+  constexpr int NFC_ALL = L::NFC;
   const Tab<P>& tb = tab<P>();
 
   extern __shared__ double smem[];
-  double* s_in = smem;
+  double* s_eo = smem;             // region A
+  double* s_acc = smem;            //   (after the z pass)
+  double* s_in = smem + L::RA;     // region B
   double* s_nb = s_in + L::R_IN;
-  double* s_eo = s_nb + L::R_NB;
-  double* s_acc = smem;  // aliases the group buffers after the last group
-  double* s_flux = smem + L::R0;
-  double* s_out = s_flux + L::R_FLUX;
-  double* s_geo = s_out + L::R_OUT;
+  double* s_out = s_in;            //   (after the last group)
+  double* s_flux = smem + L::RA + L::RB;
+  double* s_geo = s_flux + L::R_FLUX;
   double* s_S = s_geo + L::R_GEO;
   double* s_w = s_S + NQ * P1;
 
@@ -218,7 +241,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     g[2] = v3.x - v2.x - v1.x + v0.x; g[3] = v3.y - v2.y - v1.y + v0.y;  // B (bilinear term)
     g[4] = v2.x - v0.x; g[5] = v2.y - v0.y;                        // C = x_eta at xi = 0
     g[6] = v0.x; g[7] = v0.y;
-    // faces: 0 (xi=0, edge v0->v2), 1 (xi=1, v1->v3), 2 (eta=0, v0->v1), 3 (eta=1, v2->v3)
+    // faces: 0 (xi=0, edge v0->v2), 1 (xi=1, v1->v3), 2 (eta=0, v0->v1), 3 (eta=1, v2->v3);
+    // a face's normal is formed from its two vertices the same way by both cells
     double tx, tz, len;
     tx = v2.x - v0.x; tz = v2.y - v0.y; len = sqrt(tx * tx + tz * tz);
     g[8] = -tz / len; g[9] = tx / len; g[10] = len;
@@ -234,64 +258,54 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     int nb3 = j < mesh.nz - 1 ? c + mesh.nx : -1;
     g[20] = (double)nb0; g[21] = (double)nb1; g[22] = (double)nb2; g[23] = (double)nb3;
   }
-
-  // accumulators of the z-contraction (per output, per node row iz):
-  //   a = sum_qz S[qz][iz] (value JxW) + D[qz][iz] (eta-gradient),  b = sum_qz S[qz][iz] (xi-gradient)
-  double acc_a[NOUT][P1], acc_b[NOUT][P1];
-#pragma unroll
-  for (int o = 0; o < NOUT; ++o)
-#pragma unroll
-    for (int i = 0; i < P1; ++i) acc_a[o][i] = acc_b[o][i] = 0.0;
   if (Phys::FACES) {
     for (int k = tid; k < L::R_FLUX; k += NT) s_flux[k] = 0.0;
   }
 
+  // ================= per group: stage, x pass (to region A), face terms =================
   sfor<Phys::NG>([&](auto gc) {
     constexpr int G = decltype(gc)::value;
     using Gi = GroupInfo<Phys, G>;
     using Gr = typename Phys::template Grp<G>;
     constexpr int NF = Gi::NF, NFC = Gi::NF_CELL;
+    constexpr int EOFF = PhysInfo<Phys>::eo_offset(G);
     constexpr bool GFACE = Phys::FACES && Gr::FACE;
 
-    __syncthreads();  // previous group done with the smem buffers
-    // ---- load the group's arrays and the neighbours' face nodes: asynchronous copies,
-    //      all in flight, one wait (own cells: contiguous chunk per array, coalesced)
-    {
-      sfor<Gi::NARR>([&](auto ac) {
-        constexpr int A = decltype(ac)::value;
-        constexpr int NC = Gr::ncomp(A);
-        constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
-        const double* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
-        for (int e = tid; e < ncb * NC * ND; e += NT) {
-          const int cc = e / (NC * ND), r = e % (NC * ND);
-          cp_async8(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
-        }
-      });
-    }
-    // neighbour face nodes (L2-resident), ordered along the face parameter
+    __syncthreads();  // region B free (previous group done) / geometry visible
+    // own cells: contiguous chunk per array, coalesced asynchronous copies
+    sfor<Gi::NARR>([&](auto ac) {
+      constexpr int A = decltype(ac)::value;
+      constexpr int NC = Gr::ncomp(A);
+      constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+      const double* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+      for (int e = tid; e < ncb * NC * ND; e += NT) {
+        const int cc = e / (NC * ND), r = e % (NC * ND);
+        cp_async8(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
+      }
+    });
+    // neighbours' face nodes (L2-resident), ordered along the face parameter;
+    // one element per thread for each (face, field): CB * P1 <= NT for every degree
     if constexpr (GFACE) {
-      constexpr int TOT = 4 * NF * CB * P1;
-      for (int k = tid; k < TOT; k += NT) {
-        const int i = k % P1;
-        const int cc = (k / P1) % CB;
-        const int fi = (k / (P1 * CB)) % NF;
-        const int f = k / (P1 * CB * NF);
-        const int nb = (int)s_geo[cc * 24 + 20 + f];
-        double* dst = &s_nb[((f * NF + fi) * CB + cc) * L::P1P + i];
-        if (nb >= 0 && cc < ncb) {
+      static_assert(CB * P1 <= NT, "neighbour staging assumes one element per thread");
+      const int cc = tid / P1, i = tid % P1;
+      if (tid < CB * P1) {
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          const int nb = (int)s_geo[cc * 24 + 20 + f];
+          const bool ok = nb >= 0 && cc < ncb;
           const int kk = f == 0 ? i * P1 + P : (f == 1 ? i * P1 : (f == 2 ? P * P1 + i : i));
-          int a = 0, comp = fi;
+          sfor<Gi::NARR>([&](auto ac) {
+            constexpr int A = decltype(ac)::value;
+            constexpr int NC = Gr::ncomp(A);
+            constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+            const double* base = ptr.in[Gi::arr_base() + A];
 #pragma unroll
-          for (int aa = 0; aa < Gi::NARR; ++aa)
-            if (a == aa && comp >= Gr::ncomp(aa)) { comp -= Gr::ncomp(aa); ++a; }
-          const int nc = Gr::ncomp(a);
-          const double* base = nullptr;  // select with compile-time indices (no param copy)
-#pragma unroll
-          for (int aa = 0; aa < Gi::NARR; ++aa)
-            if (aa == a) base = ptr.in[Gi::arr_base() + aa];
-          cp_async8(dst, base + (size_t)nb * nc * ND + comp * ND + kk);
-        } else {
-          *dst = 0.0;
+            for (int d = 0; d < NC; ++d) {
+              double* dst = &s_nb[((f * NF + fb + d) * CB + cc) * L::P1P + i];
+              if (ok) cp_async8(dst, base + (size_t)nb * NC * ND + d * ND + kk);
+              else *dst = 0.0;
+            }
+          });
         }
       }
     }
@@ -303,7 +317,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       for (int task = m; task < NFC * NPR; task += NQ) {
         const int fi = task / NPR, k = task % NPR;
         const double* cell = s_in + (fi * CB + cl) * L::NDP;
-        double* eo = s_eo + (fi * CB + cl) * L::EOS;
+        double* eo = s_eo + ((EOFF + fi) * CB + cl) * L::EOS;
         double r[P1], y[NQ];
         if (k < H) {
 #pragma unroll
@@ -325,70 +339,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         }
       }
     }
-    __syncthreads();
-    // ---- Z pass: member = quadrature column qx.  Points are evaluated in mirror pairs
-    //      (qz, NQ-1-qz) from the even/odd rows (read from smem), and each point's
-    //      integrand is contracted into the per-row accumulators right away.
-    if constexpr (NFC > 0) {
-      const int qx = m;
-      const double* g = s_geo + cl * 24;
-      const double xi = tb.x[qx];
-      const double wx = s_w[qx];
-      const double J01 = fma(g[2], xi, g[4]);  // x_eta (x component)
-      const double J11 = fma(g[3], xi, g[5]);  // x_eta (z component)
-      auto point = [&](const double* v, const int qz) {
-        const double eta = tb.x[qz];
-        const double J00 = fma(g[2], eta, g[0]);
-        const double J10 = fma(g[3], eta, g[1]);
-        const double w = wx * tb.w[qz];
-        const double det = J00 * J11 - J01 * J10;
-        PointGeo pg;
-        if (Phys::NEED_X) {
-          pg.X[0] = g[6] + g[0] * xi + g[4] * eta + g[2] * xi * eta;
-          pg.X[1] = g[7] + g[1] * xi + g[5] * eta + g[3] * xi * eta;
-        }
-        double val[NOUT], gr[NOUT][2];
-#pragma unroll
-        for (int o = 0; o < NOUT; ++o) { val[o] = 0.0; gr[o][0] = gr[o][1] = 0.0; }
-        Phys::template point<G>(prm, v, pg, val, gr);
-#pragma unroll
-        for (int o = 0; o < NOUT; ++o) {
-          const bool hv = Phys::has_val(o), hg = Phys::has_grad(o);
-          const double fv = val[o] * det * w;
-          const double fx = (J11 * gr[o][0] - J01 * gr[o][1]) * w;  // adj(J) g, xi row
-          const double fe = (J00 * gr[o][1] - J10 * gr[o][0]) * w;  // adj(J) g, eta row
-#pragma unroll
-          for (int iz = 0; iz < P1; ++iz) {
-            if (hv) acc_a[o][iz] = fma(tb.S[qz][iz], fv, acc_a[o][iz]);
-            if (hg) {
-              acc_a[o][iz] = fma(tb.D[qz][iz], fe, acc_a[o][iz]);
-              acc_b[o][iz] = fma(tb.S[qz][iz], fx, acc_b[o][iz]);
-            }
-          }
-        }
-      };
-#pragma unroll
-      for (int k = 0; k <= P; ++k) {
-        const bool pair = k < P;
-        double v1[NF > 0 ? NF : 1], v2[NF > 0 ? NF : 1];
-#pragma unroll
-        for (int fi = 0; fi < NFC; ++fi) {
-          const double* eo = s_eo + (fi * CB + cl) * L::EOS + qx;
-          double e = 0.0, o = 0.0;
-#pragma unroll
-          for (int i = 0; i < H; ++i) {
-            e = fma(tb.Se[k][i], eo[i * NQ], e);
-            if (pair) o = fma(tb.So[k][i], eo[(H + i) * NQ], o);
-          }
-          if (MIDN) e = fma(tb.Sm[k], eo[(2 * H) * NQ], e);
-          v1[fi] = e + o;
-          v2[fi] = e - o;
-        }
-        point(v1, k);
-        if (pair) point(v2, NQ - 1 - k);
-      }
-    }
-    // ---- faces: member = face quadrature point
+    // ---- faces (same phase: reads region B only): member = face quadrature point
     if constexpr (GFACE) {
       const int q = m;
       double sq[P1];
@@ -426,8 +377,80 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     }
   });
+  __syncthreads();
 
-  __syncthreads();  // all groups done: reuse the group buffers for the accumulators
+  // ================= merged z pass: member = quadrature column qx =================
+  // All groups' fields are evaluated at each point, their integrands summed, and the sum
+  // is mapped to reference coordinates and contracted along z once.
+  double acc_a[NOUT][P1], acc_b[NOUT][P1];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+    for (int i = 0; i < P1; ++i) acc_a[o][i] = acc_b[o][i] = 0.0;
+  {
+    const int qx = m;
+    const double* g = s_geo + cl * 24;
+    const double xi = tb.x[qx];
+    const double wx = s_w[qx];
+    const double J01 = fma(g[2], xi, g[4]);  // x_eta (x component)
+    const double J11 = fma(g[3], xi, g[5]);  // x_eta (z component)
+    auto point = [&](const double* v, const int qz) {
+      const double eta = tb.x[qz];
+      const double J00 = fma(g[2], eta, g[0]);
+      const double J10 = fma(g[3], eta, g[1]);
+      const double w = wx * tb.w[qz];
+      const double dw = (J00 * J11 - J01 * J10) * w;
+      PointGeo pg;
+      if (Phys::NEED_X) {
+        pg.X[0] = g[6] + g[0] * xi + g[4] * eta + g[2] * xi * eta;
+        pg.X[1] = g[7] + g[1] * xi + g[5] * eta + g[3] * xi * eta;
+      }
+      double val[NOUT], gr[NOUT][2];
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) { val[o] = 0.0; gr[o][0] = gr[o][1] = 0.0; }
+      sfor<Phys::NG>([&](auto gc) {
+        constexpr int G = decltype(gc)::value;
+        Phys::template point<G>(prm, v + PhysInfo<Phys>::eo_offset(G), pg, val, gr);
+      });
+      const double a00 = J11 * w, a01 = J01 * w, a10 = J10 * w, a11 = J00 * w;  // adj(J) w
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) {
+        const bool hv = Phys::has_val(o), hg = Phys::has_grad(o);
+        const double fv = val[o] * dw;
+        const double fx = a00 * gr[o][0] - a01 * gr[o][1];
+        const double fe = a11 * gr[o][1] - a10 * gr[o][0];
+#pragma unroll
+        for (int iz = 0; iz < P1; ++iz) {
+          if (hv) acc_a[o][iz] = fma(tb.S[qz][iz], fv, acc_a[o][iz]);
+          if (hg) {
+            acc_a[o][iz] = fma(tb.D[qz][iz], fe, acc_a[o][iz]);
+            acc_b[o][iz] = fma(tb.S[qz][iz], fx, acc_b[o][iz]);
+          }
+        }
+      }
+    };
+#pragma unroll kZUnroll
+    for (int k = 0; k <= P; ++k) {
+      const bool pair = k < P;
+      double v1[NFC_ALL], v2[NFC_ALL];
+#pragma unroll
+      for (int fi = 0; fi < NFC_ALL; ++fi) {
+        const double* eo = s_eo + (fi * CB + cl) * L::EOS + qx;
+        double e = 0.0, o = 0.0;
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+          e = fma(tb.Se[k][i], eo[i * NQ], e);
+          if (pair) o = fma(tb.So[k][i], eo[(H + i) * NQ], o);
+        }
+        if (MIDN) e = fma(tb.Sm[k], eo[(2 * H) * NQ], e);
+        v1[fi] = e + o;
+        v2[fi] = e - o;
+      }
+      point(v1, k);
+      if (pair) point(v2, NQ - 1 - k);
+    }
+  }
+  __syncthreads();  // region A: x-contracted rows consumed -> accumulators
   {
     const int qx = m;
 #pragma unroll
@@ -508,22 +531,18 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   }
   __syncthreads();
   // ---- store (coalesced)
-  {
-    int obase = 0;
-    sfor<Phys::NOUT_ARR>([&](auto oc) {
-      constexpr int OA = decltype(oc)::value;
-      constexpr int NC = Phys::out_ncomp(OA);
-      constexpr int ob = [] { int b = 0; for (int a = 0; a < OA; ++a) b += Phys::out_ncomp(a); return b; }();
-      double* dst = ptr.out[OA] + (size_t)c0 * NC * ND;
-      for (int e = tid; e < ncb * NC * ND; e += NT) {
-        const int cc = e / (NC * ND), r = e % (NC * ND);
-        const double v = s_out[((ob + r / ND) * CB + cc) * L::NDP + r % ND];
-        if (Phys::ACCUMULATE) dst[e] += v;
-        else dst[e] = v;
-      }
-      (void)obase;
-    });
-  }
+  sfor<Phys::NOUT_ARR>([&](auto oc) {
+    constexpr int OA = decltype(oc)::value;
+    constexpr int NC = Phys::out_ncomp(OA);
+    constexpr int ob = [] { int b = 0; for (int a = 0; a < OA; ++a) b += Phys::out_ncomp(a); return b; }();
+    double* dst = ptr.out[OA] + (size_t)c0 * NC * ND;
+    for (int e = tid; e < ncb * NC * ND; e += NT) {
+      const int cc = e / (NC * ND), r = e % (NC * ND);
+      const double v = s_out[((ob + r / ND) * CB + cc) * L::NDP + r % ND];
+      if (Phys::ACCUMULATE) dst[e] += v;
+      else dst[e] = v;
+    }
+  });
 }
 
 template <int P, class Phys, int CB_ = cells_per_block<P>(), int MINB = min_blocks_per_sm<P>()>

@@ -75,6 +75,7 @@ struct RhsPhys {
     if (g < STAGE) return 3 + ((VEL || PRES) ? 1 : 0) + (quirk_group(g) ? 2 : 0);
     return STAGE < 3 ? (1 + (PRES ? 2 : 0)) : 3;
   }
+  static constexpr int nfc_of(int g) { return nf_of(g) - (quirk_group(g) ? 2 : 0); }
 
   template <int G>
   struct Grp {
@@ -212,6 +213,7 @@ struct BPhys {
   static constexpr bool has_grad(int) { return true; }
   static constexpr int narr_of(int) { return 1; }
   static constexpr int nf_of(int) { return 1; }
+  static constexpr int nfc_of(int) { return 1; }
   template <int G>
   struct Grp {
     static constexpr int NARR = 1;
@@ -260,6 +262,7 @@ struct CPhys {
   static constexpr bool has_grad(int) { return true; }
   static constexpr int narr_of(int g) { return g == GW ? 2 : 1; }
   static constexpr int nf_of(int g) { return g == GW ? 3 : 1; }
+  static constexpr int nfc_of(int g) { return nf_of(g); }
   template <int G>
   struct Grp {
     static constexpr int NARR = G == GW ? 2 : 1;
@@ -308,6 +311,7 @@ struct MassPhys {
   static constexpr bool has_grad(int) { return false; }
   static constexpr int narr_of(int) { return WEIGHTED ? 2 : 1; }
   static constexpr int nf_of(int) { return NC + (WEIGHTED ? 1 : 0); }
+  static constexpr int nfc_of(int) { return NC + (WEIGHTED ? 1 : 0); }
   template <int G>
   struct Grp {
     static constexpr int NARR = WEIGHTED ? 2 : 1;
