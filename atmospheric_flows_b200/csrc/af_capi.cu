@@ -513,3 +513,8 @@ int af_launch_count(const af_operator* o, long long* n) {
 }
 
 }  // extern "C"
+
+namespace af {
+// Lets other translation units of the library report through af_last_error_message().
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace af

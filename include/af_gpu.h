@@ -116,6 +116,19 @@ int af_n_dofs(const af_operator* op, int space, long long* n);
 /* Number of kernels this library launched on the handle since creation. */
 int af_launch_count(const af_operator* op, long long* n);
 
+/* The Schur complement apply D p - C A^{-1} B p of af_vmult (NS_stage 2) for callers that
+ * must not allocate device memory (e.g. code inside a framework whose caching allocator owns
+ * the device memory, or a time loop that budgets memory up front).  No counterpart in the
+ * reference.  It needs no handle: the mesh vertices ((nz+1)*(nx+1)*2 doubles), rho_for_fixed,
+ * pres_fixed, src and dst are DEVICE pointers owned by the caller, and all scratch lives in a
+ * static device array of the library (about 7.4 MB per GPU, held until exit) that limits the
+ * problem to nx*nz*(degree+1)^2 <= 65536 pressure DoFs (larger sizes return AF_BAD_ARG).  The
+ * first call on a device sets the array up (cudaGetSymbolAddress, basis tables); calls that
+ * overlap on the GPU share the array and race.  stream may be NULL (default stream). */
+int af_schur_apply_noalloc(int nx, int nz, int periodic_x, const double* vertices, int degree, double Mach, double dt,
+                           int hyperbolic_stage, const double* rho_for_fixed, const double* pres_fixed,
+                           const double* src, double* dst, void* stream, int* inner_iterations);
+
 /* Measures the FP64 FMA throughput of the current device (TFLOP/s) with a short
  * dependent-chain kernel; the denominator of the FP64 roofline the benchmark reports.
  * No counterpart in the reference. */
