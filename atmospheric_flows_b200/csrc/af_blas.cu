@@ -263,3 +263,150 @@ extern "C" int af_measure_fp64_peak(double* tflops) {
   cudaFree(d);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
+
+// ------------------------------------------------------------------ GMRES / IMEX pieces
+namespace af {
+
+// out[j] = V_j . w for j < k (V_j = V + j*ldv); partials per (j, block), fixed order
+__global__ void k_mdot_partial(const double* __restrict__ V, long ldv, const double* __restrict__ w, long n,
+                               double* __restrict__ partial, int nb) {
+  __shared__ double sh[RB];
+  const int j = blockIdx.y;
+  const double* v = V + (long)j * ldv;
+  double s = 0.0;
+  const long stride = (long)gridDim.x * RB;
+  for (long i = (long)blockIdx.x * RB + threadIdx.x; i < n; i += stride) s = fma(v[i], w[i], s);
+  const double b = block_sum(s, sh);
+  if (threadIdx.x == 0) partial[(long)j * nb + blockIdx.x] = b;
+}
+
+__global__ void k_mdot_final(const double* __restrict__ partial, int nb, double* __restrict__ out) {
+  __shared__ double sh[RB];
+  const int j = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nb; i += RB) s += partial[(long)j * nb + i];
+  const double b = block_sum(s, sh);
+  if (threadIdx.x == 0) out[j] = b;
+}
+
+cudaError_t mdot(const double* V, long ldv, int k, const double* w, long n, double* partial, double* out,
+                 cudaStream_t st) {
+  int nb = reduce_blocks(n);
+  if (nb * k > 4 * kMaxPartials) nb = (4 * kMaxPartials) / k;
+  if (nb < 1) nb = 1;
+  k_mdot_partial<<<dim3(nb, k), RB, 0, st>>>(V, ldv, w, n, partial, nb);
+  k_mdot_final<<<k, RB, 0, st>>>(partial, nb, out);
+  return cudaGetLastError();
+}
+
+// w -= sum_{j<k} h[j] V_j  (h on the device)
+__global__ void k_maxpy(const double* __restrict__ V, long ldv, int k, const double* __restrict__ h,
+                        double* __restrict__ w, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < k; ++j) s = fma(h[j], V[(long)j * ldv + i], s);
+  w[i] -= s;
+}
+
+cudaError_t maxpy(const double* V, long ldv, int k, const double* h, double* w, long n, cudaStream_t st) {
+  k_maxpy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(V, ldv, k, h, w, n);
+  return cudaGetLastError();
+}
+
+// x += sum_{j<k} y[j] V_j  (y passed by value, k <= 64)
+struct SmallVec { double v[64]; };
+__global__ void k_mcombine(const double* __restrict__ V, long ldv, int k, const SmallVec y, double* __restrict__ x,
+                           long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < k; ++j) s = fma(y.v[j], V[(long)j * ldv + i], s);
+  x[i] += s;
+}
+
+cudaError_t mcombine(const double* V, long ldv, int k, const double* y_host, double* x, long n, cudaStream_t st) {
+  if (k > 64) return cudaErrorInvalidValue;
+  SmallVec y{};
+  for (int j = 0; j < k; ++j) y.v[j] = y_host[j];
+  k_mcombine<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(V, ldv, k, y, x, n);
+  return cudaGetLastError();
+}
+
+// y = a*x (+ y if add)   and   z = d .* x
+__global__ void k_scale(double a, const double* __restrict__ x, double* __restrict__ y, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * x[i];
+}
+cudaError_t scale(double a, const double* x, double* y, long n, cudaStream_t st) {
+  k_scale<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, x, y, n);
+  return cudaGetLastError();
+}
+__global__ void k_dmul(const double* __restrict__ d, const double* __restrict__ x, double* __restrict__ z, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = d[i] * x[i];
+}
+cudaError_t dmul(const double* d, const double* x, double* z, long n, cudaStream_t st) {
+  k_dmul<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d, x, z, n);
+  return cudaGetLastError();
+}
+// z = x - y
+__global__ void k_sub(const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ z, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = x[i] - y[i];
+}
+cudaError_t sub(const double* x, const double* y, double* z, long n, cudaStream_t st) {
+  k_sub<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, y, z, n);
+  return cudaGetLastError();
+}
+
+// out[0] = max |x| ; out[1] = max |x - y| (y may be null -> only out[0])
+__device__ __forceinline__ double block_max(double v, double* sh) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+#pragma unroll
+  for (int s = RB / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] = fmax(sh[t], sh[t + s]);
+    __syncthreads();
+  }
+  return sh[0];
+}
+__global__ void k_maxabs2_partial(const double* __restrict__ x, const double* __restrict__ y, long n,
+                                  double* __restrict__ partial) {
+  __shared__ double sh[RB];
+  double a = 0.0, b = 0.0;
+  const long stride = (long)gridDim.x * RB;
+  for (long i = (long)blockIdx.x * RB + threadIdx.x; i < n; i += stride) {
+    a = fmax(a, fabs(x[i]));
+    if (y) b = fmax(b, fabs(x[i] - y[i]));
+  }
+  double v = block_max(a, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  __syncthreads();
+  v = block_max(b, sh);
+  if (threadIdx.x == 0) partial[kMaxPartials + blockIdx.x] = v;
+}
+__global__ void k_maxabs2_final(const double* __restrict__ partial, int nb, double* out) {
+  __shared__ double sh[RB];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < nb; i += RB) { a = fmax(a, partial[i]); b = fmax(b, partial[kMaxPartials + i]); }
+  const double ma = block_max(a, sh);
+  __syncthreads();
+  const double mb = block_max(b, sh);
+  if (threadIdx.x == 0) { out[0] = ma; out[1] = mb; }
+}
+cudaError_t maxabs2(const double* x, const double* y, long n, double* partial, double* out, cudaStream_t st) {
+  const int nb = reduce_blocks(n);
+  k_maxabs2_partial<<<nb, RB, 0, st>>>(x, y, n, partial);
+  k_maxabs2_final<<<1, RB, 0, st>>>(partial, nb, out);
+  return cudaGetLastError();
+}
+
+__global__ void k_cg_set_tol(KrylovState* s, const double* bb, double eps) { s->tol2 = eps * eps * bb[0]; }
+cudaError_t cg_set_abs_tol(KrylovState* s, const double* bb, double eps, cudaStream_t st) {
+  k_cg_set_tol<<<1, 1, 0, st>>>(s, bb, eps);
+  return cudaGetLastError();
+}
+
+}  // namespace af

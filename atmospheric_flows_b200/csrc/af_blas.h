@@ -29,4 +29,19 @@ cudaError_t cg_start(KrylovState* s, const double* b, const double* Ax, const do
 cudaError_t cg_after_apply(KrylovState* s, double* x, double* r, double* z, double* p, const double* Ap,
                            const double* invd, long n, double* part, int maxit, cudaStream_t st);
 
+// GMRES / fixed-point helpers
+// out[j] = V_j . w, j < k, V_j = V + j*ldv  (partial needs k * reduce_blocks(n) <= 4*kMaxPartials doubles)
+cudaError_t mdot(const double* V, long ldv, int k, const double* w, long n, double* partial, double* out,
+                 cudaStream_t st);
+cudaError_t maxpy(const double* V, long ldv, int k, const double* h, double* w, long n, cudaStream_t st);  // w -= V h
+cudaError_t mcombine(const double* V, long ldv, int k, const double* y_host, double* x, long n,
+                     cudaStream_t st);  // x += V y
+cudaError_t scale(double a, const double* x, double* y, long n, cudaStream_t st);   // y = a x
+cudaError_t dmul(const double* d, const double* x, double* z, long n, cudaStream_t st);  // z = d .* x
+cudaError_t sub(const double* x, const double* y, double* z, long n, cudaStream_t st);   // z = x - y
+// out[0] = max|x|, out[1] = max|x - y| (0 when y is null); partial needs 2*kMaxPartials doubles
+cudaError_t maxabs2(const double* x, const double* y, long n, double* partial, double* out, cudaStream_t st);
+// state->tol2 = eps^2 * bb[0]  (bb a device scalar, e.g. |b|^2 from dot)
+cudaError_t cg_set_abs_tol(KrylovState* s, const double* bb, double eps, cudaStream_t st);
+
 }  // namespace af

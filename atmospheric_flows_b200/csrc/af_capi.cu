@@ -12,6 +12,7 @@
 
 #include "../../include/af_gpu.h"
 #include "af_blas.h"
+#include "af_handle.h"
 #include "af_internal.h"
 
 namespace af {
@@ -45,40 +46,6 @@ static int fail(int code, const char* fmt, ...) {
     cudaError_t e_ = (call);                                                                          \
     if (e_ != cudaSuccess) return fail(AF_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
-
-struct af_operator {
-  int device = 0;
-  cudaStream_t own_stream = nullptr, stream = nullptr;
-  int P = 0, NQ = 0, ncell = 0, nd = 0;
-  MeshDev mesh{};
-  double2* d_vtx = nullptr;
-  double Ma = 1, Fr = 1, dt = 1;
-  int hs = 1, ns = 1;
-  // IMEX-ARK tableau, euler_operator.h:233-240
-  double gamma, a21, a22, a31, a32, a33, a21t, a22t, a31t, a32t, a33t, b1, b2, b3;
-  double* d_rho_fixed = nullptr;
-  double* d_pres_fixed = nullptr;
-  double* d_u_fixed = nullptr;
-  bool rho_fixed_set = false, pres_fixed_set = false;
-  // workspace: 6 velocity-space vectors (Schur t1, t2; inner CG r, z, p, Ap), reduction
-  // partials, Krylov state
-  double* d_ws = nullptr;
-  double* d_part = nullptr;
-  KrylovState* d_kst = nullptr;
-  double* d_invdA = nullptr;  // inverse diagonal of A for the current rho_for_fixed
-  bool invdA_valid = false;
-  int schur_mode = 0;
-  double schur_tol = 1e-12;
-  int schur_maxit = 10000;
-  int last_inner_its = 0;
-  long long launches = 0;
-  const DegreeOps* ops = nullptr;
-  // host-buffer entry points: device staging
-  double* d_stage = nullptr;
-  size_t stage_len = 0;
-
-  long n_scalar() const { return (long)ncell * nd; }
-};
 
 static void set_tableau(af_operator* o) {
   o->gamma = 2.0 - std::sqrt(2.0);

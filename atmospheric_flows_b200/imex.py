@@ -1,0 +1,90 @@
+"""IMEX-DG time stepping on the GPU (the reference's EulerSolver::run time loop,
+Atmospheric_Flow.cc:1100-1257) over the C ABI of libaf_gpu.so (af_imex_*)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .operator import _MeshDesc, _ptr, check, lib
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("eps", ctypes.c_double), ("max_iterations", ctypes.c_int), ("fixed_point_tol", ctypes.c_double),
+                ("fixed_point_max_iterations", ctypes.c_int), ("gmres_restart", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("fixed_point_iterations", ctypes.c_int * 2), ("gmres_iterations", ctypes.c_longlong),
+                ("cg_iterations", ctypes.c_longlong), ("last_fixed_point_error", ctypes.c_double)]
+
+
+def _bind():
+    L = lib()
+    if getattr(L, "_imex_bound", False):
+        return L
+    vp = ctypes.c_void_p
+    L.af_imex_default_options.argtypes = [ctypes.POINTER(Options)]
+    L.af_imex_create.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.POINTER(Options), ctypes.POINTER(vp)]
+    L.af_imex_destroy.argtypes = [vp]
+    L.af_imex_operator.restype = vp
+    L.af_imex_operator.argtypes = [vp]
+    L.af_imex_set_state.argtypes = [vp, vp, vp, vp]
+    L.af_imex_get_state.argtypes = [vp, vp, vp, vp]
+    L.af_imex_step.argtypes = [vp, ctypes.c_int]
+    L.af_imex_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    L._imex_bound = True
+    return L
+
+
+class IMEXStepper:
+    """GPU time stepper: set_state(rho, u, p) -> step(n) -> get_state()."""
+
+    def __init__(self, mesh, degree, Ma, Fr, dt, eps=None, max_iterations=None, fixed_point_tol=None,
+                 fixed_point_max_iterations=None, gmres_restart=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("IMEXStepper needs a CUDA device (no CPU fallback)")
+        L = _bind()
+        torch.cuda.current_device()
+        opt = Options()
+        check(L.af_imex_default_options(ctypes.byref(opt)))
+        for k, v in (("eps", eps), ("max_iterations", max_iterations), ("fixed_point_tol", fixed_point_tol),
+                     ("fixed_point_max_iterations", fixed_point_max_iterations), ("gmres_restart", gmres_restart)):
+            if v is not None:
+                setattr(opt, k, v)
+        self.mesh, self.degree = mesh, degree
+        self._vtx = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+        desc = _MeshDesc(mesh.nx, mesh.nz, int(mesh.periodic_x), self._vtx.ctypes.data, int(mesh.gravity),
+                         float(mesh.radial_a))
+        h = ctypes.c_void_p()
+        check(L.af_imex_create(ctypes.byref(desc), degree, Ma, Fr, dt, ctypes.byref(opt), ctypes.byref(h)))
+        self._h = h
+        self.n_scalar = mesh.n_cells * (degree + 1) ** 2
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _bind().af_imex_destroy(h)
+            self._h = None
+
+    def set_state(self, rho, u, p):
+        check(_bind().af_imex_set_state(self._h, _ptr(rho), _ptr(u), _ptr(p)))
+
+    def get_state(self):
+        import torch
+        rho = torch.empty(self.n_scalar, dtype=torch.float64, device="cuda")
+        u = torch.empty(2 * self.n_scalar, dtype=torch.float64, device="cuda")
+        p = torch.empty(self.n_scalar, dtype=torch.float64, device="cuda")
+        check(_bind().af_imex_get_state(self._h, _ptr(rho), _ptr(u), _ptr(p)))
+        return rho, u, p
+
+    def step(self, n=1):
+        check(_bind().af_imex_step(self._h, n))
+
+    def stats(self):
+        s = Stats()
+        check(_bind().af_imex_last_stats(self._h, ctypes.byref(s)))
+        return {"fixed_point_iterations": tuple(s.fixed_point_iterations), "gmres_iterations": s.gmres_iterations,
+                "cg_iterations": s.cg_iterations, "last_fixed_point_error": s.last_fixed_point_error}

@@ -116,6 +116,41 @@ int af_n_dofs(const af_operator* op, int space, long long* n);
 /* Number of kernels this library launched on the handle since creation. */
 int af_launch_count(const af_operator* op, long long* n);
 
+/* ---------------------------------------------------------------- IMEX time stepping
+ * One IMEX-DG step of the reference's EulerSolver::run (Atmospheric_Flow.cc:1110-1251):
+ * update_density, the pressure fixed point (pressure_fixed_point + update_velocity, at most
+ * fixed_point_max_iterations, |p - p_old|_inf / (|p|_inf + 1e-10) < fixed_point_tol) for
+ * stages 1 and 2, then update_density, update_velocity and update_pressure for stage 3.
+ * Outer solves stop at eps*|rhs| (SolverControl(max_its, eps*rhs.l2_norm())); the Schur
+ * system uses GMRES with left Jacobi preconditioning restarted after gmres_restart
+ * directions; the inner A^{-1} of pressure_fixed_point stops at 1e-12 |rhs_u|. */
+typedef struct af_imex af_imex;
+typedef struct {
+  double eps;                      /* parameter-file.prm "eps" (default 1e-8)            */
+  int max_iterations;              /* parameter-file.prm "max_iterations" (30000)        */
+  double fixed_point_tol;          /* 1e-10                                               */
+  int fixed_point_max_iterations;  /* 100                                                 */
+  int gmres_restart;               /* 28 (deal.II SolverGMRES default)                     */
+} af_imex_options;
+typedef struct {
+  int fixed_point_iterations[2];   /* stage 1, stage 2 of the last step                   */
+  long long gmres_iterations;      /* summed over the last step                           */
+  long long cg_iterations;
+  double last_fixed_point_error;
+} af_imex_stats;
+int af_imex_default_options(af_imex_options* opt);
+/* Creates its own operator handle (degree p, QGauss(2p+1)) and all stage vectors. */
+int af_imex_create(const af_mesh_desc* mesh, int degree, double Mach, double Froude, double dt,
+                   const af_imex_options* opt, af_imex** out);
+int af_imex_destroy(af_imex* h);
+/* The operator handle used by the stepper (e.g. for af_set_stream). */
+af_operator* af_imex_operator(af_imex* h);
+/* State (rho, u, p) at the start of the next step; DEVICE pointers, copied. */
+int af_imex_set_state(af_imex* h, const double* rho, const double* u, const double* p);
+int af_imex_get_state(const af_imex* h, double* rho, double* u, double* p);
+int af_imex_step(af_imex* h, int nsteps);
+int af_imex_last_stats(const af_imex* h, af_imex_stats* stats);
+
 /* The Schur complement apply D p - C A^{-1} B p of af_vmult (NS_stage 2) for callers that
  * must not allocate device memory (e.g. code inside a framework whose caching allocator owns
  * the device memory, or a time loop that budgets memory up front).  No counterpart in the

@@ -989,6 +989,199 @@ static int vmult(Op<N>& o, N* dst, const N* src) {
   return its;
 }
 
+
+template <typename N>
+static void rhs_rho_fn(const Op<N>& o, std::vector<N>& dst, const std::vector<const N*>& src) {
+  rhs_rho(o, dst.data(), src.data(), (int)src.size());
+}
+
+/* ========================================================================= */
+/* IMEX step: EulerSolver::run (Atmospheric_Flow.cc:1110-1251) restated      */
+/* ========================================================================= */
+struct Imex {
+  double eps = 1e-8, fp_tol = 1e-10;
+  int maxit = 30000, fp_max = 100, restart = 28;
+  std::vector<double> tmp1;  // persistent initial guess of A^{-1} rhs_u (member tmp_1)
+  int fp_iters[2] = {0, 0};
+};
+
+template <typename N>
+static std::vector<N> invdiag_of(Op<N>& o, int ns) {
+  int saved = o.ns_stage;
+  o.ns_stage = ns;
+  long n = o.nscalar() * ((ns == 3 || ns == 5) ? 2 : 1);
+  std::vector<N> d(n);
+  diagonal(o, d.data());
+  o.ns_stage = saved;
+  return d;
+}
+
+// SolverCG with Jacobi, tol = eps*|b|
+template <typename N>
+static int cg_abs(Op<N>& o, int ns, std::vector<N>& x, const std::vector<N>& b, N eps, int maxit) {
+  std::vector<N> invd = invdiag_of(o, ns);
+  int saved = o.ns_stage;
+  o.ns_stage = ns;
+  auto Aop = [&](std::vector<N>& y, const std::vector<N>& v) { vmult(o, y.data(), v.data()); };
+  auto jac = [&](std::vector<N>& z, const std::vector<N>& r) { for (size_t i = 0; i < r.size(); ++i) z[i] = invd[i] * r[i]; };
+  int its = pcg<N>(Aop, jac, x, b, eps * std::sqrt(vdot(b, b)), maxit);
+  o.ns_stage = saved;
+  return its;
+}
+
+// SolverGMRES, left preconditioning, restart m, modified Gram-Schmidt, tol on |P^{-1} r|
+template <typename N, typename A, typename Pc>
+static int gmres_left(A&& apply, Pc&& prec, std::vector<N>& x, const std::vector<N>& b, N tol, int m, int maxit) {
+  size_t n = b.size();
+  std::vector<std::vector<N>> V(m + 1, std::vector<N>(n));
+  std::vector<N> w(n), t(n);
+  std::vector<N> H((m + 1) * m), cs(m), sn(m), g(m + 1);
+  int total = 0;
+  while (true) {
+    apply(t, x);
+    for (size_t i = 0; i < n; ++i) t[i] = b[i] - t[i];
+    prec(w, t);
+    N beta = std::sqrt(vdot(w, w));
+    if (beta <= tol) return total;
+    if (total >= maxit) return -1;
+    for (size_t i = 0; i < n; ++i) V[0][i] = w[i] / beta;
+    std::fill(g.begin(), g.end(), (N)0);
+    g[0] = beta;
+    int k = 0;
+    N res = beta;
+    for (int j = 0; j < m; ++j) {
+      apply(t, V[j]);
+      prec(w, t);
+      for (int i = 0; i <= j; ++i) {
+        N hij = vdot(V[i], w);
+        H[i * m + j] = hij;
+        for (size_t l = 0; l < n; ++l) w[l] -= hij * V[i][l];
+      }
+      N hn = std::sqrt(vdot(w, w));
+      H[(j + 1) * m + j] = hn;
+      if (hn > 0) for (size_t l = 0; l < n; ++l) V[j + 1][l] = w[l] / hn;
+      for (int i = 0; i < j; ++i) {
+        N a = cs[i] * H[i * m + j] + sn[i] * H[(i + 1) * m + j];
+        H[(i + 1) * m + j] = -sn[i] * H[i * m + j] + cs[i] * H[(i + 1) * m + j];
+        H[i * m + j] = a;
+      }
+      N a = H[j * m + j], c = H[(j + 1) * m + j];
+      N r = std::sqrt(a * a + c * c);
+      cs[j] = r > 0 ? a / r : 1;
+      sn[j] = r > 0 ? c / r : 0;
+      H[j * m + j] = r;
+      H[(j + 1) * m + j] = 0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      res = std::fabs(g[j + 1]);
+      ++total;
+      k = j + 1;
+      if (res <= tol || total >= maxit || hn == 0) break;
+    }
+    std::vector<N> y(k);
+    for (int i = k - 1; i >= 0; --i) {
+      N sum = g[i];
+      for (int l = i + 1; l < k; ++l) sum -= H[i * m + l] * y[l];
+      y[i] = sum / H[i * m + i];
+    }
+    for (int i = 0; i < k; ++i)
+      for (size_t l = 0; l < n; ++l) x[l] += y[i] * V[i][l];
+    if (res <= tol) return total;
+    if (total >= maxit) return -1;
+  }
+}
+
+template <typename N>
+static N linf(const std::vector<N>& v) {
+  N m = 0;
+  for (auto a : v) m = std::max(m, (N)std::fabs(a));
+  return m;
+}
+
+template <typename N>
+static void imex_step(Op<N>& o, Imex& im, std::vector<N>& rho0, std::vector<N>& u0, std::vector<N>& p0) {
+  const long ns = o.nscalar();
+  std::vector<N> rho2(ns), rho3(ns), rhoc(ns), u2(2 * ns), u3(2 * ns), uc(2 * ns), ufix(2 * ns);
+  std::vector<N> p2(ns), p3(ns), pfix(ns), pfix_old(ns), rhs_rho(ns), rhs_p(ns), rhs_u(2 * ns), tmp(2 * ns);
+  if ((long)im.tmp1.size() != 2 * ns) im.tmp1.assign(2 * ns, (N)0);
+  auto density = [&](int stage, std::vector<N>& x, const std::vector<N>& x0) {
+    o.hyperbolic_stage = stage;
+    std::vector<const N*> src = {rho0.data(), u0.data()};
+    if (stage >= 2) { src.push_back(rho2.data()); src.push_back(u2.data()); }
+    if (stage >= 3) { src.push_back(rho3.data()); src.push_back(u3.data()); }
+    rhs_rho_fn(o, rhs_rho, src);
+    x = x0;
+    cg_abs(o, 1, x, rhs_rho, (N)im.eps, im.maxit);
+  };
+  auto fixed_point = [&](int stage, std::vector<N>& p_out, std::vector<N>& u_out) {
+    int it = 0;
+    for (; it < im.fp_max; ++it) {
+      o.hyperbolic_stage = stage;
+      o.pres_fixed = pfix_old;
+      o.u_fixed = ufix;
+      std::vector<const N*> sp, su;
+      if (stage == 1) {
+        sp = {rho0.data(), u0.data(), p0.data(), rho2.data(), ufix.data()};
+        su = {rho0.data(), u0.data(), p0.data(), rho2.data()};
+      } else {
+        sp = {rho0.data(), u0.data(), p0.data(), rho2.data(), u2.data(), p2.data(), rho3.data(), ufix.data()};
+        su = {rho0.data(), u0.data(), p0.data(), rho2.data(), u2.data(), p2.data(), rho3.data()};
+      }
+      rhs_pressure(o, rhs_p.data(), sp.data(), (int)sp.size());
+      rhs_velocity(o, rhs_u.data(), su.data(), (int)su.size());
+      cg_abs(o, 3, im.tmp1, rhs_u, (N)1e-12, im.maxit);
+      std::vector<N> t2(ns);
+      apply_C(o, t2.data(), im.tmp1.data());
+      for (long i = 0; i < ns; ++i) rhs_p[i] -= t2[i];
+      pfix = pfix_old;
+      std::vector<N> invd = invdiag_of(o, 2);
+      o.ns_stage = 2;
+      auto S = [&](std::vector<N>& y, const std::vector<N>& v) { vmult(o, y.data(), v.data()); };
+      auto jac = [&](std::vector<N>& z, const std::vector<N>& r) { for (size_t i = 0; i < r.size(); ++i) z[i] = invd[i] * r[i]; };
+      gmres_left<N>(S, jac, pfix, rhs_p, (N)im.eps * std::sqrt(vdot(rhs_p, rhs_p)), im.restart, im.maxit);
+      // update_velocity
+      apply_B(o, tmp.data(), pfix.data());
+      for (long i = 0; i < 2 * ns; ++i) rhs_u[i] -= tmp[i];
+      cg_abs(o, 3, ufix, rhs_u, (N)im.eps, im.maxit);
+      std::vector<N> d(ns);
+      for (long i = 0; i < ns; ++i) d[i] = pfix[i] - pfix_old[i];
+      N err = linf(d) / (linf(pfix) + (N)1e-10);
+      if (err < (N)im.fp_tol) { ++it; break; }
+      pfix_old = pfix;
+    }
+    im.fp_iters[stage - 1] = it;
+    p_out = pfix;
+    u_out = ufix;
+  };
+  density(1, rho2, rho0);
+  o.rho_for_fixed = rho2;
+  pfix_old = p0;
+  ufix = u0;
+  fixed_point(1, p2, u2);
+  density(2, rho3, rho2);
+  o.rho_for_fixed = rho3;
+  pfix_old = p2;
+  ufix = u2;
+  fixed_point(2, p3, u3);
+  density(3, rhoc, rho3);
+  o.rho_for_fixed = rhoc;
+  o.hyperbolic_stage = 3;
+  {
+    std::vector<const N*> su = {rho0.data(), u0.data(), p0.data(), rho2.data(), u2.data(), p2.data(), rho3.data(),
+                                u3.data(), p3.data()};
+    rhs_velocity(o, rhs_u.data(), su.data(), 9);
+    uc = u3;
+    cg_abs(o, 5, uc, rhs_u, (N)im.eps, im.maxit);
+    std::vector<const N*> sp = {rho0.data(), u0.data(), p0.data(), rho2.data(), u2.data(), p2.data(), rho3.data(),
+                                u3.data(), p3.data(), rhoc.data(), uc.data()};
+    rhs_pressure(o, rhs_p.data(), sp.data(), 11);
+    p0 = p3;
+    cg_abs(o, 6, p0, rhs_p, (N)im.eps, im.maxit);
+  }
+  rho0 = rhoc;
+  u0 = uc;
+}
+
 }  // namespace orc
 
 /* ========================================================================= */
@@ -1164,3 +1357,24 @@ void orc_tables(int P, int NQ, double* nodes, double* qp, double* qw, double* S,
 }
 
 }  // extern "C"
+
+extern "C" {
+/* nsteps IMEX steps on (rho, u, p) in place (double instance only); fp_iters receives the
+   fixed-point iteration counts of stages 1 and 2 of the last step. */
+int orc_imex_steps(void* h, double* rho, double* u, double* p, int nsteps, double eps, int maxit, double fp_tol,
+                   int fp_max, int restart, int* fp_iters) {
+  OrcHandle* H = (OrcHandle*)h;
+  if (H->ld) return -1;
+  Op<double>& o = *H->d;
+  long ns = o.nscalar();
+  std::vector<double> r(rho, rho + ns), uu(u, u + 2 * ns), pp(p, p + ns);
+  Imex im;
+  im.eps = eps; im.maxit = maxit; im.fp_tol = fp_tol; im.fp_max = fp_max; im.restart = restart;
+  for (int k = 0; k < nsteps; ++k) imex_step(o, im, r, uu, pp);
+  std::copy(r.begin(), r.end(), rho);
+  std::copy(uu.begin(), uu.end(), u);
+  std::copy(pp.begin(), pp.end(), p);
+  if (fp_iters) { fp_iters[0] = im.fp_iters[0]; fp_iters[1] = im.fp_iters[1]; }
+  return 0;
+}
+}
