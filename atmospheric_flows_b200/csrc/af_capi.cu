@@ -164,6 +164,8 @@ int af_destroy(af_operator* o) {
   cudaFree(o->d_part);
   cudaFree(o->d_kst);
   cudaFree(o->d_stage);
+  cudaFree(o->d_Lm);
+  cudaFree(o->d_La);
   if (o->own_stream) cudaStreamDestroy(o->own_stream);
   delete o;
   return AF_OK;
@@ -215,7 +217,7 @@ static int copy_fixed(af_operator* o, double* dst, const double* src, long n) {
 }
 int af_set_rho_for_fixed(af_operator* o, const double* v) {
   int r = copy_fixed(o, o ? o->d_rho_fixed : nullptr, v, o ? o->n_scalar() : 0);
-  if (r == AF_OK) { o->rho_fixed_set = true; o->invdA_valid = false; }
+  if (r == AF_OK) { o->rho_fixed_set = true; o->invdA_valid = false; o->La_valid = false; }
   return r;
 }
 int af_set_pres_fixed(af_operator* o, const double* v) {
@@ -404,6 +406,33 @@ static int solve_A(af_operator* o, double* x, const double* b) {
   return AF_OK;
 }
 
+// Packed Cholesky factors of the cell mass matrices (built on first use)
+static int ensure_factor(af_operator* o, bool weighted) {
+  double** L = weighted ? &o->d_La : &o->d_Lm;
+  bool* valid = weighted ? &o->La_valid : &o->Lm_valid;
+  if (*valid) return AF_OK;
+  if (weighted && !o->rho_fixed_set) return fail(AF_BAD_ARG, "set_rho_for_fixed first");
+  if (!*L) AF_CU(cudaMalloc(L, sizeof(double) * (size_t)o->ncell * o->ops->factor_len));
+  AF_CU(o->ops->mass_factor(o->mesh, weighted ? o->d_rho_fixed : nullptr, *L, o->ncell, o->stream));
+  o->launches += 1;
+  *valid = true;
+  return AF_OK;
+}
+
+int af_vmult_inverse(af_operator* o, double* dst, const double* src) {
+  if (!o || !dst || !src) return fail(AF_BAD_ARG, "null argument");
+  const int ns = o->ns;
+  if (ns == 2) return fail(AF_BAD_ARG, "af_vmult_inverse: NS_stage 2 (Schur complement) has no cell-wise inverse");
+  AF_CU(cudaSetDevice(o->device));
+  const bool weighted = (ns == 3 || ns == 5);
+  int r = ensure_factor(o, weighted);
+  if (r != AF_OK) return r;
+  const double scale = ns == 6 ? (1.4 - 1.0) : 1.0;  // D = M/(gamma-1)
+  AF_CU(o->ops->mass_solve(weighted ? o->d_La : o->d_Lm, weighted ? 2 : 1, src, scale, dst, o->ncell, o->stream));
+  o->launches += 1;
+  return AF_OK;
+}
+
 int af_vmult(af_operator* o, double* dst, const double* src) {
   if (!o || !dst || !src) return fail(AF_BAD_ARG, "null argument");
   if (!aligned16(dst) || !aligned16(src)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
@@ -432,8 +461,17 @@ int af_vmult(af_operator* o, double* dst, const double* src) {
   double* t2 = o->d_ws + n;
   AF_CU(o->ops->op_B(o->mesh, src, coeff_BC(o) * o->dt / (o->Ma * o->Ma), t1, o->ncell, o->stream));
   o->launches += 1;
-  int r = solve_A(o, t2, t1);
-  if (r != AF_OK) return r;
+  int r;
+  if (o->schur_mode == 1) {  // exact cell-wise A^{-1}
+    r = ensure_factor(o, true);
+    if (r != AF_OK) return r;
+    AF_CU(o->ops->mass_solve(o->d_La, 2, t1, 1.0, t2, o->ncell, o->stream));
+    o->launches += 1;
+    o->last_inner_its = 0;
+  } else {
+    r = solve_A(o, t2, t1);
+    if (r != AF_OK) return r;
+  }
   AF_CU(o->ops->op_C(o->mesh, t2, o->d_pres_fixed, src, c_params(o), dst, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -454,7 +492,8 @@ int af_compute_diagonal(af_operator* o, double* inv_diag) {
 }
 
 int af_set_schur_mode(af_operator* o, int mode, double rel_tol, int max_iter) {
-  if (!o || mode != 0 || !(rel_tol > 0) || max_iter < 1) return fail(AF_BAD_ARG, "af_set_schur_mode: bad argument");
+  if (!o || mode < 0 || mode > 1 || !(rel_tol > 0) || max_iter < 1)
+    return fail(AF_BAD_ARG, "af_set_schur_mode: bad argument");
   o->schur_mode = mode;
   o->schur_tol = rel_tol;
   o->schur_maxit = max_iter;

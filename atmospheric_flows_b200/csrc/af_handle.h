@@ -37,6 +37,10 @@ struct af_operator {
   int last_inner_its = 0;
   long long launches = 0;
   const DegreeOps* ops = nullptr;
+  // exact cell-wise inverses: packed Cholesky factors of M (fixed) and of A (rho_for_fixed)
+  double* d_Lm = nullptr;
+  double* d_La = nullptr;
+  bool Lm_valid = false, La_valid = false;
   // host-buffer entry points: device staging
   double* d_stage = nullptr;
   size_t stage_len = 0;

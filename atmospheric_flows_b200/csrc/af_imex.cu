@@ -188,6 +188,14 @@ static double l2norm(af_imex* h, const double* x, long n) {
   return std::sqrt(v);
 }
 
+// Mass-type system of the current NS_stage: exact cell-wise inverse or CG + Jacobi to eps
+static int mass_solve(af_imex* h, const double* invd, double* x, const double* b, long n, double eps) {
+  af_operator* o = h->op;
+  if (h->opt.mass_solver == 1) return af_vmult_inverse(o, x, b);
+  Apply M = [o](const double* in, double* out) { return af_vmult(o, out, in); };
+  return cg_solve(h, M, invd, x, b, n, eps, nullptr);
+}
+
 // ------------------------------------------------------------------ stage drivers
 static int update_density(af_imex* h, int stage) {
   af_operator* o = h->op;
@@ -211,8 +219,7 @@ static int update_density(af_imex* h, int stage) {
     x = h->rhoc;
     IM_CU(cudaMemcpyAsync(x, h->rho3, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
   }
-  Apply M = [o](const double* in, double* out) { return af_vmult(o, out, in); };
-  return cg_solve(h, M, h->invd_M, x, h->rhs_rho, ns, h->opt.eps, nullptr);
+  return mass_solve(h, h->invd_M, x, h->rhs_rho, ns, h->opt.eps);
 }
 
 static int pressure_fixed_point(af_imex* h, int stage) {
@@ -233,8 +240,7 @@ static int pressure_fixed_point(af_imex* h, int stage) {
   }
   // tmp_1 = A^{-1} rhs_u, CG to 1e-12 |rhs_u| (Atmospheric_Flow.cc:571, 642); tmp_1 persists
   IM_AF(af_set_NS_stage(o, 3));
-  Apply Aop = [o](const double* in, double* out) { return af_vmult(o, out, in); };
-  IM_AF(cg_solve(h, Aop, h->invd_u, h->tmp1, h->rhs_u, 2 * ns, 1e-12, nullptr));
+  IM_AF(mass_solve(h, h->invd_u, h->tmp1, h->rhs_u, 2 * ns, 1e-12));
   IM_AF(af_vmult_enthalpy(o, h->tmpp, h->tmp1));
   IM_CU(axpby(-1.0, h->tmpp, 1.0, h->rhs_p, ns, o->stream));
   o->launches += 1;
@@ -263,8 +269,7 @@ static int update_velocity(af_imex* h, int stage) {
     x = h->uc;
     IM_CU(cudaMemcpyAsync(x, h->u3, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
   }
-  Apply Aop = [o](const double* in, double* out) { return af_vmult(o, out, in); };
-  return cg_solve(h, Aop, h->invd_u, x, h->rhs_u, 2 * ns, h->opt.eps, nullptr);
+  return mass_solve(h, h->invd_u, x, h->rhs_u, 2 * ns, h->opt.eps);
 }
 
 static int update_pressure(af_imex* h) {
@@ -274,8 +279,7 @@ static int update_pressure(af_imex* h) {
   const double* sp[] = {h->rho0, h->u0, h->p0, h->rho2, h->u2, h->p2, h->rho3, h->u3, h->p3, h->rhoc, h->uc};
   IM_AF(af_vmult_rhs_pressure(o, h->rhs_p, sp, 11));
   IM_CU(cudaMemcpyAsync(h->p0, h->p3, ns * 8, cudaMemcpyDeviceToDevice, o->stream));  // pres_old = pres_tmp_3
-  Apply D = [o](const double* in, double* out) { return af_vmult(o, out, in); };
-  return cg_solve(h, D, h->invd_D, h->p0, h->rhs_p, ns, h->opt.eps, nullptr);
+  return mass_solve(h, h->invd_D, h->p0, h->rhs_p, ns, h->opt.eps);
 }
 
 static int set_rho_for_fixed(af_imex* h, const double* rho) {
@@ -347,6 +351,8 @@ int af_imex_default_options(af_imex_options* opt) {
   opt->fixed_point_tol = 1e-10;       // Atmospheric_Flow.cc:1149
   opt->fixed_point_max_iterations = 100;  // :1135
   opt->gmres_restart = 28;            // deal.II SolverGMRES default (30 temporary vectors)
+  opt->mass_solver = 1;
+  opt->schur_inner = 1;
   return AF_OK;
 }
 
@@ -358,7 +364,8 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   af_imex_default_options(&o);
   if (opt) o = *opt;
   if (!(o.eps > 0) || o.max_iterations < 1 || o.gmres_restart < 1 || o.gmres_restart > 60 ||
-      o.fixed_point_max_iterations < 1)
+      o.fixed_point_max_iterations < 1 || o.mass_solver < 0 || o.mass_solver > 1 || o.schur_inner < 0 ||
+      o.schur_inner > 1)
     return ierr(AF_BAD_ARG, "af_imex_create: bad options");
   auto* h = new af_imex();
   h->opt = o;
@@ -369,6 +376,7 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   const int m = o.gmres_restart;
   // scalar vectors: rho0 rho2 rho3 rhoc p0 p2 p3 pfix pfix_old rhs_rho rhs_p tmpp invd_M invd_D gw = 15
   // velocity vectors (2 ns): u0 u2 u3 uc ufix rhs_u tmp1 tmpu cg_r cg_z cg_p cg_Ap invd_u = 13
+  r = AF_OK;
   const long total = 15 * ns + 13 * 2 * ns + (long)(m + 1) * ns + 2 * (m + 1) + 8 + 4 * kMaxPartials + 16;
   if (cudaMalloc(&h->mem, total * sizeof(double)) != cudaSuccess) {
     af_destroy(h->op);
@@ -394,9 +402,10 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   h->scal = take(8);
   h->part = take(4 * kMaxPartials);
   h->kst = reinterpret_cast<KrylovState*>(take(16));
+  r = af_set_schur_mode(h->op, o.schur_inner, 1e-12, 10000);
   // fixed inverse diagonals of M and D (compute_diagonal, NS 1 and NS 2/6)
-  af_set_NS_stage(h->op, 1);
-  r = af_compute_diagonal(h->op, h->invd_M);
+  if (r == AF_OK) r = af_set_NS_stage(h->op, 1);
+  if (r == AF_OK) r = af_compute_diagonal(h->op, h->invd_M);
   if (r == AF_OK) { af_set_NS_stage(h->op, 6); r = af_compute_diagonal(h->op, h->invd_D); }
   if (r == AF_OK) r = af_synchronize(h->op);
   if (r != AF_OK) { af_imex_destroy(h); return r; }

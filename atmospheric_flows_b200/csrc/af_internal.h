@@ -37,7 +37,14 @@ struct DegreeOps {
   // inverse of the diagonal of scale*M (weight null) or of M_rho (ncomp copies)
   cudaError_t (*inv_diag)(const MeshDev&, int ncomp, const double* weight, double scale, double* dst, int ncell,
                           cudaStream_t);
+  // packed Cholesky factors of the cell mass matrices (weight null: plain mass), stored
+  // interleaved L[k * ncell + c], factor_len() doubles per cell
+  cudaError_t (*mass_factor)(const MeshDev&, const double* weight, double* L, int ncell, cudaStream_t);
+  // x = scale * M^{-1} b (block diagonal, exact), ncomp components per cell
+  cudaError_t (*mass_solve)(const double* L, int ncomp, const double* b, double scale, double* x, int ncell,
+                            cudaStream_t);
   int cells_per_block;
+  int factor_len;  // (p+1)^2 ((p+1)^2 + 1) / 2
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

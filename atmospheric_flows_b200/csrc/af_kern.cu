@@ -185,7 +185,168 @@ cudaError_t inv_diag(const MeshDev& mesh, int ncomp, const double* weight, doubl
   return cudaGetLastError();
 }
 
-const DegreeOps kOps = {upload_tables, rhs, mass, op_B, op_C, inv_diag, cells_per_block<P>()};
+// ---------------------------------------------------------------- exact cell inverse
+// Cell mass matrix  M_K[I][J] = sum_q w(q) JxW(q) phi_I(q) phi_J(q)  (w = 1 or a density),
+// assembled by sum factorisation and factored by Cholesky, one thread per cell.  The packed
+// lower factor (row-major, reciprocal diagonal) is stored interleaved, L[k * ncell + c], so
+// that the solve kernel reads it coalesced.  Per-thread work arrays live in shared memory,
+// interleaved by thread (conflict-free).
+constexpr int kND = (P + 1) * (P + 1);
+constexpr int kNPK = kND * (kND + 1) / 2;
+constexpr int kFactorThreads = P <= 2 ? 64 : (P <= 4 ? 32 : 16);
+
+__global__ void __launch_bounds__(kFactorThreads)
+    k_mass_factor(const MeshDev mesh, const double* __restrict__ weight, double* __restrict__ Lg, const int ncell) {
+  using T = Tab<P>;
+  constexpr int P1 = T::P1, NQ = T::NQ, ND = kND, NPK = kNPK, NTH = kFactorThreads;
+  extern __shared__ double sm[];
+  const int t = threadIdx.x;
+  const int c = blockIdx.x * NTH + t;
+  double* A = sm;                  // [NPK][NTH]
+  double* F = sm + NPK * NTH;      // [NQ*NQ][NTH]
+  const Tab<P>& tb = c_tab;
+  const bool valid = c < ncell;
+  const int cc = valid ? c : ncell - 1;
+  const int i = cc % mesh.nx, j = cc / mesh.nx, W = mesh.nx + 1;
+  const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
+  const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
+  const double Ax = v1.x - v0.x, Az = v1.y - v0.y, Cx = v2.x - v0.x, Cz = v2.y - v0.y;
+  const double Bx = v3.x - v2.x - v1.x + v0.x, Bz = v3.y - v2.y - v1.y + v0.y;
+  // f(q) = w(q) JxW(q)
+  for (int qx = 0; qx < NQ; ++qx) {
+    double tx[P1];
+    if (weight) {
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) {
+        double s = 0.0;
+#pragma unroll
+        for (int ix = 0; ix < P1; ++ix) s = fma(tb.S[qx][ix], weight[(size_t)cc * ND + iz * P1 + ix], s);
+        tx[iz] = s;
+      }
+    }
+    const double xi = tb.x[qx];
+    const double J01 = fma(Bx, xi, Cx), J11 = fma(Bz, xi, Cz);
+    for (int qz = 0; qz < NQ; ++qz) {
+      const double eta = tb.x[qz];
+      const double J00 = fma(Bx, eta, Ax), J10 = fma(Bz, eta, Az);
+      double f = (J00 * J11 - J01 * J10) * tb.w[qx] * tb.w[qz];
+      if (weight) {
+        double wv = 0.0;
+#pragma unroll
+        for (int iz = 0; iz < P1; ++iz) wv = fma(tb.S[qz][iz], tx[iz], wv);
+        f *= wv;
+      }
+      F[(qz * NQ + qx) * NTH + t] = f;
+    }
+  }
+  for (int k = 0; k < NPK; ++k) A[k * NTH + t] = 0.0;
+  // A[I][J] += S[qz][iz] S[qz][jz] * T[ix][jx],  T[ix][jx] = sum_qx S[qx][ix] S[qx][jx] f(qz, qx)
+  for (int qz = 0; qz < NQ; ++qz) {
+    double Tm[P1][P1];
+#pragma unroll
+    for (int ix = 0; ix < P1; ++ix)
+#pragma unroll
+      for (int jx = 0; jx <= ix; ++jx) {
+        double s = 0.0;
+        for (int qx = 0; qx < NQ; ++qx) s = fma(tb.S[qx][ix] * tb.S[qx][jx], F[(qz * NQ + qx) * NTH + t], s);
+        Tm[ix][jx] = s;
+        Tm[jx][ix] = s;
+      }
+    for (int I = 0; I < ND; ++I) {
+      const int iz = I / P1, ix = I % P1;
+      const double si = tb.S[qz][iz];
+      for (int J = 0; J <= I; ++J) {
+        const int jz = J / P1, jx = J % P1;
+        A[(I * (I + 1) / 2 + J) * NTH + t] += si * tb.S[qz][jz] * Tm[ix][jx];
+      }
+    }
+  }
+  // Cholesky, packed row-major lower; the diagonal stores 1/L_jj
+  for (int jj = 0; jj < ND; ++jj) {
+    double d = A[(jj * (jj + 1) / 2 + jj) * NTH + t];
+    for (int k = 0; k < jj; ++k) {
+      const double l = A[(jj * (jj + 1) / 2 + k) * NTH + t];
+      d -= l * l;
+    }
+    const double inv = 1.0 / sqrt(d);
+    A[(jj * (jj + 1) / 2 + jj) * NTH + t] = inv;
+    for (int ii = jj + 1; ii < ND; ++ii) {
+      double a = A[(ii * (ii + 1) / 2 + jj) * NTH + t];
+      for (int k = 0; k < jj; ++k) a -= A[(ii * (ii + 1) / 2 + k) * NTH + t] * A[(jj * (jj + 1) / 2 + k) * NTH + t];
+      A[(ii * (ii + 1) / 2 + jj) * NTH + t] = a * inv;
+    }
+  }
+  if (valid)
+    for (int k = 0; k < NPK; ++k) Lg[(size_t)k * ncell + c] = A[k * NTH + t];
+}
+
+// x = scale * M_K^{-1} b per cell and component (one thread per cell and component; the
+// working vector lives in shared memory, interleaved by thread)
+constexpr int kSolveThreads = 128;
+__global__ void __launch_bounds__(kSolveThreads)
+    k_mass_solve(const double* __restrict__ Lg, const double* __restrict__ b, double* __restrict__ x,
+                 const double scale, const int ncomp, const int ncell) {
+  constexpr int ND = kND, NTH = kSolveThreads;
+  extern __shared__ double ys[];  // [ND][NTH]
+  const int t = threadIdx.x;
+  const int gid = blockIdx.x * NTH + t;
+  if (gid >= ncell * ncomp) return;
+  const int c = gid % ncell, d = gid / ncell;
+  const double* bb = b + ((size_t)c * ncomp + d) * ND;
+  for (int k = 0; k < ND; ++k) ys[k * NTH + t] = bb[k];
+  // forward: L y = b, rows of the packed factor read in storage order
+  const double* Lp = Lg + c;
+  for (int ii = 0; ii < ND; ++ii) {
+    double a = ys[ii * NTH + t];
+    for (int k = 0; k < ii; ++k) {
+      a -= *Lp * ys[k * NTH + t];
+      Lp += ncell;
+    }
+    ys[ii * NTH + t] = a * *Lp;  // reciprocal diagonal
+    Lp += ncell;
+  }
+  // backward: L^T x = y, row by row from the last (x overwrites y)
+  for (int ii = ND - 1; ii >= 0; --ii) {
+    const double* Lr = Lg + (size_t)(ii * (ii + 1) / 2) * ncell + c;
+    const double xi = ys[ii * NTH + t] * Lr[(size_t)ii * ncell];
+    ys[ii * NTH + t] = xi;
+    for (int k = 0; k < ii; ++k) {
+      ys[k * NTH + t] -= *Lr * xi;
+      Lr += ncell;
+    }
+  }
+  double* xx = x + ((size_t)c * ncomp + d) * ND;
+  for (int k = 0; k < ND; ++k) xx[k] = scale * ys[k * NTH + t];
+}
+
+cudaError_t mass_factor(const MeshDev& mesh, const double* weight, double* L, int ncell, cudaStream_t st) {
+  const size_t bytes = sizeof(double) * (size_t)(kNPK + (2 * P + 1) * (2 * P + 1)) * kFactorThreads;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_mass_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  k_mass_factor<<<(ncell + kFactorThreads - 1) / kFactorThreads, kFactorThreads, bytes, st>>>(mesh, weight, L, ncell);
+  return cudaGetLastError();
+}
+
+cudaError_t mass_solve(const double* L, int ncomp, const double* b, double scale, double* x, int ncell,
+                       cudaStream_t st) {
+  const int n = ncell * ncomp;
+  const size_t bytes = sizeof(double) * kND * kSolveThreads;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_mass_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  k_mass_solve<<<(n + kSolveThreads - 1) / kSolveThreads, kSolveThreads, bytes, st>>>(L, b, x, scale, ncomp, ncell);
+  return cudaGetLastError();
+}
+
+const DegreeOps kOps = {upload_tables, rhs, mass, op_B, op_C, inv_diag, mass_factor, mass_solve,
+                        cells_per_block<P>(), kNPK};
 
 }  // namespace
 

@@ -11,7 +11,8 @@ from .operator import _MeshDesc, _ptr, check, lib
 
 class Options(ctypes.Structure):
     _fields_ = [("eps", ctypes.c_double), ("max_iterations", ctypes.c_int), ("fixed_point_tol", ctypes.c_double),
-                ("fixed_point_max_iterations", ctypes.c_int), ("gmres_restart", ctypes.c_int)]
+                ("fixed_point_max_iterations", ctypes.c_int), ("gmres_restart", ctypes.c_int),
+                ("mass_solver", ctypes.c_int), ("schur_inner", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -42,7 +43,7 @@ class IMEXStepper:
     """GPU time stepper: set_state(rho, u, p) -> step(n) -> get_state()."""
 
     def __init__(self, mesh, degree, Ma, Fr, dt, eps=None, max_iterations=None, fixed_point_tol=None,
-                 fixed_point_max_iterations=None, gmres_restart=None):
+                 fixed_point_max_iterations=None, gmres_restart=None, mass_solver=None, schur_inner=None):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("IMEXStepper needs a CUDA device (no CPU fallback)")
@@ -51,7 +52,8 @@ class IMEXStepper:
         opt = Options()
         check(L.af_imex_default_options(ctypes.byref(opt)))
         for k, v in (("eps", eps), ("max_iterations", max_iterations), ("fixed_point_tol", fixed_point_tol),
-                     ("fixed_point_max_iterations", fixed_point_max_iterations), ("gmres_restart", gmres_restart)):
+                     ("fixed_point_max_iterations", fixed_point_max_iterations), ("gmres_restart", gmres_restart),
+                     ("mass_solver", mass_solver), ("schur_inner", schur_inner)):
             if v is not None:
                 setattr(opt, k, v)
         self.mesh, self.degree = mesh, degree

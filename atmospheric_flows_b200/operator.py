@@ -49,7 +49,7 @@ def lib():
             getattr(L, name).argtypes = [vp, dp, ctypes.POINTER(dp), ip]
         L.af_vmult_rhs_fused.argtypes = [vp, dp, dp, dp, ctypes.POINTER(dp), ip]
         L.af_vmult_rhs_fused_host.argtypes = [vp, dp, dp, dp, ctypes.POINTER(dp), ip]
-        for name in ("af_vmult", "af_vmult_pressure", "af_vmult_enthalpy"):
+        for name in ("af_vmult", "af_vmult_pressure", "af_vmult_enthalpy", "af_vmult_inverse"):
             getattr(L, name).argtypes = [vp, dp, dp]
         L.af_compute_diagonal.argtypes = [vp, dp]
         L.af_set_schur_mode.argtypes = [vp, ip, ctypes.c_double, ip]
@@ -184,6 +184,10 @@ class EULEROperator:
     # --- implicit operators ---
     def vmult(self, dst, src):
         check(lib().af_vmult(self._h, _ptr(dst), _ptr(src)))
+
+    def vmult_inverse(self, dst, src):
+        """Exact inverse of the block-diagonal mass-type operator of the current NS_stage."""
+        check(lib().af_vmult_inverse(self._h, _ptr(dst), _ptr(src)))
 
     def vmult_pressure(self, dst, src):
         check(lib().af_vmult_pressure(self._h, _ptr(dst), _ptr(src)))

@@ -138,3 +138,36 @@ def test_implicit_parity(P, name):
         g.vmult(dst, _d(p))
         assert g.last_inner_iterations() > 0
         assert rel(_h(dst), o.vmult(p)) < 1e-10
+
+
+@pytest.mark.parametrize("P", [1, 2, 4, 6])
+def test_exact_inverse_and_schur_mode(P):
+    """af_vmult_inverse inverts the mass-type operators to rounding (checked against the
+    oracle's forward operators), and the Schur apply with the exact cell-wise A^{-1} agrees
+    with the reference's nested-CG form."""
+    m, g, o, states = _setup("hill", P)
+    ns = m.n_cells * (P + 1) ** 2
+    rng = np.random.default_rng(11)
+    for op in (g, o):
+        op.set_rho_for_fixed(_d(states[0].rho) if op is g else states[0].rho)
+        op.set_pres_fixed(_d(states[1].p) if op is g else states[1].p)
+    for ns_stage, n in ((1, ns), (6, ns), (3, 2 * ns), (5, 2 * ns)):
+        o.set_NS_stage(ns_stage)
+        g.set_NS_stage(ns_stage)
+        x = rng.standard_normal(n)
+        b = o.vmult(x)
+        dst = torch.zeros(n, dtype=torch.float64, device="cuda")
+        g.vmult_inverse(dst, _d(b))
+        assert rel(_h(dst), x) < 1e-11, ns_stage
+    for hs in (1, 2):
+        g.set_HYPERBOLIC_stage(hs)
+        o.set_HYPERBOLIC_stage(hs)
+        g.set_NS_stage(2)
+        o.set_NS_stage(2)
+        g.set_schur_mode(1)
+        p = states[2].p
+        dst = torch.zeros(ns, dtype=torch.float64, device="cuda")
+        g.vmult(dst, _d(p))
+        assert g.last_inner_iterations() == 0
+        assert rel(_h(dst), o.vmult(p)) < 1e-10
+        g.set_schur_mode(0)
