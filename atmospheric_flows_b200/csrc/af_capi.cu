@@ -406,7 +406,7 @@ static int solve_A(af_operator* o, double* x, const double* b) {
   return AF_OK;
 }
 
-// Packed Cholesky factors of the cell mass matrices (built on first use)
+// Packed inverses of the cell mass matrices (built on first use)
 static int ensure_factor(af_operator* o, bool weighted) {
   double** L = weighted ? &o->d_La : &o->d_Lm;
   bool* valid = weighted ? &o->La_valid : &o->Lm_valid;

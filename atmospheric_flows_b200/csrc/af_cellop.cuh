@@ -50,13 +50,31 @@ __device__ __forceinline__ void sfor(F&& f) {
   sfor_impl<N>(f, std::make_integer_sequence<int, N>{});
 }
 
+// 1D tables of degree P in precision R; each kernel translation unit defines the
+// specialisations it uses (constant memory is per module).
+template <int P, class R>
+__device__ __forceinline__ const TabT<P, R>& tabr();
 template <int P>
-__device__ __forceinline__ const Tab<P>& tab();
+__device__ __forceinline__ const Tab<P>& tab() {
+  return tabr<P, double>();
+}
+
+// Fused multiply-add in the working precision (no silent promotion of float operands).
+__device__ __forceinline__ double fmaR(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fmaR(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// Working precision of a Phys policy: Phys::real.
+template <class Phys>
+using RealOf = typename Phys::real;
 
 // Asynchronous global -> shared copies (all of a group in flight, one wait).
-__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+__device__ __forceinline__ void cp_async_el(double* smem_dst, const double* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_el(float* smem_dst, const float* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
@@ -81,10 +99,10 @@ constexpr int min_blocks_per_sm() {
   return P == 3 ? 1 : 2;
 }
 
-template <int MAXARR, int MAXOUT>
+template <int MAXARR, int MAXOUT, class R = double>
 struct ArgPtrs {
-  const double* in[MAXARR];
-  double* out[MAXOUT];
+  const R* in[MAXARR];
+  R* out[MAXOUT];
 };
 
 // ----------------------------------------------------------------------------------
@@ -138,7 +156,8 @@ struct PhysInfo {
 
 template <int P, class Phys, int CB_ = cells_per_block<P>()>
 struct Layout {
-  using T = Tab<P>;
+  using R = RealOf<Phys>;
+  using T = TabT<P, R>;
   static constexpr int P1 = T::P1, NQ = T::NQ, ND = P1 * P1;
   static constexpr int CB = CB_;
   static constexpr int NT = CB * NQ;
@@ -161,37 +180,37 @@ struct Layout {
   static constexpr int R_GEO = CB * 24;  // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb
   static constexpr int R_S = NQ * P1 + NQ;
   static constexpr int TOTAL = RA + RB + R_FLUX + R_GEO + R_S;
-  static constexpr size_t BYTES = sizeof(double) * TOTAL;
+  static constexpr size_t BYTES = sizeof(R) * TOTAL;
 };
 
 // even/odd contraction of a P1-vector r along one direction to NQ values
-template <int P>
-__device__ __forceinline__ void contract_eo(const double* r, double* y) {
-  using T = Tab<P>;
-  const Tab<P>& t = tab<P>();
-  double re[T::H > 0 ? T::H : 1], ro[T::H > 0 ? T::H : 1];
+template <int P, class R>
+__device__ __forceinline__ void contract_eo(const R* r, R* y) {
+  using T = TabT<P, R>;
+  const T& t = tabr<P, R>();
+  R re[T::H > 0 ? T::H : 1], ro[T::H > 0 ? T::H : 1];
 #pragma unroll
   for (int i = 0; i < T::H; ++i) {
     re[i] = r[i] + r[P - i];
     ro[i] = r[i] - r[P - i];
   }
-  const double rm = T::MIDN ? r[P / 2] : 0.0;
+  const R rm = T::MIDN ? r[P / 2] : 0.0;
 #pragma unroll
   for (int k = 0; k < P; ++k) {
-    double e = 0.0, o = 0.0;
+    R e = 0.0, o = 0.0;
 #pragma unroll
     for (int i = 0; i < T::H; ++i) {
-      e = fma(t.Se[k][i], re[i], e);
-      o = fma(t.So[k][i], ro[i], o);
+      e = fmaR(t.Se[k][i], re[i], e);
+      o = fmaR(t.So[k][i], ro[i], o);
     }
-    if (T::MIDN) e = fma(t.Sm[k], rm, e);
+    if (T::MIDN) e = fmaR(t.Sm[k], rm, e);
     y[k] = e + o;
     y[T::NQ - 1 - k] = e - o;
   }
-  double e = 0.0;
+  R e = 0.0;
 #pragma unroll
-  for (int i = 0; i < T::H; ++i) e = fma(t.Se[P][i], re[i], e);
-  if (T::MIDN) e = fma(t.Sm[P], rm, e);
+  for (int i = 0; i < T::H; ++i) e = fmaR(t.Se[P][i], re[i], e);
+  if (T::MIDN) e = fmaR(t.Sm[P], rm, e);
   y[P] = e;
 }
 
@@ -200,27 +219,29 @@ __device__ __forceinline__ void contract_eo(const double* r, double* y) {
 // ----------------------------------------------------------------------------------
 template <int P, class Phys, int CB_ = cells_per_block<P>(), int MINB = min_blocks_per_sm<P>()>
 __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
-    k_cellop(const MeshDev mesh, const ArgPtrs<PhysInfo<Phys>::NARR_TOTAL, Phys::NOUT_ARR> ptr,
+    k_cellop(const MeshDev mesh, const ArgPtrs<PhysInfo<Phys>::NARR_TOTAL, Phys::NOUT_ARR, RealOf<Phys>> ptr,
              const typename Phys::Params prm, const int ncell) {
   using L = Layout<P, Phys, CB_>;
-  using T = Tab<P>;
+  using R = RealOf<Phys>;
+  using T = TabT<P, R>;
   constexpr int P1 = L::P1, NQ = L::NQ, ND = L::ND, CB = L::CB, NT = L::NT;
   constexpr int H = T::H;
   constexpr bool MIDN = T::MIDN;
   constexpr int NOUT = Phys::NOUT;
   constexpr int NFC_ALL = L::NFC;
-  const Tab<P>& tb = tab<P>();
+  const T& tb = tabr<P, R>();
 
-  extern __shared__ double smem[];
-  double* s_eo = smem;             // region A
-  double* s_acc = smem;            //   (after the z pass)
-  double* s_in = smem + L::RA;     // region B
-  double* s_nb = s_in + L::R_IN;
-  double* s_out = s_in;            //   (after the last group)
-  double* s_flux = smem + L::RA + L::RB;
-  double* s_geo = s_flux + L::R_FLUX;
-  double* s_S = s_geo + L::R_GEO;
-  double* s_w = s_S + NQ * P1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* smem = reinterpret_cast<R*>(smem_raw);
+  R* s_eo = smem;             // region A
+  R* s_acc = smem;            //   (after the z pass)
+  R* s_in = smem + L::RA;     // region B
+  R* s_nb = s_in + L::R_IN;
+  R* s_out = s_in;            //   (after the last group)
+  R* s_flux = smem + L::RA + L::RB;
+  R* s_geo = s_flux + L::R_FLUX;
+  R* s_S = s_geo + L::R_GEO;
+  R* s_w = s_S + NQ * P1;
 
   const int tid = threadIdx.x;
   const int m = tid / CB;   // member: row / column / face point
@@ -236,7 +257,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     const int i = c % mesh.nx, j = c / mesh.nx, W = mesh.nx + 1;
     const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
     const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
-    double* g = s_geo + cl * 24;
+    R* g = s_geo + cl * 24;
     g[0] = v1.x - v0.x; g[1] = v1.y - v0.y;                        // A = x_xi at eta = 0
     g[2] = v3.x - v2.x - v1.x + v0.x; g[3] = v3.y - v2.y - v1.y + v0.y;  // B (bilinear term)
     g[4] = v2.x - v0.x; g[5] = v2.y - v0.y;                        // C = x_eta at xi = 0
@@ -256,7 +277,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     int nb1 = i < mesh.nx - 1 ? c + 1 : (mesh.periodic_x ? c - mesh.nx + 1 : -1);
     int nb2 = j > 0 ? c - mesh.nx : -1;
     int nb3 = j < mesh.nz - 1 ? c + mesh.nx : -1;
-    g[20] = (double)nb0; g[21] = (double)nb1; g[22] = (double)nb2; g[23] = (double)nb3;
+    g[20] = (R)nb0; g[21] = (R)nb1; g[22] = (R)nb2; g[23] = (R)nb3;
   }
   if (Phys::FACES) {
     for (int k = tid; k < L::R_FLUX; k += NT) s_flux[k] = 0.0;
@@ -277,10 +298,10 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       constexpr int A = decltype(ac)::value;
       constexpr int NC = Gr::ncomp(A);
       constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
-      const double* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+      const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
       for (int e = tid; e < ncb * NC * ND; e += NT) {
         const int cc = e / (NC * ND), r = e % (NC * ND);
-        cp_async8(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
+        cp_async_el(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
       }
     });
     // neighbours' face nodes (L2-resident), ordered along the face parameter;
@@ -298,11 +319,11 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
             constexpr int A = decltype(ac)::value;
             constexpr int NC = Gr::ncomp(A);
             constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
-            const double* base = ptr.in[Gi::arr_base() + A];
+            const R* base = ptr.in[Gi::arr_base() + A];
 #pragma unroll
             for (int d = 0; d < NC; ++d) {
-              double* dst = &s_nb[((f * NF + fb + d) * CB + cc) * L::P1P + i];
-              if (ok) cp_async8(dst, base + (size_t)nb * NC * ND + d * ND + kk);
+              R* dst = &s_nb[((f * NF + fb + d) * CB + cc) * L::P1P + i];
+              if (ok) cp_async_el(dst, base + (size_t)nb * NC * ND + d * ND + kk);
               else *dst = 0.0;
             }
           });
@@ -316,9 +337,9 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       constexpr int NPR = H + (MIDN ? 1 : 0);
       for (int task = m; task < NFC * NPR; task += NQ) {
         const int fi = task / NPR, k = task % NPR;
-        const double* cell = s_in + (fi * CB + cl) * L::NDP;
-        double* eo = s_eo + ((EOFF + fi) * CB + cl) * L::EOS;
-        double r[P1], y[NQ];
+        const R* cell = s_in + (fi * CB + cl) * L::NDP;
+        R* eo = s_eo + ((EOFF + fi) * CB + cl) * L::EOS;
+        R r[P1], y[NQ];
         if (k < H) {
 #pragma unroll
           for (int ix = 0; ix < P1; ++ix) r[ix] = cell[k * P1 + ix] + cell[(P - k) * P1 + ix];
@@ -342,32 +363,32 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     // ---- faces (same phase: reads region B only): member = face quadrature point
     if constexpr (GFACE) {
       const int q = m;
-      double sq[P1];
+      R sq[P1];
 #pragma unroll
       for (int i = 0; i < P1; ++i) sq[i] = s_S[q * P1 + i];
-      const double wq = s_w[q];
-      const double* g = s_geo + cl * 24;
+      const R wq = s_w[q];
+      const R* g = s_geo + cl * 24;
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
         const int nb = (int)g[20 + f];
-        double vp[NF], vm[NF];
+        R vp[NF], vm[NF];
 #pragma unroll
         for (int fi = 0; fi < NF; ++fi) {
-          const double* cell = s_in + (fi * CB + cl) * L::NDP;
-          const double* nbv = s_nb + ((f * NF + fi) * CB + cl) * L::P1P;
-          double a = 0.0, b = 0.0;
+          const R* cell = s_in + (fi * CB + cl) * L::NDP;
+          const R* nbv = s_nb + ((f * NF + fi) * CB + cl) * L::P1P;
+          R a = 0.0, b = 0.0;
 #pragma unroll
           for (int i = 0; i < P1; ++i) {
             const int kk = f == 0 ? i * P1 : (f == 1 ? i * P1 + P : (f == 2 ? i : P * P1 + i));
-            a = fma(sq[i], cell[kk], a);
-            b = fma(sq[i], nbv[i], b);
+            a = fmaR(sq[i], cell[kk], a);
+            b = fmaR(sq[i], nbv[i], b);
           }
           vp[fi] = a;
           vm[fi] = b;
         }
-        const double n[2] = {g[8 + 3 * f], g[9 + 3 * f]};
-        const double jxw = g[10 + 3 * f] * wq;
-        double flux[NOUT];
+        const R n[2] = {g[8 + 3 * f], g[9 + 3 * f]};
+        const R jxw = g[10 + 3 * f] * wq;
+        R flux[NOUT];
 #pragma unroll
         for (int o = 0; o < NOUT; ++o) flux[o] = 0.0;
         if (nb >= 0) Phys::template face<G>(prm, vp, vm, n, flux);
@@ -382,49 +403,49 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   // ================= merged z pass: member = quadrature column qx =================
   // All groups' fields are evaluated at each point, their integrands summed, and the sum
   // is mapped to reference coordinates and contracted along z once.
-  double acc_a[NOUT][P1], acc_b[NOUT][P1];
+  R acc_a[NOUT][P1], acc_b[NOUT][P1];
 #pragma unroll
   for (int o = 0; o < NOUT; ++o)
 #pragma unroll
     for (int i = 0; i < P1; ++i) acc_a[o][i] = acc_b[o][i] = 0.0;
   {
     const int qx = m;
-    const double* g = s_geo + cl * 24;
-    const double xi = tb.x[qx];
-    const double wx = s_w[qx];
-    const double J01 = fma(g[2], xi, g[4]);  // x_eta (x component)
-    const double J11 = fma(g[3], xi, g[5]);  // x_eta (z component)
-    auto point = [&](const double* v, const int qz) {
-      const double eta = tb.x[qz];
-      const double J00 = fma(g[2], eta, g[0]);
-      const double J10 = fma(g[3], eta, g[1]);
-      const double w = wx * tb.w[qz];
-      const double dw = (J00 * J11 - J01 * J10) * w;
+    const R* g = s_geo + cl * 24;
+    const R xi = tb.x[qx];
+    const R wx = s_w[qx];
+    const R J01 = fmaR(g[2], xi, g[4]);  // x_eta (x component)
+    const R J11 = fmaR(g[3], xi, g[5]);  // x_eta (z component)
+    auto point = [&](const R* v, const int qz) {
+      const R eta = tb.x[qz];
+      const R J00 = fmaR(g[2], eta, g[0]);
+      const R J10 = fmaR(g[3], eta, g[1]);
+      const R w = wx * tb.w[qz];
+      const R dw = (J00 * J11 - J01 * J10) * w;
       PointGeo pg;
       if (Phys::NEED_X) {
         pg.X[0] = g[6] + g[0] * xi + g[4] * eta + g[2] * xi * eta;
         pg.X[1] = g[7] + g[1] * xi + g[5] * eta + g[3] * xi * eta;
       }
-      double val[NOUT], gr[NOUT][2];
+      R val[NOUT], gr[NOUT][2];
 #pragma unroll
       for (int o = 0; o < NOUT; ++o) { val[o] = 0.0; gr[o][0] = gr[o][1] = 0.0; }
       sfor<Phys::NG>([&](auto gc) {
         constexpr int G = decltype(gc)::value;
         Phys::template point<G>(prm, v + PhysInfo<Phys>::eo_offset(G), pg, val, gr);
       });
-      const double a00 = J11 * w, a01 = J01 * w, a10 = J10 * w, a11 = J00 * w;  // adj(J) w
+      const R a00 = J11 * w, a01 = J01 * w, a10 = J10 * w, a11 = J00 * w;  // adj(J) w
 #pragma unroll
       for (int o = 0; o < NOUT; ++o) {
         const bool hv = Phys::has_val(o), hg = Phys::has_grad(o);
-        const double fv = val[o] * dw;
-        const double fx = a00 * gr[o][0] - a01 * gr[o][1];
-        const double fe = a11 * gr[o][1] - a10 * gr[o][0];
+        const R fv = val[o] * dw;
+        const R fx = a00 * gr[o][0] - a01 * gr[o][1];
+        const R fe = a11 * gr[o][1] - a10 * gr[o][0];
 #pragma unroll
         for (int iz = 0; iz < P1; ++iz) {
-          if (hv) acc_a[o][iz] = fma(tb.S[qz][iz], fv, acc_a[o][iz]);
+          if (hv) acc_a[o][iz] = fmaR(tb.S[qz][iz], fv, acc_a[o][iz]);
           if (hg) {
-            acc_a[o][iz] = fma(tb.D[qz][iz], fe, acc_a[o][iz]);
-            acc_b[o][iz] = fma(tb.S[qz][iz], fx, acc_b[o][iz]);
+            acc_a[o][iz] = fmaR(tb.D[qz][iz], fe, acc_a[o][iz]);
+            acc_b[o][iz] = fmaR(tb.S[qz][iz], fx, acc_b[o][iz]);
           }
         }
       }
@@ -432,17 +453,17 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
 #pragma unroll kZUnroll
     for (int k = 0; k <= P; ++k) {
       const bool pair = k < P;
-      double v1[NFC_ALL], v2[NFC_ALL];
+      R v1[NFC_ALL], v2[NFC_ALL];
 #pragma unroll
       for (int fi = 0; fi < NFC_ALL; ++fi) {
-        const double* eo = s_eo + (fi * CB + cl) * L::EOS + qx;
-        double e = 0.0, o = 0.0;
+        const R* eo = s_eo + (fi * CB + cl) * L::EOS + qx;
+        R e = 0.0, o = 0.0;
 #pragma unroll
         for (int i = 0; i < H; ++i) {
-          e = fma(tb.Se[k][i], eo[i * NQ], e);
-          if (pair) o = fma(tb.So[k][i], eo[(H + i) * NQ], o);
+          e = fmaR(tb.Se[k][i], eo[i * NQ], e);
+          if (pair) o = fmaR(tb.So[k][i], eo[(H + i) * NQ], o);
         }
-        if (MIDN) e = fma(tb.Sm[k], eo[(2 * H) * NQ], e);
+        if (MIDN) e = fmaR(tb.Sm[k], eo[(2 * H) * NQ], e);
         v1[fi] = e + o;
         v2[fi] = e - o;
       }
@@ -455,8 +476,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     const int qx = m;
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
-      double* A = s_acc + ((o * 2 + 0) * CB + cl) * L::EOS;
-      double* B = s_acc + ((o * 2 + 1) * CB + cl) * L::EOS;
+      R* A = s_acc + ((o * 2 + 0) * CB + cl) * L::EOS;
+      R* B = s_acc + ((o * 2 + 1) * CB + cl) * L::EOS;
 #pragma unroll
       for (int iz = 0; iz < P1; ++iz) {
         A[iz * NQ + qx] = acc_a[o][iz];
@@ -468,34 +489,34 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   // ---- XT pass: task (output, row iz) -> P1 outputs, plus face terms on face nodes
   for (int task = m; task < NOUT * P1; task += NQ) {
     const int o = task / P1, iz = task % P1;
-    const double* A = s_acc + ((o * 2 + 0) * CB + cl) * L::EOS + iz * NQ;
-    const double* B = s_acc + ((o * 2 + 1) * CB + cl) * L::EOS + iz * NQ;
-    double oE[H > 0 ? H : 1], oO[H > 0 ? H : 1], oM = 0.0;
+    const R* A = s_acc + ((o * 2 + 0) * CB + cl) * L::EOS + iz * NQ;
+    const R* B = s_acc + ((o * 2 + 1) * CB + cl) * L::EOS + iz * NQ;
+    R oE[H > 0 ? H : 1], oO[H > 0 ? H : 1], oM = 0.0;
 #pragma unroll
     for (int i = 0; i < H; ++i) oE[i] = oO[i] = 0.0;
 #pragma unroll
     for (int k = 0; k < P; ++k) {
-      const double a1 = A[k], a2 = A[NQ - 1 - k], b1 = B[k], b2 = B[NQ - 1 - k];
-      const double As = a1 + a2, Ad = a1 - a2, Bs = b1 + b2, Bd = b1 - b2;
+      const R a1 = A[k], a2 = A[NQ - 1 - k], b1 = B[k], b2 = B[NQ - 1 - k];
+      const R As = a1 + a2, Ad = a1 - a2, Bs = b1 + b2, Bd = b1 - b2;
 #pragma unroll
       for (int i = 0; i < H; ++i) {
-        oE[i] = fma(tb.Se[k][i], As, oE[i]);
-        oE[i] = fma(tb.De[k][i], Bd, oE[i]);
-        oO[i] = fma(tb.So[k][i], Ad, oO[i]);
-        oO[i] = fma(tb.Do[k][i], Bs, oO[i]);
+        oE[i] = fmaR(tb.Se[k][i], As, oE[i]);
+        oE[i] = fmaR(tb.De[k][i], Bd, oE[i]);
+        oO[i] = fmaR(tb.So[k][i], Ad, oO[i]);
+        oO[i] = fmaR(tb.Do[k][i], Bs, oO[i]);
       }
-      if (MIDN) { oM = fma(tb.Sm[k], As, oM); oM = fma(tb.Dm[k], Bd, oM); }
+      if (MIDN) { oM = fmaR(tb.Sm[k], As, oM); oM = fmaR(tb.Dm[k], Bd, oM); }
     }
     {
-      const double am = A[P], bm = B[P];
+      const R am = A[P], bm = B[P];
 #pragma unroll
       for (int i = 0; i < H; ++i) {
-        oE[i] = fma(tb.Se[P][i], am, oE[i]);
-        oO[i] = fma(tb.Do[P][i], bm, oO[i]);
+        oE[i] = fmaR(tb.Se[P][i], am, oE[i]);
+        oO[i] = fmaR(tb.Do[P][i], bm, oO[i]);
       }
-      if (MIDN) oM = fma(tb.Sm[P], am, oM);
+      if (MIDN) oM = fmaR(tb.Sm[P], am, oM);
     }
-    double out[P1];
+    R out[P1];
 #pragma unroll
     for (int i = 0; i < H; ++i) {
       out[i] = oE[i] + oO[i];
@@ -503,29 +524,29 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     }
     if (MIDN) out[P / 2] = oM;
     if (Phys::FACES) {
-      const double* F0 = s_flux + ((0 * NOUT + o) * CB + cl) * NQ;
-      const double* F1 = s_flux + ((1 * NOUT + o) * CB + cl) * NQ;
-      double l = 0.0, r = 0.0;
+      const R* F0 = s_flux + ((0 * NOUT + o) * CB + cl) * NQ;
+      const R* F1 = s_flux + ((1 * NOUT + o) * CB + cl) * NQ;
+      R l = 0.0, r = 0.0;
 #pragma unroll
       for (int q = 0; q < NQ; ++q) {
-        const double s = s_S[q * P1 + iz];
-        l = fma(s, F0[q], l);
-        r = fma(s, F1[q], r);
+        const R s = s_S[q * P1 + iz];
+        l = fmaR(s, F0[q], l);
+        r = fmaR(s, F1[q], r);
       }
       out[0] += l;
       out[P] += r;
       if (iz == 0 || iz == P) {
-        const double* F = s_flux + (((iz == 0 ? 2 : 3) * NOUT + o) * CB + cl) * NQ;
+        const R* F = s_flux + (((iz == 0 ? 2 : 3) * NOUT + o) * CB + cl) * NQ;
 #pragma unroll
         for (int ix = 0; ix < P1; ++ix) {
-          double s = 0.0;
+          R s = 0.0;
 #pragma unroll
-          for (int q = 0; q < NQ; ++q) s = fma(tb.S[q][ix], F[q], s);
+          for (int q = 0; q < NQ; ++q) s = fmaR(tb.S[q][ix], F[q], s);
           out[ix] += s;
         }
       }
     }
-    double* dst = s_out + (o * CB + cl) * L::NDP + iz * P1;
+    R* dst = s_out + (o * CB + cl) * L::NDP + iz * P1;
 #pragma unroll
     for (int ix = 0; ix < P1; ++ix) dst[ix] = out[ix];
   }
@@ -535,10 +556,10 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     constexpr int OA = decltype(oc)::value;
     constexpr int NC = Phys::out_ncomp(OA);
     constexpr int ob = [] { int b = 0; for (int a = 0; a < OA; ++a) b += Phys::out_ncomp(a); return b; }();
-    double* dst = ptr.out[OA] + (size_t)c0 * NC * ND;
+    R* dst = ptr.out[OA] + (size_t)c0 * NC * ND;
     for (int e = tid; e < ncb * NC * ND; e += NT) {
       const int cc = e / (NC * ND), r = e % (NC * ND);
-      const double v = s_out[((ob + r / ND) * CB + cc) * L::NDP + r % ND];
+      const R v = s_out[((ob + r / ND) * CB + cc) * L::NDP + r % ND];
       if (Phys::ACCUMULATE) dst[e] += v;
       else dst[e] = v;
     }
@@ -546,7 +567,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
 }
 
 template <int P, class Phys, int CB_ = cells_per_block<P>(), int MINB = min_blocks_per_sm<P>()>
-cudaError_t launch_cellop(const MeshDev& mesh, const ArgPtrs<PhysInfo<Phys>::NARR_TOTAL, Phys::NOUT_ARR>& ptr,
+cudaError_t launch_cellop(const MeshDev& mesh,
+                          const ArgPtrs<PhysInfo<Phys>::NARR_TOTAL, Phys::NOUT_ARR, RealOf<Phys>>& ptr,
                           const typename Phys::Params& prm, int ncell, cudaStream_t stream) {
   using L = Layout<P, Phys, CB_>;
   static bool configured = false;  // per instantiation; the attribute is per device function

@@ -37,14 +37,40 @@ struct DegreeOps {
   // inverse of the diagonal of scale*M (weight null) or of M_rho (ncomp copies)
   cudaError_t (*inv_diag)(const MeshDev&, int ncomp, const double* weight, double scale, double* dst, int ncell,
                           cudaStream_t);
-  // packed Cholesky factors of the cell mass matrices (weight null: plain mass), stored
-  // interleaved L[k * ncell + c], factor_len() doubles per cell
+  // packed inverses (lower triangle) of the cell mass matrices (weight null: plain mass),
+  // stored interleaved L[k * ncell + c], factor_len() doubles per cell
   cudaError_t (*mass_factor)(const MeshDev&, const double* weight, double* L, int ncell, cudaStream_t);
   // x = scale * M^{-1} b (block diagonal, exact), ncomp components per cell
   cudaError_t (*mass_solve)(const double* L, int ncomp, const double* b, double scale, double* x, int ncell,
                             cudaStream_t);
   int cells_per_block;
   int factor_len;  // (p+1)^2 ((p+1)^2 + 1) / 2
+
+  // ---- h-multigrid level kernels, in FP64 (_d) and FP32 (_f) ----
+  // u = B p (BPhys, coefficient c = coeff dt / Ma^2)
+  cudaError_t (*mg_B_f)(const MeshDev&, const float* p, float c, float* u, int ncell, cudaStream_t);
+  // r += C0 w - D p: the residual update of the linearised Schur complement (C0 = C
+  // without the wave-speed term); prm.g1 carries +1/(gamma-1)
+  cudaError_t (*mg_res_d)(const MeshDev&, const double* w, const double* pf, const double* p, const CParams&,
+                          double* r, int ncell, cudaStream_t);
+  cudaError_t (*mg_res_f)(const MeshDev&, const float* w, const float* pf, const float* p, const CParamsT<float>&,
+                          float* r, int ncell, cudaStream_t);
+  // x = M_K^{-1} b per cell with the packed inverses in FP32
+  cudaError_t (*mass_solve_f)(const float* L, int ncomp, const float* b, float scale, float* x, int ncell,
+                              cudaStream_t);
+  // Chebyshev update with the cell-wise inverse D^{-1} = s M^{-1}:
+  //   d = alpha d + s M^{-1} r  (alpha == 0: d not read);  x = d (first) or x += d
+  cudaError_t (*cheb_d)(const double* L, const double* r, double alpha, double s, double* d, double* x, int first,
+                        int ncell, cudaStream_t);
+  cudaError_t (*cheb_f)(const float* L, const float* r, float alpha, float s, float* d, float* x, int first,
+                        int ncell, cudaStream_t);
+  // xf += P xc (coarse nx_c x nz_c cells, fine 2nx_c x 2nz_c); rc = P^T rf
+  cudaError_t (*prolong_d)(const double* xc, double* xf, int nxc, int nzc, cudaStream_t);
+  cudaError_t (*prolong_f)(const float* xc, float* xf, int nxc, int nzc, cudaStream_t);
+  cudaError_t (*restrict_d)(const double* rf, double* rc, int nxc, int nzc, cudaStream_t);
+  cudaError_t (*restrict_f)(const float* rf, float* rc, int nxc, int nzc, cudaStream_t);
+  // coarse nodal values of a fine coefficient field (injection from the child cell)
+  cudaError_t (*inject)(const double* ff, double* fc, int nxc, int nzc, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

@@ -12,10 +12,17 @@
 namespace af {
 
 static __constant__ Tab<AF_P> c_tab;
+static __constant__ TabT<AF_P, float> c_tabf;
+static __constant__ TransT<AF_P, double> c_tr;
+static __constant__ TransT<AF_P, float> c_trf;
 
 template <>
-__device__ __forceinline__ const Tab<AF_P>& tab<AF_P>() {
+__device__ __forceinline__ const Tab<AF_P>& tabr<AF_P, double>() {
   return c_tab;
+}
+template <>
+__device__ __forceinline__ const TabT<AF_P, float>& tabr<AF_P, float>() {
+  return c_tabf;
 }
 
 namespace {
@@ -24,7 +31,14 @@ constexpr int P = AF_P;
 
 cudaError_t upload_tables() {
   static const Tab<P> t = host::make_tab<P>();
-  return cudaMemcpyToSymbol(c_tab, &t, sizeof(t));
+  static const TabT<P, float> tf = host::make_tab<P, float>();
+  static const TransT<P, double> tr = host::make_trans<P, double>();
+  static const TransT<P, float> trf = host::make_trans<P, float>();
+  cudaError_t e = cudaMemcpyToSymbol(c_tab, &t, sizeof(t));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tabf, &tf, sizeof(tf));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tr, &tr, sizeof(tr));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_trf, &trf, sizeof(trf));
+  return e;
 }
 
 template <int STAGE, int MASK>
@@ -187,10 +201,10 @@ cudaError_t inv_diag(const MeshDev& mesh, int ncomp, const double* weight, doubl
 
 // ---------------------------------------------------------------- exact cell inverse
 // Cell mass matrix  M_K[I][J] = sum_q w(q) JxW(q) phi_I(q) phi_J(q)  (w = 1 or a density),
-// assembled by sum factorisation and factored by Cholesky, one thread per cell.  The packed
-// lower factor (row-major, reciprocal diagonal) is stored interleaved, L[k * ncell + c], so
-// that the solve kernel reads it coalesced.  Per-thread work arrays live in shared memory,
-// interleaved by thread (conflict-free).
+// assembled by sum factorisation, factored by Cholesky and inverted (M^{-1} = L^{-T} L^{-1}),
+// one thread per cell.  The packed lower triangle of the symmetric inverse (row-major) is
+// stored interleaved, Minv[k * ncell + c], so that the apply kernel reads it coalesced.
+// Per-thread work arrays live in shared memory, interleaved by thread (conflict-free).
 constexpr int kND = (P + 1) * (P + 1);
 constexpr int kNPK = kND * (kND + 1) / 2;
 constexpr int kFactorThreads = P <= 2 ? 64 : (P <= 4 ? 32 : 16);
@@ -276,47 +290,86 @@ __global__ void __launch_bounds__(kFactorThreads)
       A[(ii * (ii + 1) / 2 + jj) * NTH + t] = a * inv;
     }
   }
+  // X = L^{-1} (lower), row by row: X_ii = 1/L_ii, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj; the
+  // row is formed in scratch (the quadrature region F) because it still reads L_i.
+  double* Xr = F;
+  for (int ii = 0; ii < ND; ++ii) {
+    const double di = A[(ii * (ii + 1) / 2 + ii) * NTH + t];
+    for (int jj = 0; jj < ii; ++jj) {
+      double s = 0.0;
+      for (int k = jj; k < ii; ++k) s += A[(ii * (ii + 1) / 2 + k) * NTH + t] * A[(k * (k + 1) / 2 + jj) * NTH + t];
+      Xr[jj * NTH + t] = -s * di;
+    }
+    for (int jj = 0; jj < ii; ++jj) A[(ii * (ii + 1) / 2 + jj) * NTH + t] = Xr[jj * NTH + t];
+  }
+  // M^{-1} = X^T X, (i, j <= i) = sum_{k >= i} X_ki X_kj, in place: rows ascending, j
+  // ascending (row i's own X_ii is overwritten last; rows k > i are still X)
+  for (int ii = 0; ii < ND; ++ii)
+    for (int jj = 0; jj <= ii; ++jj) {
+      double s = 0.0;
+      for (int k = ii; k < ND; ++k) s += A[(k * (k + 1) / 2 + ii) * NTH + t] * A[(k * (k + 1) / 2 + jj) * NTH + t];
+      A[(ii * (ii + 1) / 2 + jj) * NTH + t] = s;
+    }
   if (valid)
     for (int k = 0; k < NPK; ++k) Lg[(size_t)k * ncell + c] = A[k * NTH + t];
 }
 
-// x = scale * M_K^{-1} b per cell and component (one thread per cell and component; the
-// working vector lives in shared memory, interleaved by thread)
+// x = scale * M_K^{-1} b per cell and component: one thread per (cell, component) applies
+// the packed symmetric inverse (storage order, read coalesced across cells) with all ND
+// accumulators in registers, so the loads are independent of each other.  MODE 1 is the
+// Chebyshev update of the multigrid smoother: with y = M_K^{-1} b,  d = alpha d + scale y
+// (d not read when alpha == 0), then x = d (first step) or x += d.
 constexpr int kSolveThreads = 128;
+template <class R, int MODE>
 __global__ void __launch_bounds__(kSolveThreads)
-    k_mass_solve(const double* __restrict__ Lg, const double* __restrict__ b, double* __restrict__ x,
-                 const double scale, const int ncomp, const int ncell) {
-  constexpr int ND = kND, NTH = kSolveThreads;
-  extern __shared__ double ys[];  // [ND][NTH]
-  const int t = threadIdx.x;
-  const int gid = blockIdx.x * NTH + t;
+    k_mass_solve(const R* __restrict__ Minv, const R* __restrict__ b, R* __restrict__ x, R* __restrict__ dv,
+                 const R scale, const R alpha, const int first, const int ncomp, const int ncell) {
+  constexpr int ND = kND;
+  const int gid = blockIdx.x * kSolveThreads + threadIdx.x;
   if (gid >= ncell * ncomp) return;
   const int c = gid % ncell, d = gid / ncell;
-  const double* bb = b + ((size_t)c * ncomp + d) * ND;
-  for (int k = 0; k < ND; ++k) ys[k * NTH + t] = bb[k];
-  // forward: L y = b, rows of the packed factor read in storage order
-  const double* Lp = Lg + c;
-  for (int ii = 0; ii < ND; ++ii) {
-    double a = ys[ii * NTH + t];
-    for (int k = 0; k < ii; ++k) {
-      a -= *Lp * ys[k * NTH + t];
-      Lp += ncell;
-    }
-    ys[ii * NTH + t] = a * *Lp;  // reciprocal diagonal
-    Lp += ncell;
+  const size_t off = ((size_t)c * ncomp + d) * ND;
+  R bv[ND], y[ND];
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    bv[k] = b[off + k];
+    y[k] = R(0);
   }
-  // backward: L^T x = y, row by row from the last (x overwrites y)
-  for (int ii = ND - 1; ii >= 0; --ii) {
-    const double* Lr = Lg + (size_t)(ii * (ii + 1) / 2) * ncell + c;
-    const double xi = ys[ii * NTH + t] * Lr[(size_t)ii * ncell];
-    ys[ii * NTH + t] = xi;
-    for (int k = 0; k < ii; ++k) {
-      ys[k * NTH + t] -= *Lr * xi;
-      Lr += ncell;
+  const R* mp = Minv + c;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+#pragma unroll
+    for (int j = 0; j < i; ++j) {
+      const R m = __ldg(mp);
+      mp += ncell;
+      y[i] = fmaR(m, bv[j], y[i]);
+      y[j] = fmaR(m, bv[i], y[j]);
+    }
+    y[i] = fmaR(__ldg(mp), bv[i], y[i]);
+    mp += ncell;
+  }
+  R* xx = x + off;
+  if constexpr (MODE == 0) {
+#pragma unroll
+    for (int k = 0; k < ND; ++k) xx[k] = scale * y[k];
+  } else {
+    R* dd = dv + off;
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+      const R nd = (alpha != R(0) ? alpha * dd[k] : R(0)) + scale * y[k];
+      dd[k] = nd;
+      xx[k] = first ? nd : xx[k] + nd;
     }
   }
-  double* xx = x + ((size_t)c * ncomp + d) * ND;
-  for (int k = 0; k < ND; ++k) xx[k] = scale * ys[k * NTH + t];
+}
+
+template <class R, int MODE>
+cudaError_t launch_mass_solve(const R* L, int ncomp, const R* b, R scale, R* x, R* d, R alpha, int first, int ncell,
+                              cudaStream_t st) {
+  const int n = ncell * ncomp;
+  k_mass_solve<R, MODE><<<(n + kSolveThreads - 1) / kSolveThreads, kSolveThreads, 0, st>>>(L, b, x, d, scale, alpha,
+                                                                                          first, ncomp, ncell);
+  return cudaGetLastError();
 }
 
 cudaError_t mass_factor(const MeshDev& mesh, const double* weight, double* L, int ncell, cudaStream_t st) {
@@ -333,20 +386,154 @@ cudaError_t mass_factor(const MeshDev& mesh, const double* weight, double* L, in
 
 cudaError_t mass_solve(const double* L, int ncomp, const double* b, double scale, double* x, int ncell,
                        cudaStream_t st) {
-  const int n = ncell * ncomp;
-  const size_t bytes = sizeof(double) * kND * kSolveThreads;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_mass_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
-    configured = true;
+  return launch_mass_solve<double, 0>(L, ncomp, b, scale, x, nullptr, 0.0, 0, ncell, st);
+}
+
+// ------------------------------------------------------------------ multigrid kernels
+cudaError_t mg_B_f(const MeshDev& mesh, const float* p, float c, float* u, int ncell, cudaStream_t st) {
+  ArgPtrs<1, 1, float> a{{p}, {u}};
+  return launch_cellop<P, BPhysT<float>>(mesh, a, BParamsT<float>{c}, ncell, st);
+}
+
+// r += C0 w - D p: CPhys with SIGN +1 gives +C0 w; the D term enters with -g1
+template <class R>
+cudaError_t mg_res(const MeshDev& mesh, const R* w, const R* pf, const R* p, const CParamsT<R>& prm, R* r, int ncell,
+                   cudaStream_t st) {
+  ArgPtrs<3, 1, R> a{{p, w, pf}, {r}};
+  CParamsT<R> q = prm;
+  q.g1 = -prm.g1;
+  return launch_cellop<P, CPhys<true, 1, R, false, true>>(mesh, a, q, ncell, st);
+}
+
+cudaError_t mass_solve_f(const float* L, int ncomp, const float* b, float scale, float* x, int ncell,
+                         cudaStream_t st) {
+  return launch_mass_solve<float, 0>(L, ncomp, b, scale, x, nullptr, 0.0f, 0, ncell, st);
+}
+
+template <class R>
+cudaError_t cheb(const R* L, const R* r, R alpha, R s, R* d, R* x, int first, int ncell, cudaStream_t st) {
+  return launch_mass_solve<R, 1>(L, 1, r, s, x, d, alpha, first, ncell, st);
+}
+
+template <class R>
+__device__ __forceinline__ const TransT<P, R>& trans();
+template <>
+__device__ __forceinline__ const TransT<P, double>& trans<double>() {
+  return c_tr;
+}
+template <>
+__device__ __forceinline__ const TransT<P, float>& trans<float>() {
+  return c_trf;
+}
+
+// One thread per fine node: xf[k] += sum_j Pz[kz][jz] Px[kx][jx] xc[j] over the parent cell.
+template <class R>
+__global__ void k_prolong(const R* __restrict__ xc, R* __restrict__ xf, const int nxc, const int nzc) {
+  constexpr int P1 = P + 1, ND = P1 * P1;
+  __shared__ R sP[2][P1][P1];
+  for (int k = threadIdx.x; k < 2 * P1 * P1; k += blockDim.x) (&sP[0][0][0])[k] = (&trans<R>().Pm[0][0][0])[k];
+  __syncthreads();
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = 4L * nxc * nzc * ND;
+  if (idx >= total) return;
+  const int cf = (int)(idx / ND), k = (int)(idx % ND);
+  const int nxf = 2 * nxc, i_f = cf % nxf, j_f = cf / nxf;
+  const int ox = i_f & 1, oz = j_f & 1, cc = (j_f >> 1) * nxc + (i_f >> 1);
+  const int kx = k % P1, kz = k / P1;
+  const R* x = xc + (size_t)cc * ND;
+  R s = 0;
+#pragma unroll
+  for (int jz = 0; jz < P1; ++jz) {
+    R t = 0;
+#pragma unroll
+    for (int jx = 0; jx < P1; ++jx) t = fmaR(sP[ox][kx][jx], x[jz * P1 + jx], t);
+    s = fmaR(sP[oz][kz][jz], t, s);
   }
-  k_mass_solve<<<(n + kSolveThreads - 1) / kSolveThreads, kSolveThreads, bytes, st>>>(L, b, x, scale, ncomp, ncell);
+  xf[idx] += s;
+}
+
+// One thread per coarse node: rc[k] = sum over children and child nodes of P^T rf.
+template <class R>
+__global__ void k_restrict(const R* __restrict__ rf, R* __restrict__ rc, const int nxc, const int nzc) {
+  constexpr int P1 = P + 1, ND = P1 * P1;
+  __shared__ R sP[2][P1][P1];
+  for (int k = threadIdx.x; k < 2 * P1 * P1; k += blockDim.x) (&sP[0][0][0])[k] = (&trans<R>().Pm[0][0][0])[k];
+  __syncthreads();
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)nxc * nzc * ND;
+  if (idx >= total) return;
+  const int cc = (int)(idx / ND), k = (int)(idx % ND);
+  const int ic = cc % nxc, jc = cc / nxc, nxf = 2 * nxc;
+  const int kx = k % P1, kz = k / P1;
+  R s = 0;
+#pragma unroll
+  for (int oz = 0; oz < 2; ++oz)
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+      const R* r = rf + (size_t)((2 * jc + oz) * nxf + 2 * ic + ox) * ND;
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) {
+        R t = 0;
+#pragma unroll
+        for (int ix = 0; ix < P1; ++ix) t = fmaR(sP[ox][ix][kx], r[iz * P1 + ix], t);
+        s = fmaR(sP[oz][iz][kz], t, s);
+      }
+    }
+  rc[idx] = s;
+}
+
+// One thread per coarse node: value of the child polynomial containing the node.
+__global__ void k_inject(const double* __restrict__ ff, double* __restrict__ fc, const int nxc, const int nzc) {
+  constexpr int P1 = P + 1, ND = P1 * P1;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)nxc * nzc * ND;
+  if (idx >= total) return;
+  const TransT<P, double>& tr = c_tr;
+  const int cc = (int)(idx / ND), k = (int)(idx % ND);
+  const int ic = cc % nxc, jc = cc / nxc, nxf = 2 * nxc;
+  const int kx = k % P1, kz = k / P1;
+  const int ox = tr.ch[kx], oz = tr.ch[kz];
+  const double* f = ff + (size_t)((2 * jc + oz) * nxf + 2 * ic + ox) * ND;
+  double s = 0.0;
+  for (int jz = 0; jz < P1; ++jz) {
+    double t = 0.0;
+    for (int jx = 0; jx < P1; ++jx) t = fma(tr.E[kx][jx], f[jz * P1 + jx], t);
+    s = fma(tr.E[kz][jz], t, s);
+  }
+  fc[idx] = s;
+}
+
+constexpr int kTransferThreads = 256;
+
+template <class R>
+cudaError_t prolong(const R* xc, R* xf, int nxc, int nzc, cudaStream_t st) {
+  const long n = 4L * nxc * nzc * kND;
+  k_prolong<R><<<(unsigned)((n + kTransferThreads - 1) / kTransferThreads), kTransferThreads, 0, st>>>(xc, xf, nxc, nzc);
+  return cudaGetLastError();
+}
+template <class R>
+cudaError_t restrict_(const R* rf, R* rc, int nxc, int nzc, cudaStream_t st) {
+  const long n = (long)nxc * nzc * kND;
+  k_restrict<R><<<(unsigned)((n + kTransferThreads - 1) / kTransferThreads), kTransferThreads, 0, st>>>(rf, rc, nxc, nzc);
+  return cudaGetLastError();
+}
+cudaError_t inject(const double* ff, double* fc, int nxc, int nzc, cudaStream_t st) {
+  const long n = (long)nxc * nzc * kND;
+  k_inject<<<(unsigned)((n + kTransferThreads - 1) / kTransferThreads), kTransferThreads, 0, st>>>(ff, fc, nxc, nzc);
   return cudaGetLastError();
 }
 
-const DegreeOps kOps = {upload_tables, rhs, mass, op_B, op_C, inv_diag, mass_factor, mass_solve,
-                        cells_per_block<P>(), kNPK};
+const DegreeOps kOps = {upload_tables,     rhs,
+                        mass,              op_B,
+                        op_C,              inv_diag,
+                        mass_factor,       mass_solve,
+                        cells_per_block<P>(), kNPK,
+                        mg_B_f,            mg_res<double>,
+                        mg_res<float>,     mass_solve_f,
+                        cheb<double>,      cheb<float>,
+                        prolong<double>,   prolong<float>,
+                        restrict_<double>, restrict_<float>,
+                        inject};
 
 }  // namespace
 

@@ -58,6 +58,7 @@ struct RhsPhys {
   static constexpr int NOUT = (RHO ? 1 : 0) + (VEL ? 2 : 0) + (PRES ? 1 : 0);
   static constexpr int O_RHO = 0, O_U = RHO ? 1 : 0, O_P = (RHO ? 1 : 0) + (VEL ? 2 : 0);
   using Params = RhsParams;
+  using real = double;
 
   static constexpr int out_ncomp(int a) {
     // output arrays in the order rho, u, p (present ones only)
@@ -199,15 +200,21 @@ struct RhsPhys {
 };
 
 // ---------------------------------------------------------------- B: p -> u
-struct BParams {
-  double c;  // coeff * dt / Ma^2, coeff = a~22 (stage 1) or a~33
+// R is the working precision: double for the operator itself, float for the multigrid
+// preconditioner's level operators.
+template <class R>
+struct BParamsT {
+  R c;  // coeff * dt / Ma^2, coeff = a~22 (stage 1) or a~33
 };
+using BParams = BParamsT<double>;
 
-struct BPhys {
+template <class R = double>
+struct BPhysT {
   static constexpr int NG = 1;
   static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
   static constexpr int NOUT_ARR = 1, NOUT = 2;
-  using Params = BParams;
+  using Params = BParamsT<R>;
+  using real = R;
   static constexpr int out_ncomp(int) { return 2; }
   static constexpr bool has_val(int) { return false; }
   static constexpr bool has_grad(int) { return true; }
@@ -222,41 +229,45 @@ struct BPhys {
     static constexpr bool face_only(int) { return false; }
   };
   template <int G>
-  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo&, double*,
-                                               double (*gr)[2]) {
-    const double s = -prm.c * v[0];  // submit_divergence (:1536)
+  __device__ __forceinline__ static void point(const Params& prm, const R* v, const PointGeo&, R*, R (*gr)[2]) {
+    const R s = -prm.c * v[0];  // submit_divergence (:1536)
     gr[0][0] += s;
     gr[1][1] += s;
   }
   template <int G>
-  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
-                                              const double* n, double* flux) {
-    const double a = prm.c * 0.5 * (vp[0] + vm[0]);  // :1574-1577
+  __device__ __forceinline__ static void face(const Params& prm, const R* vp, const R* vm, const R* n, R* flux) {
+    const R a = prm.c * R(0.5) * (vp[0] + vm[0]);  // :1574-1577
     flux[0] = a * n[0];
     flux[1] = a * n[1];
   }
   template <int G>
-  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
-                                                  double* flux) {
-    const double a = prm.c * 0.5 * (vp[0] + vp[0]);  // :1611-1613
+  __device__ __forceinline__ static void boundary(const Params& prm, const R* vp, const R* n, R* flux) {
+    const R a = prm.c * R(0.5) * (vp[0] + vp[0]);  // :1611-1613
     flux[0] = a * n[0];
     flux[1] = a * n[1];
   }
 };
+using BPhys = BPhysT<double>;
 
 // ------------------------------------------- C (u -> p), optionally D p - C w (Schur)
-struct CParams {
-  double cdt;     // coeff * dt
-  double g1, gg;  // 1/(gamma-1), gamma/(gamma-1)
+template <class R>
+struct CParamsT {
+  R cdt;     // coeff * dt
+  R g1, gg;  // 1/(gamma-1), gamma/(gamma-1)
 };
+using CParams = CParamsT<double>;
 
-template <bool WITH_D, int SIGN>
+// LAM = false drops the reference's wave-speed term 0.5 lambda(w) [p_fixed]/(gamma-1):
+// the linear part of C, used by the multigrid preconditioner's level operators.
+// ACC = true adds the result to dst instead of overwriting it.
+template <bool WITH_D, int SIGN, class R = double, bool LAM = true, bool ACC = false>
 struct CPhys {
   static constexpr int NG = WITH_D ? 2 : 1;
   static constexpr int GW = WITH_D ? 1 : 0;  // group of (w, p_fixed)
-  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
+  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = ACC;
   static constexpr int NOUT_ARR = 1, NOUT = 1;
-  using Params = CParams;
+  using Params = CParamsT<R>;
+  using real = R;
   static constexpr int out_ncomp(int) { return 1; }
   static constexpr bool has_val(int) { return WITH_D; }
   static constexpr bool has_grad(int) { return true; }
@@ -271,10 +282,10 @@ struct CPhys {
     static constexpr bool face_only(int) { return false; }
   };
   template <int G>
-  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo&, double* val,
-                                               double (*gr)[2]) {
+  __device__ __forceinline__ static void point(const Params& prm, const R* v, const PointGeo&, R* val,
+                                               R (*gr)[2]) {
     if constexpr (G == GW) {  // :1444
-      const double s = -SIGN * prm.cdt * prm.gg * v[2];
+      const R s = R(-SIGN) * prm.cdt * prm.gg * v[2];
       gr[0][0] += s * v[0];
       gr[0][1] += s * v[1];
     } else {                  // :1403
@@ -282,17 +293,21 @@ struct CPhys {
     }
   }
   template <int G>
-  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
-                                              const double* n, double* flux) {
+  __device__ __forceinline__ static void face(const Params& prm, const R* vp, const R* vm, const R* n, R* flux) {
     if constexpr (G == GW) {  // :1494-1502
-      const double wnp = vp[0] * n[0] + vp[1] * n[1], wnm = vm[0] * n[0] + vm[1] * n[1];
-      const double lam = fmax(fabs(wnp), fabs(wnm));
-      const double F = prm.cdt * (0.5 * prm.gg * (vp[2] * wnp + vm[2] * wnm) + 0.5 * lam * (prm.g1 * (vp[2] - vm[2])));
-      flux[0] = SIGN * F;
+      const R wnp = vp[0] * n[0] + vp[1] * n[1], wnm = vm[0] * n[0] + vm[1] * n[1];
+      R F;
+      if constexpr (LAM) {
+        const R lam = fmax(fabs(wnp), fabs(wnm));
+        F = prm.cdt * (R(0.5) * prm.gg * (vp[2] * wnp + vm[2] * wnm) + R(0.5) * lam * (prm.g1 * (vp[2] - vm[2])));
+      } else {
+        F = prm.cdt * (R(0.5) * prm.gg * (vp[2] * wnp + vm[2] * wnm));
+      }
+      flux[0] = R(SIGN) * F;
     }
   }
   template <int G>
-  __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
+  __device__ __forceinline__ static void boundary(const Params&, const R*, const R*, R*) {}
 };
 
 // ---------------------------------------------------------------- mass-type operators
@@ -306,6 +321,7 @@ struct MassPhys {
   static constexpr bool FACES = false, NEED_X = false, ACCUMULATE = false;
   static constexpr int NOUT_ARR = 1, NOUT = NC;
   using Params = MassParams;
+  using real = double;
   static constexpr int out_ncomp(int) { return NC; }
   static constexpr bool has_val(int) { return true; }
   static constexpr bool has_grad(int) { return false; }

@@ -15,17 +15,34 @@
 
 namespace af {
 
-template <int P>
-struct Tab {
+template <int P, class R = double>
+struct TabT {
   static constexpr int P1 = P + 1;
   static constexpr int NQ = 2 * P + 1;
   static constexpr int H = P1 / 2;        // node pairs (i, P-i), i < H
   static constexpr bool MIDN = (P % 2) == 0;  // a middle node exists
-  double S[NQ][P1], D[NQ][P1];
-  double Se[P + 1][H > 0 ? H : 1], So[P + 1][H > 0 ? H : 1];
-  double De[P + 1][H > 0 ? H : 1], Do[P + 1][H > 0 ? H : 1];
-  double Sm[P + 1], Dm[P + 1];
-  double w[NQ], x[NQ];
+  R S[NQ][P1], D[NQ][P1];
+  R Se[P + 1][H > 0 ? H : 1], So[P + 1][H > 0 ? H : 1];
+  R De[P + 1][H > 0 ? H : 1], Do[P + 1][H > 0 ? H : 1];
+  R Sm[P + 1], Dm[P + 1];
+  R w[NQ], x[NQ];
+};
+template <int P>
+using Tab = TabT<P, double>;
+
+
+// Level-transfer tables of the h-multigrid (same degree on every level; a coarse cell's
+// reference square is split into 2 x 2 children, child o in {0,1} per direction covering
+// [o/2, (o+1)/2]):
+//   Pm[o][i][j] = l_j((o + x_i)/2)   value of coarse basis j at child-o node i (prolongation;
+//                                    its transpose restricts residuals)
+//   E[i][j]     = l_j(2 x_i - ch[i]) value of the child-ch[i] basis j at coarse node i
+//                                    (injection of coefficient fields; ch[i] = 0 for x_i <= 1/2)
+template <int P, class R = double>
+struct TransT {
+  R Pm[2][P + 1][P + 1];
+  R E[P + 1][P + 1];
+  int ch[P + 1];
 };
 
 namespace host {
@@ -104,9 +121,9 @@ inline LD dlag(const std::vector<LD>& nd, int i, LD s) {
   return acc;
 }
 
-template <int P>
-inline Tab<P> make_tab() {
-  using T = Tab<P>;
+template <int P, class R = double>
+inline TabT<P, R> make_tab() {
+  using T = TabT<P, R>;
   T t{};
   std::vector<LD> nd = gll(P), x, w;
   gauss(T::NQ, x, w);
@@ -115,22 +132,37 @@ inline Tab<P> make_tab() {
     for (int i = 0; i < T::P1; ++i) {
       S[q][i] = lag(nd, i, x[q]);
       D[q][i] = dlag(nd, i, x[q]);
-      t.S[q][i] = (double)S[q][i];
-      t.D[q][i] = (double)D[q][i];
+      t.S[q][i] = (R)S[q][i];
+      t.D[q][i] = (R)D[q][i];
     }
   for (int q = 0; q <= P; ++q) {
     for (int i = 0; i < T::H; ++i) {
-      t.Se[q][i] = (double)((S[q][i] + S[q][P - i]) / 2);
-      t.So[q][i] = (double)((S[q][i] - S[q][P - i]) / 2);
-      t.De[q][i] = (double)((D[q][i] + D[q][P - i]) / 2);
-      t.Do[q][i] = (double)((D[q][i] - D[q][P - i]) / 2);
+      t.Se[q][i] = (R)((S[q][i] + S[q][P - i]) / 2);
+      t.So[q][i] = (R)((S[q][i] - S[q][P - i]) / 2);
+      t.De[q][i] = (R)((D[q][i] + D[q][P - i]) / 2);
+      t.Do[q][i] = (R)((D[q][i] - D[q][P - i]) / 2);
     }
-    t.Sm[q] = T::MIDN ? (double)S[q][P / 2] : 0.0;
-    t.Dm[q] = T::MIDN ? (double)D[q][P / 2] : 0.0;
+    t.Sm[q] = T::MIDN ? (R)S[q][P / 2] : R(0);
+    t.Dm[q] = T::MIDN ? (R)D[q][P / 2] : R(0);
   }
   for (int q = 0; q < T::NQ; ++q) {
-    t.w[q] = (double)w[q];
-    t.x[q] = (double)x[q];
+    t.w[q] = (R)w[q];
+    t.x[q] = (R)x[q];
+  }
+  return t;
+}
+
+template <int P, class R = double>
+inline TransT<P, R> make_trans() {
+  TransT<P, R> t{};
+  std::vector<LD> nd = gll(P);
+  for (int o = 0; o < 2; ++o)
+    for (int i = 0; i <= P; ++i)
+      for (int j = 0; j <= P; ++j) t.Pm[o][i][j] = (R)lag(nd, j, (o + nd[i]) / 2);
+  for (int i = 0; i <= P; ++i) {
+    const int c = nd[i] <= 0.5L ? 0 : 1;
+    t.ch[i] = c;
+    for (int j = 0; j <= P; ++j) t.E[i][j] = (R)lag(nd, j, 2 * nd[i] - c);
   }
   return t;
 }

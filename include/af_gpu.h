@@ -101,7 +101,8 @@ int af_vmult_pressure(af_operator* op, double* dst, const double* src);
 /* C: velocity -> pressure space (vmult_enthalpy, :2440-2453), uses pres_fixed */
 int af_vmult_enthalpy(af_operator* op, double* dst, const double* src);
 /* Exact inverse of the block-diagonal mass-type operator selected by NS_stage (1/4: M,
- * 6: D = M/(gamma-1), 3/5: A weighted by rho_for_fixed): per-cell Cholesky factors, built
+ * 6: D = M/(gamma-1), 3/5: A weighted by rho_for_fixed): per-cell inverses (from a Cholesky
+ * factorisation, stored as packed symmetric matrices), built
  * on first use and after set_rho_for_fixed.  Replaces the CG + multigrid solves of the
  * reference's update_density / update_velocity / update_pressure (Atmospheric_Flow.cc:
  * 527-535, 775-779, 870) by a direct solve; NS_stage 2 returns AF_BAD_ARG. */
@@ -113,7 +114,7 @@ int af_compute_diagonal(af_operator* op, double* inv_diag);
 /* A^{-1} inside the Schur apply: mode 0 = CG + Jacobi to rel_tol (the reference:
  * SolverControl(10000, 1e-12 |B p|), euler_operator.h:2391-2397; the default, with rel_tol
  * 1e-12 and max_iter 10000); mode 1 = exact cell-wise inverse (A is block diagonal for DG:
- * per-cell Cholesky factors), which replaces the nested CG. */
+ * per-cell inverses), which replaces the nested CG. */
 int af_set_schur_mode(af_operator* op, int mode, double rel_tol, int max_iter);
 /* iterations of the last inner A^{-1} solve */
 int af_last_inner_iterations(const af_operator* op, int* its);
