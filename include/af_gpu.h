@@ -124,6 +124,51 @@ int af_n_dofs(const af_operator* op, int space, long long* n);
 /* Number of kernels this library launched on the handle since creation. */
 int af_launch_count(const af_operator* op, long long* n);
 
+/* ---------------------------------------------------------------- Schur pressure solver
+ * Solves the NS_stage-2 system (D - C A^{-1} B) p = b of af_vmult, the linear solve of the
+ * reference's pressure_fixed_point (Atmospheric_Flow.cc:544-673: SolverGMRES + Jacobi on the
+ * diagonal of D, euler_operator.h:2607-2611), by flexible GMRES in FP64 (right
+ * preconditioning; converged when the TRUE residual |b - S x| <= rel_tol |b|).  The
+ * preconditioner is Jacobi on diag(D) or a geometric h-multigrid V-cycle (the role of the
+ * reference's MGLevelObject / MGTransferMatrixFree / PreconditionChebyshev stack,
+ * Atmospheric_Flow.cc:455-522, which the reference applies to the mass-type systems only):
+ * 2:1 coarsened meshes of the same degree, the linearised Schur operator (C without its
+ * wave-speed term) on every level, Chebyshev smoothing on D^{-1} S with the exact cell-wise
+ * D^{-1}, transfer by polynomial embedding and its transpose, a Chebyshev coarse solve.  Its
+ * levels run in FP64 (AF_SCHUR_MG_FP64) or FP32 (AF_SCHUR_MG_FP32).
+ * The solver uses the operator's stream and its rho_for_fixed / pres_fixed / dt / Mach /
+ * HYPERBOLIC_stage at af_schur_solver_setup time; af_schur_solve sets NS_stage 2. */
+typedef struct af_schur_solver af_schur_solver;
+enum { AF_SCHUR_JACOBI = 0, AF_SCHUR_MG_FP64 = 1, AF_SCHUR_MG_FP32 = 2 };
+typedef struct {
+  int preconditioner;       /* AF_SCHUR_* (default AF_SCHUR_MG_FP32)                          */
+  int smoother_degree;      /* Chebyshev degree of each pre/post smoothing (5)                 */
+  double smoothing_range;   /* the smoother targets [lmax/range, lmax] (15)                    */
+  int coarse_degree;        /* Chebyshev degree of the coarse solve (8)                        */
+  int max_levels;           /* 0: coarsen while nx, nz are even and cells > min_coarse_cells  */
+  int min_coarse_cells;     /* 16                                                              */
+  int eig_iterations;       /* power iterations of the per-level lmax estimate (20)            */
+  int restart;              /* FGMRES directions per cycle, 1..64 (30)                         */
+} af_schur_options;
+typedef struct {
+  int iterations;           /* FGMRES iterations of the last solve                             */
+  double initial_residual;  /* |b - S x0|                                                      */
+  double final_residual;    /* |b - S x| (Arnoldi estimate when it stopped inside a cycle)     */
+  double seconds;           /* device time of the last solve (CUDA events on the stream)       */
+} af_schur_stats;
+int af_schur_default_options(af_schur_options* opt);
+int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schur_solver** out);
+int af_schur_solver_destroy(af_schur_solver* s);
+/* Rebuilds the level coefficients and cell inverses from the operator's current state;
+ * the per-level eigenvalue estimate runs on the first setup or when estimate_eigenvalues. */
+int af_schur_solver_setup(af_schur_solver* s, int estimate_eigenvalues);
+int af_schur_solver_levels(const af_schur_solver* s, int* n_levels, double* lmax);
+/* dst = one application of the preconditioner to src (DEVICE pointers, pressure space). */
+int af_schur_solver_precondition(af_schur_solver* s, double* dst, const double* src);
+/* x (initial guess in, solution out) for S x = b; returns AF_NO_CONVERGENCE at the cap. */
+int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_tol, int max_iterations,
+                   af_schur_stats* stats);
+
 /* ---------------------------------------------------------------- IMEX time stepping
  * One IMEX-DG step of the reference's EulerSolver::run (Atmospheric_Flow.cc:1110-1251):
  * update_density, the pressure fixed point (pressure_fixed_point + update_velocity, at most
