@@ -203,7 +203,8 @@ cudaError_t inv_diag(const MeshDev& mesh, int ncomp, const double* weight, doubl
 // Cell mass matrix  M_K[I][J] = sum_q w(q) JxW(q) phi_I(q) phi_J(q)  (w = 1 or a density),
 // assembled by sum factorisation, factored by Cholesky and inverted (M^{-1} = L^{-T} L^{-1}),
 // one thread per cell.  The packed lower triangle of the symmetric inverse (row-major) is
-// stored interleaved, Minv[k * ncell + c], so that the apply kernel reads it coalesced.
+// stored cell-major, Minv[c * NPK + k], so that one warp of the apply kernel reads a cell's
+// inverse as one contiguous block.
 // Per-thread work arrays live in shared memory, interleaved by thread (conflict-free).
 constexpr int kND = (P + 1) * (P + 1);
 constexpr int kNPK = kND * (kND + 1) / 2;
@@ -310,55 +311,56 @@ __global__ void __launch_bounds__(kFactorThreads)
       for (int k = ii; k < ND; ++k) s += A[(k * (k + 1) / 2 + ii) * NTH + t] * A[(k * (k + 1) / 2 + jj) * NTH + t];
       A[(ii * (ii + 1) / 2 + jj) * NTH + t] = s;
     }
-  if (valid)
-    for (int k = 0; k < NPK; ++k) Lg[(size_t)k * ncell + c] = A[k * NTH + t];
+  // cell-major output, written cooperatively (coalesced): Minv[c * NPK + k]
+  __syncthreads();
+  const int c0 = blockIdx.x * NTH;
+  for (int e = t; e < NTH * NPK; e += NTH) {
+    const int cl = e / NPK, k = e % NPK;
+    if (c0 + cl < ncell) Lg[(size_t)(c0 + cl) * NPK + k] = A[k * NTH + cl];
+  }
 }
 
-// x = scale * M_K^{-1} b per cell and component: one thread per (cell, component) applies
-// the packed symmetric inverse (storage order, read coalesced across cells) with all ND
-// accumulators in registers, so the loads are independent of each other.  MODE 1 is the
-// Chebyshev update of the multigrid smoother: with y = M_K^{-1} b,  d = alpha d + scale y
-// (d not read when alpha == 0), then x = d (first step) or x += d.
-constexpr int kSolveThreads = 128;
+// x = scale * M_K^{-1} b per cell and component: one warp per cell stages the cell's packed
+// symmetric inverse (contiguous, coalesced) and its right-hand sides in shared memory by
+// asynchronous copies, then lane i forms row i.  One load round trip per cell, so small
+// grids are not latency-bound.
+// MODE 1 is the Chebyshev update of the multigrid smoother: with y = M_K^{-1} b,
+// d = alpha d + scale y (d not read when alpha == 0), then x = d (first step) or x += d.
+constexpr int kSolveWarps = 4;
 template <class R, int MODE>
-__global__ void __launch_bounds__(kSolveThreads)
+__global__ void __launch_bounds__(32 * kSolveWarps)
     k_mass_solve(const R* __restrict__ Minv, const R* __restrict__ b, R* __restrict__ x, R* __restrict__ dv,
                  const R scale, const R alpha, const int first, const int ncomp, const int ncell) {
-  constexpr int ND = kND;
-  const int gid = blockIdx.x * kSolveThreads + threadIdx.x;
-  if (gid >= ncell * ncomp) return;
-  const int c = gid % ncell, d = gid / ncell;
-  const size_t off = ((size_t)c * ncomp + d) * ND;
-  R bv[ND], y[ND];
+  constexpr int ND = kND, NPK = kNPK;
+  __shared__ R sM[kSolveWarps][NPK];
+  __shared__ R sb[kSolveWarps][2 * ND];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kSolveWarps + warp;
+  if (c >= ncell) return;  // whole warps only; no block-wide barrier below
+  // asynchronous copies: every load of the warp is in flight before the single wait
+  const R* mp = Minv + (size_t)c * NPK;
+  for (int k = lane; k < NPK; k += 32) cp_async_el(&sM[warp][k], mp + k);
+  const R* bp = b + (size_t)c * ncomp * ND;
+  for (int k = lane; k < ncomp * ND; k += 32) cp_async_el(&sb[warp][k], bp + k);
+  cp_async_wait_all();
+  __syncwarp();
+  for (int i = lane; i < ND; i += 32) {
+    const int ri = i * (i + 1) / 2;
+    for (int d = 0; d < ncomp; ++d) {
+      R y = R(0);
 #pragma unroll
-  for (int k = 0; k < ND; ++k) {
-    bv[k] = b[off + k];
-    y[k] = R(0);
-  }
-  const R* mp = Minv + c;
-#pragma unroll
-  for (int i = 0; i < ND; ++i) {
-#pragma unroll
-    for (int j = 0; j < i; ++j) {
-      const R m = __ldg(mp);
-      mp += ncell;
-      y[i] = fmaR(m, bv[j], y[i]);
-      y[j] = fmaR(m, bv[i], y[j]);
-    }
-    y[i] = fmaR(__ldg(mp), bv[i], y[i]);
-    mp += ncell;
-  }
-  R* xx = x + off;
-  if constexpr (MODE == 0) {
-#pragma unroll
-    for (int k = 0; k < ND; ++k) xx[k] = scale * y[k];
-  } else {
-    R* dd = dv + off;
-#pragma unroll
-    for (int k = 0; k < ND; ++k) {
-      const R nd = (alpha != R(0) ? alpha * dd[k] : R(0)) + scale * y[k];
-      dd[k] = nd;
-      xx[k] = first ? nd : xx[k] + nd;
+      for (int j = 0; j < ND; ++j) {
+        const int idx = j <= i ? ri + j : j * (j + 1) / 2 + i;
+        y = fmaR(sM[warp][idx], sb[warp][d * ND + j], y);
+      }
+      const size_t o = ((size_t)c * ncomp + d) * ND + i;
+      if constexpr (MODE == 0) {
+        x[o] = scale * y;
+      } else {
+        const R nd = (alpha != R(0) ? alpha * dv[o] : R(0)) + scale * y;
+        dv[o] = nd;
+        x[o] = first ? nd : x[o] + nd;
+      }
     }
   }
 }
@@ -366,9 +368,9 @@ __global__ void __launch_bounds__(kSolveThreads)
 template <class R, int MODE>
 cudaError_t launch_mass_solve(const R* L, int ncomp, const R* b, R scale, R* x, R* d, R alpha, int first, int ncell,
                               cudaStream_t st) {
-  const int n = ncell * ncomp;
-  k_mass_solve<R, MODE><<<(n + kSolveThreads - 1) / kSolveThreads, kSolveThreads, 0, st>>>(L, b, x, d, scale, alpha,
-                                                                                          first, ncomp, ncell);
+  if (ncomp < 1 || ncomp > 2) return cudaErrorInvalidValue;
+  k_mass_solve<R, MODE><<<(ncell + kSolveWarps - 1) / kSolveWarps, 32 * kSolveWarps, 0, st>>>(L, b, x, d, scale, alpha,
+                                                                                             first, ncomp, ncell);
   return cudaGetLastError();
 }
 
