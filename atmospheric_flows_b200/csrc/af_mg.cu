@@ -17,8 +17,9 @@
 //               cell, interval [1.2 lmax / range, 1.2 lmax], lmax from power iteration;
 //   transfer    prolongation = embedding of the coarse polynomial in the four children,
 //               restriction = its transpose;
-//   coarse      Chebyshev of higher degree on [0.9, 1.2 lmax]: on the coarsest level the
-//               acoustic Courant number is far below one and D dominates S0.
+//   coarse      Chebyshev of higher degree on [0.9, 1.2 lmax] on the first level whose lmax
+//               is at most coarse_lmax (levels are trimmed there after the eigenvalue
+//               estimate): the acoustic Courant number has dropped and D dominates S0.
 // The FP32 variant keeps FP64 in the outer Krylov residual and orthogonalisation; the
 // V-cycle only has to be a good approximate inverse.
 #include <cuda_runtime.h>
@@ -158,6 +159,7 @@ struct af_schur_solver {
   af_operator* op = nullptr;
   af_schur_options opt{};
   std::vector<Level> lv;
+  int nact = 0;                 // levels in use (the coarsest has lmax <= coarse_lmax)
   bool fp32 = false;
   bool setup_done = false, eig_done = false;
   double cB = 0, cdt = 0;       // B and C coefficients of the last setup
@@ -281,7 +283,7 @@ int vcycle_level(af_schur_solver* s, int l) {
   Level& L = s->lv[l];
   const af_schur_options& opt = s->opt;
   const double hi = 1.2 * L.lmax;
-  if (l + 1 == (int)s->lv.size()) {
+  if (l + 1 == s->nact) {
     const double lo = std::fmin(0.9, hi / opt.smoothing_range);
     return chebyshev<R>(s, L, opt.coarse_degree, lo, hi, true, false);
   }
@@ -329,7 +331,7 @@ int setup_levels(af_schur_solver* s, bool estimate) {
   const double coeff = o->hs == 1 ? o->a22t : o->a33t;  // euler_operator.h:1428, 1526
   s->cB = coeff * o->dt / (o->Ma * o->Ma);
   s->cdt = coeff * o->dt;
-  for (size_t l = 0; l < s->lv.size(); ++l) {
+  for (int l = 0; l < s->nact; ++l) {
     Level& L = s->lv[l];
     if (l == 0) {
       L.rho = o->d_rho_fixed;
@@ -351,8 +353,15 @@ int setup_levels(af_schur_solver* s, bool estimate) {
     MG_CU(cudaGetLastError());
     o->launches += 3;
   }
-  if (estimate)
-    for (auto& L : s->lv) MG_AF(estimate_lmax<R>(s, L));
+  if (estimate) {  // top-down; the first level with lmax <= coarse_lmax becomes the coarsest
+    for (int l = 0; l < s->nact; ++l) {
+      MG_AF(estimate_lmax<R>(s, s->lv[l]));
+      if (s->lv[l].lmax <= s->opt.coarse_lmax) {
+        s->nact = l + 1;
+        break;
+      }
+    }
+  }
   return AF_OK;
 }
 
@@ -410,7 +419,8 @@ int af_schur_default_options(af_schur_options* opt) {
   opt->preconditioner = AF_SCHUR_MG_FP32;
   opt->smoother_degree = 5;
   opt->smoothing_range = 15.0;
-  opt->coarse_degree = 8;
+  opt->coarse_degree = 10;
+  opt->coarse_lmax = 25.0;
   opt->max_levels = 0;
   opt->min_coarse_cells = 16;
   opt->eig_iterations = 20;
@@ -427,7 +437,7 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
   if (o.preconditioner < AF_SCHUR_JACOBI || o.preconditioner > AF_SCHUR_MG_FP32)
     return merr(AF_BAD_ARG, "af_schur_solver_create: unknown preconditioner");
   if (o.smoother_degree < 1 || o.coarse_degree < 1 || o.smoothing_range <= 1.0 || o.eig_iterations < 1 ||
-      o.restart < 1 || o.restart > 64)
+      o.restart < 1 || o.restart > 64 || !(o.coarse_lmax >= 0.0))
     return merr(AF_BAD_ARG, "af_schur_solver_create: invalid options");
   MG_CU(cudaSetDevice(op->device));
   auto* s = new af_schur_solver();
@@ -493,6 +503,7 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
     for (void** p : {&L.u, &L.w})
       if ((r = alloc(s, p, rs * 2 * L.ns)) != AF_OK) return cleanup(r);
   }
+  s->nact = (int)s->lv.size();
   if (s->fp32 && (r = alloc(s, (void**)&s->dtmp, sizeof(double) * maxf)) != AF_OK) return cleanup(r);
   r = s->fp32 ? build_mass_inverses<float>(s) : build_mass_inverses<double>(s);
   if (r != AF_OK) return cleanup(r);
@@ -530,9 +541,9 @@ int af_schur_solver_setup(af_schur_solver* s, int estimate_eigenvalues) {
 
 int af_schur_solver_levels(const af_schur_solver* s, int* n_levels, double* lmax) {
   if (!s || !n_levels) return merr(AF_BAD_ARG, "null argument");
-  *n_levels = (int)s->lv.size();
+  *n_levels = s->nact;
   if (lmax)
-    for (size_t l = 0; l < s->lv.size(); ++l) lmax[l] = s->lv[l].lmax;
+    for (int l = 0; l < s->nact; ++l) lmax[l] = s->lv[l].lmax;
   return AF_OK;
 }
 

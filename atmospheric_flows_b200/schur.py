@@ -20,7 +20,7 @@ class Options(ctypes.Structure):
     _fields_ = [("preconditioner", ctypes.c_int), ("smoother_degree", ctypes.c_int),
                 ("smoothing_range", ctypes.c_double), ("coarse_degree", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("min_coarse_cells", ctypes.c_int),
-                ("eig_iterations", ctypes.c_int), ("restart", ctypes.c_int)]
+                ("eig_iterations", ctypes.c_int), ("restart", ctypes.c_int), ("coarse_lmax", ctypes.c_double)]
 
 
 class Stats(ctypes.Structure):

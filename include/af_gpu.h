@@ -144,11 +144,12 @@ typedef struct {
   int preconditioner;       /* AF_SCHUR_* (default AF_SCHUR_MG_FP32)                          */
   int smoother_degree;      /* Chebyshev degree of each pre/post smoothing (5)                 */
   double smoothing_range;   /* the smoother targets [lmax/range, lmax] (15)                    */
-  int coarse_degree;        /* Chebyshev degree of the coarse solve (8)                        */
+  int coarse_degree;        /* Chebyshev degree of the coarse solve (10)                       */
   int max_levels;           /* 0: coarsen while nx, nz are even and cells > min_coarse_cells  */
   int min_coarse_cells;     /* 16                                                              */
   int eig_iterations;       /* power iterations of the per-level lmax estimate (20)            */
   int restart;              /* FGMRES directions per cycle, 1..64 (30)                         */
+  double coarse_lmax;       /* the first level with lmax <= this is the coarsest (25)          */
 } af_schur_options;
 typedef struct {
   int iterations;           /* FGMRES iterations of the last solve                             */

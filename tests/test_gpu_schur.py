@@ -104,7 +104,7 @@ def test_vcycle_matches_dense_restatement(precision, tol):
     op.set_pres_fixed(one)
     op.set_NS_stage(2)
     b = np.random.default_rng(3).standard_normal(n)
-    s = SchurSolver(op, precision, max_levels=2, coarse_degree=60, smoother_degree=3)
+    s = SchurSolver(op, precision, max_levels=2, coarse_degree=60, smoother_degree=3, coarse_lmax=0.0)
     s.setup()
     z = torch.zeros(n, dtype=torch.float64, device="cuda")
     s.precondition(z, torch.from_numpy(b).cuda())
