@@ -46,6 +46,7 @@ struct af_imex {
   double *V, *gw, *d_h, *scal;
   double* part;
   KrylovState* kst;
+  af_schur_solver* schur = nullptr;  // FGMRES + Jacobi/multigrid (schur_preconditioner >= 0)
   af_imex_stats stats{};
 };
 
@@ -222,7 +223,7 @@ static int update_density(af_imex* h, int stage) {
   return mass_solve(h, h->invd_M, x, h->rhs_rho, ns, h->opt.eps);
 }
 
-static int pressure_fixed_point(af_imex* h, int stage) {
+static int pressure_fixed_point(af_imex* h, int stage, int iter) {
   af_operator* o = h->op;
   const long ns = h->ns;
   IM_AF(af_set_pres_fixed(o, h->pfix_old));
@@ -247,6 +248,16 @@ static int pressure_fixed_point(af_imex* h, int stage) {
   // (D - C A^{-1} B) p = rhs_p by GMRES + Jacobi(diag D), x0 = pres_fixed_old
   IM_AF(af_set_NS_stage(o, 2));
   IM_CU(cudaMemcpyAsync(h->pfix, h->pfix_old, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  if (h->schur) {
+    // FGMRES to eps |rhs_p| on the true residual; the preconditioner is rebuilt at the first
+    // fixed-point iteration of each stage (rho_for_fixed changes there; pres_fixed changes
+    // every iteration but only enters the preconditioner, which may lag)
+    if (iter == 0) IM_AF(af_schur_solver_setup(h->schur, 0));
+    af_schur_stats st{};
+    const int r = af_schur_solve(h->schur, h->pfix, h->rhs_p, h->opt.eps, h->opt.max_iterations, &st);
+    h->stats.gmres_iterations += st.iterations;
+    return r;
+  }
   Apply S = [o](const double* in, double* out) { return af_vmult(o, out, in); };
   const double tol = h->opt.eps * l2norm(h, h->rhs_p, ns);
   return gmres_solve(h, S, h->invd_D, h->pfix, h->rhs_p, ns, tol, nullptr);
@@ -295,7 +306,7 @@ static int fixed_point(af_imex* h, int stage, double* p_out, double* u_out) {
   int iters = 0;
   double err = 0.0;
   for (int iter = 0; iter < h->opt.fixed_point_max_iterations; ++iter) {
-    IM_AF(pressure_fixed_point(h, stage));
+    IM_AF(pressure_fixed_point(h, stage, iter));
     IM_AF(update_velocity(h, stage));
     ++iters;
     IM_CU(maxabs2(h->pfix, h->pfix_old, ns, h->part, h->scal, o->stream));
@@ -353,6 +364,7 @@ int af_imex_default_options(af_imex_options* opt) {
   opt->gmres_restart = 28;            // deal.II SolverGMRES default (30 temporary vectors)
   opt->mass_solver = 1;
   opt->schur_inner = 1;
+  opt->schur_preconditioner = -1;
   return AF_OK;
 }
 
@@ -365,7 +377,7 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   if (opt) o = *opt;
   if (!(o.eps > 0) || o.max_iterations < 1 || o.gmres_restart < 1 || o.gmres_restart > 60 ||
       o.fixed_point_max_iterations < 1 || o.mass_solver < 0 || o.mass_solver > 1 || o.schur_inner < 0 ||
-      o.schur_inner > 1)
+      o.schur_inner > 1 || o.schur_preconditioner < -1 || o.schur_preconditioner > AF_SCHUR_MG_FP32)
     return ierr(AF_BAD_ARG, "af_imex_create: bad options");
   auto* h = new af_imex();
   h->opt = o;
@@ -407,6 +419,13 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   if (r == AF_OK) r = af_set_NS_stage(h->op, 1);
   if (r == AF_OK) r = af_compute_diagonal(h->op, h->invd_M);
   if (r == AF_OK) { af_set_NS_stage(h->op, 6); r = af_compute_diagonal(h->op, h->invd_D); }
+  if (r == AF_OK && o.schur_preconditioner >= 0) {
+    af_schur_options so{};
+    af_schur_default_options(&so);
+    so.preconditioner = o.schur_preconditioner;
+    so.restart = o.gmres_restart;
+    r = af_schur_solver_create(h->op, &so, &h->schur);
+  }
   if (r == AF_OK) r = af_synchronize(h->op);
   if (r != AF_OK) { af_imex_destroy(h); return r; }
   *out = h;
@@ -416,6 +435,7 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
 int af_imex_destroy(af_imex* h) {
   if (!h) return AF_OK;
   if (h->op) af_synchronize(h->op);
+  af_schur_solver_destroy(h->schur);
   cudaFree(h->mem);
   af_destroy(h->op);
   delete h;

@@ -12,7 +12,7 @@ from .operator import _MeshDesc, _ptr, check, lib
 class Options(ctypes.Structure):
     _fields_ = [("eps", ctypes.c_double), ("max_iterations", ctypes.c_int), ("fixed_point_tol", ctypes.c_double),
                 ("fixed_point_max_iterations", ctypes.c_int), ("gmres_restart", ctypes.c_int),
-                ("mass_solver", ctypes.c_int), ("schur_inner", ctypes.c_int)]
+                ("mass_solver", ctypes.c_int), ("schur_inner", ctypes.c_int), ("schur_preconditioner", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -43,7 +43,8 @@ class IMEXStepper:
     """GPU time stepper: set_state(rho, u, p) -> step(n) -> get_state()."""
 
     def __init__(self, mesh, degree, Ma, Fr, dt, eps=None, max_iterations=None, fixed_point_tol=None,
-                 fixed_point_max_iterations=None, gmres_restart=None, mass_solver=None, schur_inner=None):
+                 fixed_point_max_iterations=None, gmres_restart=None, mass_solver=None, schur_inner=None,
+                 schur_preconditioner=None):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("IMEXStepper needs a CUDA device (no CPU fallback)")
@@ -53,7 +54,9 @@ class IMEXStepper:
         check(L.af_imex_default_options(ctypes.byref(opt)))
         for k, v in (("eps", eps), ("max_iterations", max_iterations), ("fixed_point_tol", fixed_point_tol),
                      ("fixed_point_max_iterations", fixed_point_max_iterations), ("gmres_restart", gmres_restart),
-                     ("mass_solver", mass_solver), ("schur_inner", schur_inner)):
+                     ("mass_solver", mass_solver), ("schur_inner", schur_inner),
+                     ("schur_preconditioner", {"jacobi": 0, "mg_fp64": 1, "mg_fp32": 2}.get(schur_preconditioner,
+                                                                                        schur_preconditioner))):
             if v is not None:
                 setattr(opt, k, v)
         self.mesh, self.degree = mesh, degree

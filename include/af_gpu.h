@@ -187,6 +187,9 @@ typedef struct {
   int gmres_restart;               /* 28 (deal.II SolverGMRES default)                     */
   int mass_solver;                 /* 0: CG + Jacobi to eps; 1: exact cell-wise inverse (default) */
   int schur_inner;                 /* A^{-1} in the Schur apply: 0 nested CG; 1 exact (default)   */
+  int schur_preconditioner;        /* -1: the reference's GMRES + left Jacobi (default);
+                                      AF_SCHUR_*: af_schur_solve (FGMRES, true residual <= eps |rhs_p|,
+                                      preconditioner rebuilt once per stage) */
 } af_imex_options;
 typedef struct {
   int fixed_point_iterations[2];   /* stage 1, stage 2 of the last step                   */

@@ -1001,6 +1001,7 @@ static void rhs_rho_fn(const Op<N>& o, std::vector<N>& dst, const std::vector<co
 struct Imex {
   double eps = 1e-8, fp_tol = 1e-10;
   int maxit = 30000, fp_max = 100, restart = 28;
+  int true_residual = 0;  // pressure GMRES: 0 the reference's left Jacobi; 1 right Jacobi, tol on |b - S x|
   std::vector<double> tmp1;  // persistent initial guess of A^{-1} rhs_u (member tmp_1)
   int fp_iters[2] = {0, 0};
 };
@@ -1029,18 +1030,23 @@ static int cg_abs(Op<N>& o, int ns, std::vector<N>& x, const std::vector<N>& b, 
   return its;
 }
 
-// SolverGMRES, left preconditioning, restart m, modified Gram-Schmidt, tol on |P^{-1} r|
+// SolverGMRES, restart m, modified Gram-Schmidt.  right = false: left preconditioning, tol
+// on |P^{-1} r| (deal.II's default, the reference's setting); right = true: right
+// preconditioning, tol on the true residual |b - A x| (the criterion of the library's
+// af_schur_solve).
 template <typename N, typename A, typename Pc>
-static int gmres_left(A&& apply, Pc&& prec, std::vector<N>& x, const std::vector<N>& b, N tol, int m, int maxit) {
+static int gmres_left(A&& apply, Pc&& prec, std::vector<N>& x, const std::vector<N>& b, N tol, int m, int maxit,
+                      bool right = false) {
   size_t n = b.size();
   std::vector<std::vector<N>> V(m + 1, std::vector<N>(n));
-  std::vector<N> w(n), t(n);
+  std::vector<N> w(n), t(n), z(n);
   std::vector<N> H((m + 1) * m), cs(m), sn(m), g(m + 1);
   int total = 0;
   while (true) {
     apply(t, x);
     for (size_t i = 0; i < n; ++i) t[i] = b[i] - t[i];
-    prec(w, t);
+    if (right) w = t;
+    else prec(w, t);
     N beta = std::sqrt(vdot(w, w));
     if (beta <= tol) return total;
     if (total >= maxit) return -1;
@@ -1050,8 +1056,13 @@ static int gmres_left(A&& apply, Pc&& prec, std::vector<N>& x, const std::vector
     int k = 0;
     N res = beta;
     for (int j = 0; j < m; ++j) {
-      apply(t, V[j]);
-      prec(w, t);
+      if (right) {
+        prec(z, V[j]);
+        apply(w, z);
+      } else {
+        apply(t, V[j]);
+        prec(w, t);
+      }
       for (int i = 0; i <= j; ++i) {
         N hij = vdot(V[i], w);
         H[i * m + j] = hij;
@@ -1083,6 +1094,14 @@ static int gmres_left(A&& apply, Pc&& prec, std::vector<N>& x, const std::vector
       N sum = g[i];
       for (int l = i + 1; l < k; ++l) sum -= H[i * m + l] * y[l];
       y[i] = sum / H[i * m + i];
+    }
+    if (right) {
+      std::fill(t.begin(), t.end(), (N)0);
+      for (int i = 0; i < k; ++i)
+        for (size_t l = 0; l < n; ++l) t[l] += y[i] * V[i][l];
+      prec(z, t);
+      for (size_t l = 0; l < n; ++l) x[l] += z[l];
+      continue;  // converged only when the recomputed true residual is below tol
     }
     for (int i = 0; i < k; ++i)
       for (size_t l = 0; l < n; ++l) x[l] += y[i] * V[i][l];
@@ -1138,7 +1157,8 @@ static void imex_step(Op<N>& o, Imex& im, std::vector<N>& rho0, std::vector<N>& 
       o.ns_stage = 2;
       auto S = [&](std::vector<N>& y, const std::vector<N>& v) { vmult(o, y.data(), v.data()); };
       auto jac = [&](std::vector<N>& z, const std::vector<N>& r) { for (size_t i = 0; i < r.size(); ++i) z[i] = invd[i] * r[i]; };
-      gmres_left<N>(S, jac, pfix, rhs_p, (N)im.eps * std::sqrt(vdot(rhs_p, rhs_p)), im.restart, im.maxit);
+      gmres_left<N>(S, jac, pfix, rhs_p, (N)im.eps * std::sqrt(vdot(rhs_p, rhs_p)), im.restart, im.maxit,
+                    im.true_residual != 0);
       // update_velocity
       apply_B(o, tmp.data(), pfix.data());
       for (long i = 0; i < 2 * ns; ++i) rhs_u[i] -= tmp[i];
@@ -1362,7 +1382,7 @@ extern "C" {
 /* nsteps IMEX steps on (rho, u, p) in place (double instance only); fp_iters receives the
    fixed-point iteration counts of stages 1 and 2 of the last step. */
 int orc_imex_steps(void* h, double* rho, double* u, double* p, int nsteps, double eps, int maxit, double fp_tol,
-                   int fp_max, int restart, int* fp_iters) {
+                   int fp_max, int restart, int* fp_iters, int true_residual) {
   OrcHandle* H = (OrcHandle*)h;
   if (H->ld) return -1;
   Op<double>& o = *H->d;
@@ -1370,6 +1390,7 @@ int orc_imex_steps(void* h, double* rho, double* u, double* p, int nsteps, doubl
   std::vector<double> r(rho, rho + ns), uu(u, u + 2 * ns), pp(p, p + ns);
   Imex im;
   im.eps = eps; im.maxit = maxit; im.fp_tol = fp_tol; im.fp_max = fp_max; im.restart = restart;
+  im.true_residual = true_residual;
   for (int k = 0; k < nsteps; ++k) imex_step(o, im, r, uu, pp);
   std::copy(r.begin(), r.end(), rho);
   std::copy(uu.begin(), uu.end(), u);

@@ -46,6 +46,33 @@ def test_imex_steps_match_oracle(P, nsteps, mesh, exact):
     assert rel(p, p_ref) < STATE_TOL
 
 
+@pytest.mark.parametrize("pc", ["jacobi", "mg_fp64", "mg_fp32"])
+def test_imex_schur_solver_options_match_oracle(pc):
+    """The pressure system solved by af_schur_solve (FGMRES on the true residual, Jacobi or
+    multigrid preconditioning with FP64 or FP32 levels) instead of the reference's
+    left-Jacobi GMRES, against the oracle run with the same true-residual criterion (its
+    GMRES right-preconditioned): same states after two steps to the stated tolerance."""
+    from atmospheric_flows_b200.imex import IMEXStepper
+    from oracle.oracle import OracleOperator, imex_steps
+    P, nsteps, dt = 3, 2, 2.0
+    m = M.hill_mesh(16, 8)
+    sc = M.Scaling()
+    st = M.hill_state(m, P, amplitude=1e-3)
+    o = OracleOperator(m, P, sc.Ma, sc.Fr, dt)
+    r_ref, u_ref, p_ref, fp_ref = imex_steps(o, st.rho, st.u, st.p, nsteps, eps=1e-12, true_residual=True)
+    g = IMEXStepper(m, P, sc.Ma, sc.Fr, dt, eps=1e-12, schur_preconditioner=pc)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    g.set_state(d(st.rho), d(st.u), d(st.p))
+    g.step(nsteps)
+    r, u, p = (t.cpu().numpy() for t in g.get_state())
+    s = g.stats()
+    assert s["gmres_iterations"] > 0
+    assert abs(s["fixed_point_iterations"][0] - fp_ref[0]) <= 1
+    assert rel(r, r_ref) < STATE_TOL
+    assert rel(u, u_ref) < STATE_TOL
+    assert rel(p, p_ref) < STATE_TOL
+
+
 def test_imex_rest_state_stays_balanced():
     """An isothermal atmosphere at rest on a flat box is a discrete steady state up to the
     hydrostatic discretisation residual: velocities stay tiny after a few steps."""
