@@ -377,7 +377,7 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   if (opt) o = *opt;
   if (!(o.eps > 0) || o.max_iterations < 1 || o.gmres_restart < 1 || o.gmres_restart > 60 ||
       o.fixed_point_max_iterations < 1 || o.mass_solver < 0 || o.mass_solver > 1 || o.schur_inner < 0 ||
-      o.schur_inner > 1 || o.schur_preconditioner < -1 || o.schur_preconditioner > AF_SCHUR_MG_FP32)
+      o.schur_inner > 1 || o.schur_preconditioner < -1 || o.schur_preconditioner > AF_SCHUR_CHEB_FP32)
     return ierr(AF_BAD_ARG, "af_imex_create: bad options");
   auto* h = new af_imex();
   h->opt = o;

@@ -1,8 +1,9 @@
 // af_mg.cu -- the Schur-complement pressure solver: flexible GMRES in FP64 around the
 // operator's NS_stage-2 apply D p - C A^{-1} B p (euler_operator.h:2374-2408), preconditioned
-// by either Jacobi on diag(D) (what the reference uses, Atmospheric_Flow.cc:657-672 with the
-// diagonal of euler_operator.h:2607-2611) or a geometric h-multigrid V-cycle whose levels run
-// in FP64 or FP32.
+// by Jacobi on diag(D) (what the reference uses, Atmospheric_Flow.cc:657-672 with the
+// diagonal of euler_operator.h:2607-2611), by a geometric h-multigrid V-cycle whose levels run
+// in FP64 or FP32, or by its single-level case, a Chebyshev polynomial in D^{-1} S0 over the
+// whole spectrum (FP64 or FP32).
 //
 // Multigrid (the role of the reference's MGLevelObject / MGTransferMatrixFree /
 // PreconditionChebyshev / coarse-solver stack, Atmospheric_Flow.cc:455-522, rebuilt for the
@@ -416,11 +417,12 @@ extern "C" {
 
 int af_schur_default_options(af_schur_options* opt) {
   if (!opt) return merr(AF_BAD_ARG, "null options");
-  opt->preconditioner = AF_SCHUR_MG_FP32;
+  opt->preconditioner = AF_SCHUR_CHEB_FP32;
   opt->smoother_degree = 5;
   opt->smoothing_range = 15.0;
   opt->coarse_degree = 10;
   opt->coarse_lmax = 25.0;
+  opt->poly_degree = 16;
   opt->max_levels = 0;
   opt->min_coarse_cells = 16;
   opt->eig_iterations = 20;
@@ -434,16 +436,21 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
   af_schur_options o{};
   if (opt) o = *opt;
   else af_schur_default_options(&o);
-  if (o.preconditioner < AF_SCHUR_JACOBI || o.preconditioner > AF_SCHUR_MG_FP32)
+  if (o.preconditioner < AF_SCHUR_JACOBI || o.preconditioner > AF_SCHUR_CHEB_FP32)
     return merr(AF_BAD_ARG, "af_schur_solver_create: unknown preconditioner");
   if (o.smoother_degree < 1 || o.coarse_degree < 1 || o.smoothing_range <= 1.0 || o.eig_iterations < 1 ||
-      o.restart < 1 || o.restart > 64 || !(o.coarse_lmax >= 0.0))
+      o.restart < 1 || o.restart > 64 || !(o.coarse_lmax >= 0.0) || o.poly_degree < 1)
     return merr(AF_BAD_ARG, "af_schur_solver_create: invalid options");
+  if (o.preconditioner == AF_SCHUR_CHEB_FP64 || o.preconditioner == AF_SCHUR_CHEB_FP32) {
+    // single level: the "coarse solve" on the operator's own mesh is the polynomial
+    o.max_levels = 1;
+    o.coarse_degree = o.poly_degree;
+  }
   MG_CU(cudaSetDevice(op->device));
   auto* s = new af_schur_solver();
   s->op = op;
   s->opt = o;
-  s->fp32 = o.preconditioner == AF_SCHUR_MG_FP32;
+  s->fp32 = o.preconditioner == AF_SCHUR_MG_FP32 || o.preconditioner == AF_SCHUR_CHEB_FP32;
   const size_t rs = s->fp32 ? sizeof(float) : sizeof(double);
   const long ns0 = op->n_scalar();
   auto cleanup = [&](int code) {

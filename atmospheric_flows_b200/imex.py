@@ -7,6 +7,7 @@ import ctypes
 import numpy as np
 
 from .operator import _MeshDesc, _ptr, check, lib
+from .schur import NAMES as SCHUR_NAMES
 
 
 class Options(ctypes.Structure):
@@ -55,8 +56,7 @@ class IMEXStepper:
         for k, v in (("eps", eps), ("max_iterations", max_iterations), ("fixed_point_tol", fixed_point_tol),
                      ("fixed_point_max_iterations", fixed_point_max_iterations), ("gmres_restart", gmres_restart),
                      ("mass_solver", mass_solver), ("schur_inner", schur_inner),
-                     ("schur_preconditioner", {"jacobi": 0, "mg_fp64": 1, "mg_fp32": 2}.get(schur_preconditioner,
-                                                                                        schur_preconditioner))):
+                     ("schur_preconditioner", SCHUR_NAMES.get(schur_preconditioner, schur_preconditioner))):
             if v is not None:
                 setattr(opt, k, v)
         self.mesh, self.degree = mesh, degree

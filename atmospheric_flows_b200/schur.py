@@ -2,8 +2,8 @@
 Atmospheric_Flow.cc:544-673) over the C ABI of libaf_gpu.so (af_schur_*).
 
 ``SchurSolver(op, preconditioner)`` wraps flexible GMRES in FP64 around the operator's
-NS_stage-2 apply with a Jacobi (diag D) or geometric-multigrid (FP64 or FP32 levels)
-preconditioner.  Vectors are CUDA float64 tensors in the pressure space; the solver runs on
+NS_stage-2 apply with a Jacobi (diag D), geometric-multigrid (FP64 or FP32 levels) or
+single-level Chebyshev-polynomial (FP64 or FP32) preconditioner.  Vectors are CUDA float64 tensors in the pressure space; the solver runs on
 the operator's stream.
 """
 from __future__ import annotations
@@ -12,15 +12,16 @@ import ctypes
 
 from .operator import AFError, _ptr, check, lib
 
-JACOBI, MG_FP64, MG_FP32 = 0, 1, 2
-_NAMES = {"jacobi": JACOBI, "mg_fp64": MG_FP64, "mg_fp32": MG_FP32}
+JACOBI, MG_FP64, MG_FP32, CHEB_FP64, CHEB_FP32 = 0, 1, 2, 3, 4
+NAMES = {"jacobi": JACOBI, "mg_fp64": MG_FP64, "mg_fp32": MG_FP32, "cheb_fp64": CHEB_FP64, "cheb_fp32": CHEB_FP32}
 
 
 class Options(ctypes.Structure):
     _fields_ = [("preconditioner", ctypes.c_int), ("smoother_degree", ctypes.c_int),
                 ("smoothing_range", ctypes.c_double), ("coarse_degree", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("min_coarse_cells", ctypes.c_int),
-                ("eig_iterations", ctypes.c_int), ("restart", ctypes.c_int), ("coarse_lmax", ctypes.c_double)]
+                ("eig_iterations", ctypes.c_int), ("restart", ctypes.c_int), ("coarse_lmax", ctypes.c_double),
+                ("poly_degree", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -54,10 +55,10 @@ class SchurSolver:
     """FGMRES for (D - C A^{-1} B) p = b on an EULEROperator (its rho_for_fixed and
     pres_fixed must be set before ``setup``)."""
 
-    def __init__(self, op, preconditioner="mg_fp32", **options):
+    def __init__(self, op, preconditioner="cheb_fp32", **options):
         L = _bind()
         opt = default_options()
-        opt.preconditioner = _NAMES[preconditioner] if isinstance(preconditioner, str) else int(preconditioner)
+        opt.preconditioner = NAMES[preconditioner] if isinstance(preconditioner, str) else int(preconditioner)
         for k, v in options.items():
             if not hasattr(opt, k):
                 raise TypeError(f"unknown option {k}")

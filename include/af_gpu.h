@@ -135,13 +135,15 @@ int af_launch_count(const af_operator* op, long long* n);
  * 2:1 coarsened meshes of the same degree, the linearised Schur operator (C without its
  * wave-speed term) on every level, Chebyshev smoothing on D^{-1} S with the exact cell-wise
  * D^{-1}, transfer by polynomial embedding and its transpose, a Chebyshev coarse solve.  Its
- * levels run in FP64 (AF_SCHUR_MG_FP64) or FP32 (AF_SCHUR_MG_FP32).
+ * levels run in FP64 (AF_SCHUR_MG_FP64) or FP32 (AF_SCHUR_MG_FP32).  AF_SCHUR_CHEB_FP64 /
+ * _FP32 is the single-level case: a Chebyshev polynomial of degree poly_degree in D^{-1} S
+ * over its whole spectrum [0.9, 1.2 lmax] (no coarse levels).
  * The solver uses the operator's stream and its rho_for_fixed / pres_fixed / dt / Mach /
  * HYPERBOLIC_stage at af_schur_solver_setup time; af_schur_solve sets NS_stage 2. */
 typedef struct af_schur_solver af_schur_solver;
-enum { AF_SCHUR_JACOBI = 0, AF_SCHUR_MG_FP64 = 1, AF_SCHUR_MG_FP32 = 2 };
+enum { AF_SCHUR_JACOBI = 0, AF_SCHUR_MG_FP64 = 1, AF_SCHUR_MG_FP32 = 2, AF_SCHUR_CHEB_FP64 = 3, AF_SCHUR_CHEB_FP32 = 4 };
 typedef struct {
-  int preconditioner;       /* AF_SCHUR_* (default AF_SCHUR_MG_FP32)                          */
+  int preconditioner;       /* AF_SCHUR_* (default AF_SCHUR_CHEB_FP32)                        */
   int smoother_degree;      /* Chebyshev degree of each pre/post smoothing (5)                 */
   double smoothing_range;   /* the smoother targets [lmax/range, lmax] (15)                    */
   int coarse_degree;        /* Chebyshev degree of the coarse solve (10)                       */
@@ -150,6 +152,7 @@ typedef struct {
   int eig_iterations;       /* power iterations of the per-level lmax estimate (20)            */
   int restart;              /* FGMRES directions per cycle, 1..64 (30)                         */
   double coarse_lmax;       /* the first level with lmax <= this is the coarsest (25)          */
+  int poly_degree;          /* degree of the AF_SCHUR_CHEB_* polynomial preconditioner (16)    */
 } af_schur_options;
 typedef struct {
   int iterations;           /* FGMRES iterations of the last solve                             */

@@ -46,7 +46,7 @@ def test_imex_steps_match_oracle(P, nsteps, mesh, exact):
     assert rel(p, p_ref) < STATE_TOL
 
 
-@pytest.mark.parametrize("pc", ["jacobi", "mg_fp64", "mg_fp32"])
+@pytest.mark.parametrize("pc", ["jacobi", "mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32"])
 def test_imex_schur_solver_options_match_oracle(pc):
     """The pressure system solved by af_schur_solve (FGMRES on the true residual, Jacobi or
     multigrid preconditioning with FP64 or FP32 levels) instead of the reference's

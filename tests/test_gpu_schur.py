@@ -4,7 +4,8 @@
    oracle's operator matrices (box mesh, constant coefficients, so the wave-speed term of C
    vanishes and the operator is linear): FP64 levels agree to 1e-12 relative, FP32 levels to
    1e-4.
-2. FGMRES with each preconditioner (Jacobi, FP64 and FP32 multigrid) solves S x = S x_true
+2. FGMRES with each preconditioner (Jacobi, FP64 and FP32 multigrid, FP64 and FP32 Chebyshev
+   polynomial) solves S x = S x_true
    on a hill mesh to a true residual of 1e-10; the solution matches x_true and its residual,
    recomputed by the oracle's Schur apply on the CPU, is below 1e-9.
 """
@@ -152,7 +153,7 @@ def test_schur_solve_all_preconditioners():
     o.set_pres_fixed(st.p)
     o.set_NS_stage(2)
     its = {}
-    for pc in ("jacobi", "mg_fp64", "mg_fp32"):
+    for pc in ("jacobi", "mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32"):
         s = SchurSolver(op, pc)
         s.setup()
         x = torch.zeros_like(b)
@@ -163,5 +164,6 @@ def test_schur_solve_all_preconditioners():
         assert out["final_residual"] <= 1e-10 * np.linalg.norm(bh) * (1 + 1e-6)
         assert rel(xh, xt) < 1e-8, pc
         assert rel(o.vmult(xh), bh) < 1e-9, pc
-    # the multigrid preconditioners take far fewer iterations than Jacobi
-    assert its["mg_fp64"] * 2 < its["jacobi"] and its["mg_fp32"] * 2 < its["jacobi"], its
+    # the multigrid and polynomial preconditioners take far fewer iterations than Jacobi
+    for pc in ("mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32"):
+        assert its[pc] * 2 < its["jacobi"], its
