@@ -1,7 +1,7 @@
 """Benchmark: GDoF/s of the Euler operator explicit apply (fused stage-1 right-hand side
 triple: density, velocity, pressure) on the 2D terrain-following 512x256 mesh, degree 4, FP64.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-sweep]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-sweep] [--no-solvers]
 
 One step = one fused apply over the whole mesh with inputs resident in HBM (`value`);
 `e2e` is the same apply through the host-buffer C-ABI call (pinned host inputs copied in,
@@ -11,6 +11,8 @@ N > 1: one process per GPU (torchrun), independent replicas ("replicas only": th
 operator apply has no cross-GPU exchange in this library), max time over ranks.
 --impl reference: the CPU restatement of the reference operators (the reference itself
 needs deal.II, which is not installable here) on the host cores, same metric.
+Rank 0 also reports the second half of the metric (`imex`: s per IMEX step, FP64 vs mixed
+precision at the same solver tolerance) and the Schur pressure solve (`schur_solve`).
 """
 import argparse
 import json
@@ -198,6 +200,90 @@ def time_device(op, bufs, src, stream, K, W):
     return e0.elapsed_time(e1) * 1e-3 / K
 
 
+def run_solvers(dev):
+    """The second half of the metric, s per IMEX step FP64 vs mixed at the same tolerance, and
+    the Schur pressure solve those steps are made of (device time, CUDA events)."""
+    import torch
+    from atmospheric_flows_b200 import mesh as M
+    from atmospheric_flows_b200.imex import IMEXStepper
+    from atmospheric_flows_b200.operator import EULEROperator
+    from atmospheric_flows_b200.schur import SchurSolver
+    sc = M.Scaling()
+    P = DEGREE
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    out = {}
+    # ---- Schur pressure solve: 1024x256 hill mesh, degree 4, seeded smooth rhs, rel. residual 1e-10
+    nx, nz, dt = 1024, 256, 0.5
+    m = M.hill_mesh(nx, nz)
+    st = M.hill_state(m, P, seed=SEED, modes=4)
+    rhs = M.hill_state(m, P, seed=SEED + 7, modes=8, amplitude=1e-2).p - 1.0
+    op = EULEROperator(m, P, sc.Ma, sc.Fr, dt)
+    op.set_stream(torch.cuda.current_stream(dev))
+    op.set_schur_mode(1)
+    op.set_HYPERBOLIC_stage(1)
+    op.set_rho_for_fixed(d(st.rho))
+    op.set_pres_fixed(d(st.p))
+    b = d(rhs)
+    sol = {}
+    res = {}
+    for pc in ("jacobi", "mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32"):
+        s = SchurSolver(op, pc)
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        s.setup()
+        torch.cuda.synchronize(dev)
+        t_setup = time.perf_counter() - t
+        for _ in range(2):  # the second solve is timed (first includes lazy allocations)
+            x = torch.zeros_like(b)
+            r = s.solve(x, b, rel_tol=1e-10, max_iterations=5000)
+        sol[pc] = x
+        res[pc] = {"iterations": r["iterations"], "solve_s": r["seconds"], "setup_s": t_setup,
+                   "levels": len(s.levels())}
+        del s
+    for pc in res:
+        res[pc]["rel_error_vs_fp64_jacobi"] = float(torch.linalg.norm(sol[pc] - sol["jacobi"]) /
+                                                    torch.linalg.norm(sol["jacobi"]))
+    out["schur_solve"] = {
+        "config": f"(D - C A^-1 B) p = b on the hill mesh {nx}x{nz}, degree {P} ({m.n_cells * (P + 1) ** 2} pressure "
+                  f"DoFs), dt={dt} s, seeded smooth rhs, FGMRES(30) to |b - S p| <= 1e-10 |b|",
+        "results": res,
+        "speedup_cheb_fp32_vs_fp64_jacobi": res["jacobi"]["solve_s"] / res["cheb_fp32"]["solve_s"],
+        "speedup_mg_fp32_vs_mg_fp64": res["mg_fp64"]["solve_s"] / res["mg_fp32"]["solve_s"],
+    }
+    del op, sol, b
+    # ---- IMEX steps: periodic hill 512x256, degree 4, dt 0.5 s, eps 1e-8
+    nx, nz, dt, nsteps = 512, 256, 0.5, 3
+    m = M.hill_mesh(nx, nz, periodic_x=True)
+    st = M.hill_state(m, P, seed=SEED, modes=4)
+    steps = {}
+    states = {}
+    for name, pc in (("fp64", "jacobi"), ("mixed", "cheb_fp32"), ("reference_criterion", -1)):
+        g = IMEXStepper(m, P, sc.Ma, sc.Fr, dt, schur_preconditioner=pc)
+        g.set_state(d(st.rho), d(st.u), d(st.p))
+        g.step(1)  # warm-up step
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.step(nsteps)
+        e1.record()
+        e1.synchronize()
+        steps[name] = {"s_per_step": e0.elapsed_time(e1) * 1e-3 / nsteps, "stats_last_step": g.stats()}
+        states[name] = [t.clone() for t in g.get_state()]
+        del g
+    for name in ("mixed", "reference_criterion"):
+        steps[name]["rel_error_vs_fp64"] = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+                                               for a, b in zip(states[name], states["fp64"]))
+    out["imex"] = {
+        "config": f"periodic hill {nx}x{nz}, degree {P}, dt={dt} s, eps=1e-8, 1 warm-up + {nsteps} timed steps; "
+                  "fp64: Schur FGMRES + Jacobi (FP64); mixed: Schur FGMRES (FP64) + FP32 Chebyshev polynomial "
+                  "preconditioner, both to |b - S p| <= eps |b|; reference_criterion: the reference's left-Jacobi "
+                  "GMRES stopping on |D^-1 r| <= eps |b| (a looser criterion, shown for scale)",
+        "results": steps,
+        "speedup_mixed_vs_fp64": steps["fp64"]["s_per_step"] / steps["mixed"]["s_per_step"],
+    }
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -301,6 +387,7 @@ def run_ours(args, rank, world, local_rank):
                 sweep[str(Pd)] = {"gdofs": 4 * nsd / td / 1e9, "us_per_apply": td * 1e6,
                                   "hbm_frac": 8 * nsd * 11 / td / 1e9 / peak}
                 del opd, sd, bd
+        solvers = {} if args.no_solvers else run_solvers(dev)
         threads = os.cpu_count() or 1
         cpu_v, cpu_m = cpu_baseline_oracle(64, 3, threads)
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
@@ -314,7 +401,7 @@ def run_ours(args, rank, world, local_rank):
                 "clocks": clk.summary(),
                 "cpu_baseline": {"value": cpu_v, "unit": "GDoF/s", "cores": threads, "kind": "port",
                                  "sample": f"{NX}x64 strip of the workload mesh, best of 3 (1/4 of the work)"},
-                "degree_sweep": sweep}
+                "degree_sweep": sweep, **solvers}
         print(json.dumps(line), flush=True)
     return line
 
@@ -326,6 +413,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-solvers", action="store_true", help="skip the Schur-solve and IMEX-step measurements")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
