@@ -56,11 +56,18 @@ def lib():
         L.af_last_inner_iterations.argtypes = [vp, ctypes.POINTER(ip)]
         L.af_n_dofs.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_longlong)]
         L.af_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.af_compute_diagnostics.argtypes = [vp, dp, dp, dp, dp, ctypes.POINTER(Diagnostics)]
+        L.af_l2_norm.argtypes = [vp, ip, dp, ctypes.POINTER(ctypes.c_double)]
         L.af_error_string.restype = ctypes.c_char_p
         L.af_error_string.argtypes = [ip]
         L.af_last_error_message.restype = ctypes.c_char_p
         _lib = L
     return _lib
+
+
+class Diagnostics(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("max_velocity", "min_density", "max_density", "max_celerity",
+                                                "min_cell_diameter", "cfl_c", "cfl_u")]
 
 
 def check(status):
@@ -197,6 +204,19 @@ class EULEROperator:
 
     def compute_diagonal(self, dst):
         check(lib().af_compute_diagonal(self._h, _ptr(dst)))
+
+    # --- diagnostics (Atmospheric_Flow.cc:925-1087) ---
+    def compute_diagnostics(self, rho, u, p, rho_stage=None):
+        """max |u|, min/max density, max celerity, min cell diameter and Courant numbers."""
+        d = Diagnostics()
+        check(lib().af_compute_diagnostics(self._h, _ptr(rho), _ptr(rho_stage), _ptr(u), _ptr(p), ctypes.byref(d)))
+        return {k: getattr(d, k) for k, _ in Diagnostics._fields_}
+
+    def l2_norm(self, v, ncomp=1):
+        """L2 norm of a field over the mesh by QGauss(p+1) (integrate_difference's norm)."""
+        out = ctypes.c_double()
+        check(lib().af_l2_norm(self._h, ncomp, _ptr(v), ctypes.byref(out)))
+        return out.value
 
     def set_schur_mode(self, mode=0, rel_tol=1e-12, max_iter=10000):
         check(lib().af_set_schur_mode(self._h, mode, rel_tol, max_iter))

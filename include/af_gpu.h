@@ -226,6 +226,45 @@ int af_schur_apply_noalloc(int nx, int nz, int periodic_x, const double* vertice
                            int hyperbolic_stage, const double* rho_for_fixed, const double* pres_fixed,
                            const double* src, double* dst, void* stream, int* inner_iterations);
 
+/* ---------------------------------------------------------------- diagnostics
+ * The reference's time-loop diagnostics (Atmospheric_Flow.cc:991-1087, 1224-1235), which it
+ * evaluates at QGaussLobatto(p+1) = the DG support points: max |u| (get_max_velocity),
+ * min / max density (get_min_density / get_max_density, taken from the current stage's
+ * density: pass it as rho_stage, or NULL to use rho), max sqrt(gamma p / rho)
+ * (compute_max_celerity, from rho and p), the minimal cell diameter (longer diagonal of the
+ * mapped cell, GridTools::minimal_cell_diameter) and the Courant numbers
+ * CFL_c = dt max_celerity / Ma * degree sqrt(2) / d_min, CFL_u = dt max|u| degree sqrt(2) / d_min.
+ * DEVICE vectors; synchronises the operator's stream. */
+typedef struct {
+  double max_velocity, min_density, max_density, max_celerity, min_cell_diameter, cfl_c, cfl_u;
+} af_diagnostics;
+int af_compute_diagnostics(af_operator* op, const double* rho, const double* rho_stage, const double* u,
+                           const double* p, af_diagnostics* out);
+/* L2 norm over the mesh of a DEVICE field with ncomp (1 or 2) components per cell, by
+ * QGauss(p+1) as the reference's integrate_difference(..., L2_norm) in analyze_results
+ * (Atmospheric_Flow.cc:925-985); the difference to a reference field is the caller's. */
+int af_l2_norm(af_operator* op, int ncomp, const double* v, double* norm);
+
+/* ---------------------------------------------------------------- state files and VTU output
+ * HOST arrays; no GPU needed.  af_io_write_vtu writes what the reference's output_results
+ * (Atmospheric_Flow.cc:886-918) writes in 2D: each cell subdivided into degree x degree
+ * quadrilaterals at equispaced reference points (DataOut::build_patches with n_subdivisions =
+ * degree), fields rho, u, p interpolated there, ASCII .vtu.  af_io_write_state /
+ * af_io_read_state: a binary restart file (mesh, degree, time, step, rho, u, p) with no
+ * counterpart in the reference (it has no restart). */
+typedef struct {
+  int nx, nz, degree, periodic_x, gravity;
+  double radial_a, time;
+  long long step;
+} af_state_header;
+int af_io_write_state(const char* path, const af_mesh_desc* mesh, int degree, double time, long long step,
+                      const double* rho, const double* u, const double* p);
+int af_io_read_state_header(const char* path, af_state_header* header);
+/* vertices: (nz+1)(nx+1)2, rho and p: n, u: 2n doubles, n = nx nz (degree+1)^2 */
+int af_io_read_state(const char* path, double* vertices, double* rho, double* u, double* p);
+int af_io_write_vtu(const char* path, const af_mesh_desc* mesh, int degree, const double* rho, const double* u,
+                    const double* p);
+
 /* Measures the FP64 FMA throughput of the current device (TFLOP/s) with a short
  * dependent-chain kernel; the denominator of the FP64 roofline the benchmark reports.
  * No counterpart in the reference. */
