@@ -39,6 +39,20 @@ struct MeshDev {
 
 struct PointGeo {
   double X[2];  // physical position (valid when Phys::NEED_X)
+  double J[4];  // Jacobian (x_xi, x_eta, z_xi, z_eta) (valid for policies with gradient fields)
+};
+
+// Policies may declare "gradient fields": the last nfg_of(G) cell fields of group G, whose
+// reference-coordinate derivatives at the quadrature points are passed to their point
+// function as well (point<G>(prm, v, deta, pg, val, gr): v holds the group's values, then
+// d/dxi of the gradient fields; deta holds their d/deta).  Policies without nfg_of have none.
+template <class Phys, class = void>
+struct NfgOf {
+  static constexpr int get(int) { return 0; }
+};
+template <class Phys>
+struct NfgOf<Phys, std::void_t<decltype(Phys::nfg_of(0))>> {
+  static constexpr int get(int g) { return Phys::nfg_of(g); }
 };
 
 template <int N, class F, int... I>
@@ -121,6 +135,7 @@ struct GroupInfo {
     for (int a = 0; a < NARR; ++a) n += Phys::template Grp<G>::ncomp(a);
     return n;
   }();
+  static constexpr int NF_GRAD = NfgOf<Phys>::get(G);  // the last NF_GRAD cell fields
   static constexpr int NF_CELL = [] {  // fields used by cell integrals (face-only ones last)
     int n = 0;
     for (int a = 0; a < NARR; ++a)
@@ -142,14 +157,26 @@ struct PhysInfo {
     return n;
   }();
   // cell fields (all groups) evaluated together in the merged z pass
+  // x-contracted slots: per group its cell fields (S rows), then its gradient fields again
+  // (D rows, for d/dxi)
   static constexpr int NFC_TOTAL = [] {
     int n = 0;
-    for (int g = 0; g < Phys::NG; ++g) n += Phys::nfc_of(g);
+    for (int g = 0; g < Phys::NG; ++g) n += Phys::nfc_of(g) + NfgOf<Phys>::get(g);
     return n;
   }();
   static constexpr int eo_offset(int G) {
     int n = 0;
-    for (int g = 0; g < G; ++g) n += Phys::nfc_of(g);
+    for (int g = 0; g < G; ++g) n += Phys::nfc_of(g) + NfgOf<Phys>::get(g);
+    return n;
+  }
+  static constexpr int NFG_TOTAL = [] {
+    int n = 0;
+    for (int g = 0; g < Phys::NG; ++g) n += NfgOf<Phys>::get(g);
+    return n;
+  }();
+  static constexpr int grad_offset(int G) {
+    int n = 0;
+    for (int g = 0; g < G; ++g) n += NfgOf<Phys>::get(g);
     return n;
   }
 };
@@ -212,6 +239,32 @@ __device__ __forceinline__ void contract_eo(const R* r, R* y) {
   for (int i = 0; i < T::H; ++i) e = fmaR(t.Se[P][i], re[i], e);
   if (T::MIDN) e = fmaR(t.Sm[P], rm, e);
   y[P] = e;
+}
+
+// derivative counterpart: y[q] = sum_i D[q][i] r[i] with D[NQ-1-q][i] = -D[q][P-i]
+template <int P, class R>
+__device__ __forceinline__ void contract_eo_D(const R* r, R* y) {
+  using T = TabT<P, R>;
+  const T& t = tabr<P, R>();
+  R re[T::H > 0 ? T::H : 1], ro[T::H > 0 ? T::H : 1];
+#pragma unroll
+  for (int i = 0; i < T::H; ++i) {
+    re[i] = r[i] + r[P - i];
+    ro[i] = r[i] - r[P - i];
+  }
+  const R rm = T::MIDN ? r[P / 2] : R(0);
+#pragma unroll
+  for (int k = 0; k <= P; ++k) {
+    R e = 0.0, o = 0.0;
+#pragma unroll
+    for (int i = 0; i < T::H; ++i) {
+      e = fmaR(t.De[k][i], re[i], e);
+      o = fmaR(t.Do[k][i], ro[i], o);
+    }
+    if (T::MIDN) e = fmaR(t.Dm[k], rm, e);
+    y[k] = e + o;
+    if (k < P) y[T::NQ - 1 - k] = o - e;
+  }
 }
 
 // ----------------------------------------------------------------------------------
@@ -332,29 +385,37 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     }
     cp_async_wait_all();
     __syncthreads();
-    // ---- X pass: rows (k, P-k) even/odd, contracted along x, for the cell fields
+    // ---- X pass: rows (k, P-k) even/odd, contracted along x, for the cell fields (S) and
+    //      again for the gradient fields (D, slots NFC..NFC+NFG-1)
     {
       constexpr int NPR = H + (MIDN ? 1 : 0);
-      for (int task = m; task < NFC * NPR; task += NQ) {
+      constexpr int NFG = Gi::NF_GRAD;
+      for (int task = m; task < (NFC + NFG) * NPR; task += NQ) {
         const int fi = task / NPR, k = task % NPR;
-        const R* cell = s_in + (fi * CB + cl) * L::NDP;
+        const bool dxi = NFG > 0 && fi >= NFC;
+        const int src = dxi ? fi - NFG : fi;  // gradient fields are the last NFG cell fields
+        const R* cell = s_in + (src * CB + cl) * L::NDP;
         R* eo = s_eo + ((EOFF + fi) * CB + cl) * L::EOS;
         R r[P1], y[NQ];
+        auto contract = [&]() {
+          if (NFG > 0 && dxi) contract_eo_D<P>(r, y);
+          else contract_eo<P>(r, y);
+        };
         if (k < H) {
 #pragma unroll
           for (int ix = 0; ix < P1; ++ix) r[ix] = cell[k * P1 + ix] + cell[(P - k) * P1 + ix];
-          contract_eo<P>(r, y);
+          contract();
 #pragma unroll
           for (int q = 0; q < NQ; ++q) eo[k * NQ + q] = y[q];
 #pragma unroll
           for (int ix = 0; ix < P1; ++ix) r[ix] = cell[k * P1 + ix] - cell[(P - k) * P1 + ix];
-          contract_eo<P>(r, y);
+          contract();
 #pragma unroll
           for (int q = 0; q < NQ; ++q) eo[(H + k) * NQ + q] = y[q];
         } else {
 #pragma unroll
           for (int ix = 0; ix < P1; ++ix) r[ix] = cell[(P / 2) * P1 + ix];
-          contract_eo<P>(r, y);
+          contract();
 #pragma unroll
           for (int q = 0; q < NQ; ++q) eo[(2 * H) * NQ + q] = y[q];
         }
@@ -415,7 +476,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     const R wx = s_w[qx];
     const R J01 = fmaR(g[2], xi, g[4]);  // x_eta (x component)
     const R J11 = fmaR(g[3], xi, g[5]);  // x_eta (z component)
-    auto point = [&](const R* v, const int qz) {
+    constexpr int NFG_ALL = PhysInfo<Phys>::NFG_TOTAL;
+    auto point = [&](const R* v, const R* deta, const int qz) {
       const R eta = tb.x[qz];
       const R J00 = fmaR(g[2], eta, g[0]);
       const R J10 = fmaR(g[3], eta, g[1]);
@@ -426,12 +488,19 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         pg.X[0] = g[6] + g[0] * xi + g[4] * eta + g[2] * xi * eta;
         pg.X[1] = g[7] + g[1] * xi + g[5] * eta + g[3] * xi * eta;
       }
+      if constexpr (NFG_ALL > 0) {
+        pg.J[0] = J00; pg.J[1] = J01; pg.J[2] = J10; pg.J[3] = J11;
+      }
       R val[NOUT], gr[NOUT][2];
 #pragma unroll
       for (int o = 0; o < NOUT; ++o) { val[o] = 0.0; gr[o][0] = gr[o][1] = 0.0; }
       sfor<Phys::NG>([&](auto gc) {
         constexpr int G = decltype(gc)::value;
-        Phys::template point<G>(prm, v + PhysInfo<Phys>::eo_offset(G), pg, val, gr);
+        if constexpr (NFG_ALL > 0)
+          Phys::template point<G>(prm, v + PhysInfo<Phys>::eo_offset(G), deta + PhysInfo<Phys>::grad_offset(G), pg,
+                                  val, gr);
+        else
+          Phys::template point<G>(prm, v + PhysInfo<Phys>::eo_offset(G), pg, val, gr);
       });
       const R a00 = J11 * w, a01 = J01 * w, a10 = J10 * w, a11 = J00 * w;  // adj(J) w
 #pragma unroll
@@ -467,8 +536,31 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         v1[fi] = e + o;
         v2[fi] = e - o;
       }
-      point(v1, k);
-      if (pair) point(v2, NQ - 1 - k);
+      // d/deta of the gradient fields: their S-row slots contracted with D along z
+      R d1[NFG_ALL > 0 ? NFG_ALL : 1], d2[NFG_ALL > 0 ? NFG_ALL : 1];
+      if constexpr (NFG_ALL > 0) {
+        sfor<Phys::NG>([&](auto gc) {
+          constexpr int G = decltype(gc)::value;
+          using Gi = GroupInfo<Phys, G>;
+          constexpr int NFG = Gi::NF_GRAD;
+#pragma unroll
+          for (int kk = 0; kk < NFG; ++kk) {
+            const int slot = PhysInfo<Phys>::eo_offset(G) + Gi::NF_CELL - NFG + kk;
+            const R* eo = s_eo + (slot * CB + cl) * L::EOS + qx;
+            R e = 0.0, o = 0.0;
+#pragma unroll
+            for (int i = 0; i < H; ++i) {
+              e = fmaR(tb.De[k][i], eo[i * NQ], e);
+              o = fmaR(tb.Do[k][i], eo[(H + i) * NQ], o);  // at the middle point only o remains
+            }
+            if (MIDN) e = fmaR(tb.Dm[k], eo[(2 * H) * NQ], e);
+            d1[PhysInfo<Phys>::grad_offset(G) + kk] = e + o;
+            d2[PhysInfo<Phys>::grad_offset(G) + kk] = o - e;
+          }
+        });
+      }
+      point(v1, d1, k);
+      if (pair) point(v2, d2, NQ - 1 - k);
     }
   }
   __syncthreads();  // region A: x-contracted rows consumed -> accumulators

@@ -71,6 +71,14 @@ struct DegreeOps {
   cudaError_t (*restrict_f)(const float* rf, float* rc, int nxc, int nzc, cudaStream_t);
   // coarse nodal values of a fine coefficient field (injection from the child cell)
   cudaError_t (*inject)(const double* ff, double* fc, int nxc, int nzc, cudaStream_t);
+
+  // adjoint of the fused stage-1 rhs triple: in = rho0 u0 p0 rho2 u_fixed, ybar = cotangents of
+  // the rho, u, p outputs, xbar = cotangents of the five inputs (overwritten)
+  cudaError_t (*rhs_adjoint1)(const MeshDev&, const double* const* in, const double* const* ybar, double* const* xbar,
+                              const RhsParams&, int ncell, cudaStream_t);
+  // its tangent-linear: dy (rho, u, p) = J(in) din
+  cudaError_t (*rhs_tangent1)(const MeshDev&, const double* const* in, const double* const* din, double* const* dy,
+                              const RhsParams&, int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

@@ -3,6 +3,7 @@
 // the C ABI (af_capi.cu).
 #include <cstdio>
 
+#include "af_adjoint.cuh"
 #include "af_internal.h"
 
 #ifndef AF_P
@@ -505,6 +506,21 @@ __global__ void k_inject(const double* __restrict__ ff, double* __restrict__ fc,
   fc[idx] = s;
 }
 
+// ------------------------------------------------------------------ adjoint
+constexpr int kAdjCells = P <= 2 ? 16 : 8;
+cudaError_t rhs_adjoint1(const MeshDev& mesh, const double* const* in, const double* const* ybar,
+                         double* const* xbar, const RhsParams& prm, int ncell, cudaStream_t st) {
+  ArgPtrs<8, 5> a{{in[0], in[1], in[2], in[3], in[4], ybar[0], ybar[1], ybar[2]},
+                  {xbar[0], xbar[1], xbar[2], xbar[3], xbar[4]}};
+  return launch_cellop<P, RhsAdj1Phys, kAdjCells, 2>(mesh, a, prm, ncell, st);
+}
+
+cudaError_t rhs_tangent1(const MeshDev& mesh, const double* const* in, const double* const* din, double* const* dy,
+                         const RhsParams& prm, int ncell, cudaStream_t st) {
+  ArgPtrs<10, 3> a{{in[0], in[1], in[2], in[3], in[4], din[0], din[1], din[2], din[3], din[4]}, {dy[0], dy[1], dy[2]}};
+  return launch_cellop<P, RhsTlm1Phys, kAdjCells, 2>(mesh, a, prm, ncell, st);
+}
+
 constexpr int kTransferThreads = 256;
 
 template <class R>
@@ -535,7 +551,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         cheb<double>,      cheb<float>,
                         prolong<double>,   prolong<float>,
                         restrict_<double>, restrict_<float>,
-                        inject};
+                        inject,            rhs_adjoint1,
+                        rhs_tangent1};
 
 }  // namespace
 

@@ -49,6 +49,8 @@ def lib():
             getattr(L, name).argtypes = [vp, dp, ctypes.POINTER(dp), ip]
         L.af_vmult_rhs_fused.argtypes = [vp, dp, dp, dp, ctypes.POINTER(dp), ip]
         L.af_vmult_rhs_fused_host.argtypes = [vp, dp, dp, dp, ctypes.POINTER(dp), ip]
+        L.af_vmult_rhs_fused_backward.argtypes = [vp, ctypes.POINTER(dp), ip, dp, dp, dp, ctypes.POINTER(dp)]
+        L.af_vmult_rhs_fused_tangent.argtypes = [vp, ctypes.POINTER(dp), ip, ctypes.POINTER(dp), dp, dp, dp]
         for name in ("af_vmult", "af_vmult_pressure", "af_vmult_enthalpy", "af_vmult_inverse"):
             getattr(L, name).argtypes = [vp, dp, dp]
         L.af_compute_diagonal.argtypes = [vp, dp]
@@ -187,6 +189,17 @@ class EULEROperator:
         arr = (ctypes.c_void_p * len(src))(*[s.ctypes.data for s in src])
         p = lambda a: None if a is None else ctypes.c_void_p(a.ctypes.data)
         check(lib().af_vmult_rhs_fused_host(self._h, p(dst_rho), p(dst_u), p(dst_p), arr, len(src)))
+
+    # --- forward / backward pair of the fused stage-1 rhs (autograd-style) ---
+    def vmult_rhs_fused_backward(self, src, ybar_rho, ybar_u, ybar_p, xbar):
+        """xbar[k] = (d rhs / d src[k])^T ybar for the five stage-1 sources (overwritten)."""
+        check(lib().af_vmult_rhs_fused_backward(self._h, _ptr_array(src), len(src), _ptr(ybar_rho), _ptr(ybar_u),
+                                                _ptr(ybar_p), _ptr_array(xbar)))
+
+    def vmult_rhs_fused_tangent(self, src, dsrc, d_rho, d_u, d_p):
+        """(d_rho, d_u, d_p) = (d rhs / d src) dsrc."""
+        check(lib().af_vmult_rhs_fused_tangent(self._h, _ptr_array(src), len(src), _ptr_array(dsrc), _ptr(d_rho),
+                                               _ptr(d_u), _ptr(d_p)))
 
     # --- implicit operators ---
     def vmult(self, dst, src):
