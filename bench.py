@@ -387,6 +387,29 @@ def run_ours(args, rank, world, local_rank):
                 sweep[str(Pd)] = {"gdofs": 4 * nsd / td / 1e9, "us_per_apply": td * 1e6,
                                   "hbm_frac": 8 * nsd * 11 / td / 1e9 / peak}
                 del opd, sd, bd
+        # ---- tangent and backward of the same apply (device-resident, same inputs)
+        rng = np.random.default_rng(SEED + 3)
+        dsrc = [torch.from_numpy(rng.standard_normal(a.size)).to(dev) for a in src_h]
+        ybar = [torch.from_numpy(rng.standard_normal(k * ns)).to(dev) for k in (1, 2, 1)]
+        xbar = [torch.empty(a.size, dtype=torch.float64, device=dev) for a in src_h]
+        dy = [torch.empty(k * ns, dtype=torch.float64, device=dev) for k in (1, 2, 1)]
+
+        def timed(fn, K=10, W=3):
+            for _ in range(W):
+                fn()
+            stream.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(K):
+                fn()
+            a1.record(stream)
+            a1.synchronize()
+            return a0.elapsed_time(a1) * 1e-3 / K
+        t_tan = timed(lambda: op.vmult_rhs_fused_tangent(src, dsrc, *dy))
+        t_bwd = timed(lambda: op.vmult_rhs_fused_backward(src, *ybar, xbar))
+        autodiff = {"forward_ms": t_step * 1e3, "tangent_ms": t_tan * 1e3, "backward_ms": t_bwd * 1e3,
+                    "backward_over_forward": t_bwd / t_step,
+                    "note": "af_vmult_rhs_fused_tangent / _backward on the bench workload (one launch each)"}
         solvers = {} if args.no_solvers else run_solvers(dev)
         threads = os.cpu_count() or 1
         cpu_v, cpu_m = cpu_baseline_oracle(64, 3, threads)
@@ -401,7 +424,7 @@ def run_ours(args, rank, world, local_rank):
                 "clocks": clk.summary(),
                 "cpu_baseline": {"value": cpu_v, "unit": "GDoF/s", "cores": threads, "kind": "port",
                                  "sample": f"{NX}x64 strip of the workload mesh, best of 3 (1/4 of the work)"},
-                "degree_sweep": sweep, **solvers}
+                "degree_sweep": sweep, "autodiff": autodiff, **solvers}
         print(json.dumps(line), flush=True)
     return line
 
