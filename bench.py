@@ -429,6 +429,48 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def run_profile_case(kind):
+    """A short run of one workload for ncu captures (no timing, no JSON): 'rhs' the fused
+    stage-1 apply, 'adjoint' its tangent and backward, 'schur' the FP32 multigrid setup and
+    one V-cycle on the 1024x256 pressure system."""
+    import torch
+    from atmospheric_flows_b200 import mesh as M
+    from atmospheric_flows_b200.operator import EULEROperator
+    sc = M.Scaling()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    if kind in ("rhs", "adjoint"):
+        m, src_h = workload(DEGREE, modes=2)
+        op = EULEROperator(m, DEGREE, sc.Ma, sc.Fr, 2.0)
+        op.set_stream(torch.cuda.current_stream())
+        op.set_HYPERBOLIC_stage(1)
+        ns = m.n_cells * (DEGREE + 1) ** 2
+        src = [d(a) for a in src_h]
+        dy = [torch.empty(k * ns, dtype=torch.float64, device="cuda") for k in (1, 2, 1)]
+        for _ in range(2):
+            op.vmult_rhs_fused(*dy, src)
+        if kind == "adjoint":
+            yb = [d(np.random.default_rng(1).standard_normal(k * ns)) for k in (1, 2, 1)]
+            xb = [torch.empty_like(a) for a in src]
+            op.vmult_rhs_fused_tangent(src, src, *dy)
+            op.vmult_rhs_fused_backward(src, *yb, xb)
+    else:
+        from atmospheric_flows_b200.schur import SchurSolver
+        m = M.hill_mesh(1024, 256)
+        st = M.hill_state(m, DEGREE, modes=2)
+        op = EULEROperator(m, DEGREE, sc.Ma, sc.Fr, 0.5)
+        op.set_stream(torch.cuda.current_stream())
+        op.set_schur_mode(1)
+        op.set_HYPERBOLIC_stage(1)
+        op.set_rho_for_fixed(d(st.rho))
+        op.set_pres_fixed(d(st.p))
+        op.set_NS_stage(2)
+        s = SchurSolver(op, "mg_fp32", smoother_degree=5)
+        s.setup()
+        z = torch.empty(m.n_cells * (DEGREE + 1) ** 2, dtype=torch.float64, device="cuda")
+        s.precondition(z, d(st.p))
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -437,7 +479,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-solvers", action="store_true", help="skip the Schur-solve and IMEX-step measurements")
+    ap.add_argument("--profile", choices=["rhs", "adjoint", "schur"],
+                    help="run one workload briefly for an ncu capture and exit (no measurement)")
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args.profile)
+        return
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
