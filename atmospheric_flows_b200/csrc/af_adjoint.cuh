@@ -262,4 +262,145 @@ struct RhsTlm1Phys {
   }
 };
 
+// ------------------------------------------------------------- implicit operators
+// B^T (vmult_pressure transposed, euler_operator.h:1512-1617): pbar = B^T ubar.
+//   cell:  (B p)_{i,d} = -c int p d_d psi_i  ->  pbar_j = -c int phi_j div(ubar_h)
+//   face:  c {p} n.psi  -> own side c/2 n, so  pbar += c/2 (ubar+ - ubar-).n
+//   wall:  c p n.psi    ->  pbar += c ubar+.n
+struct BTPhys {
+  static constexpr int NG = 1;
+  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = 1;
+  using Params = BParams;
+  using real = double;
+  static constexpr int out_ncomp(int) { return 1; }
+  static constexpr bool has_val(int) { return true; }
+  static constexpr bool has_grad(int) { return false; }
+  static constexpr int narr_of(int) { return 1; }
+  static constexpr int nf_of(int) { return 2; }
+  static constexpr int nfc_of(int) { return 2; }
+  static constexpr int nfg_of(int) { return 2; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = 1;
+    static constexpr bool FACE = true;
+    static constexpr int ncomp(int) { return 2; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const double* deta,
+                                               const PointGeo& pg, double* val, double (*)[2]) {
+    const double J00 = pg.J[0], J01 = pg.J[1], J10 = pg.J[2], J11 = pg.J[3];
+    const double idet = 1.0 / (J00 * J11 - J01 * J10);
+    const double dxux = (J11 * v[2] - J10 * deta[0]) * idet;  // d ubar_x / dx
+    const double dzuz = (J00 * deta[1] - J01 * v[3]) * idet;  // d ubar_z / dz
+    val[0] += -prm.c * (dxux + dzuz);
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    flux[0] = prm.c * 0.5 * ((vp[0] - vm[0]) * n[0] + (vp[1] - vm[1]) * n[1]);
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
+                                                  double* flux) {
+    flux[0] = prm.c * (vp[0] * n[0] + vp[1] * n[1]);
+  }
+};
+
+// Jacobian of C (vmult_enthalpy, euler_operator.h:1413-1507) at w, applied to dw; the
+// wave speed lambda(w) is differentiated along the forward's branch.
+//   cell:  -cdt gg p_f dw . grad phi
+//   face:  cdt (gg/2 (p_f+ dw+.n + p_f- dw-.n) + g1/2 dlambda (p_f+ - p_f-))
+// One group: w (2), dw (2), p_f.  Output: a pressure-space field.
+struct CTlmPhys {
+  static constexpr int NG = 1;
+  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = 1;
+  using Params = CParams;
+  using real = double;
+  static constexpr int out_ncomp(int) { return 1; }
+  static constexpr bool has_val(int) { return false; }
+  static constexpr bool has_grad(int) { return true; }
+  static constexpr int narr_of(int) { return 3; }
+  static constexpr int nf_of(int) { return 5; }
+  static constexpr int nfc_of(int) { return 5; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = 3;
+    static constexpr bool FACE = true;
+    static constexpr int ncomp(int a) { return a < 2 ? 2 : 1; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo&, double*,
+                                               double (*gr)[2]) {
+    const double s = -prm.cdt * prm.gg * v[4];
+    gr[0][0] += s * v[2];
+    gr[0][1] += s * v[3];
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    const double wnp = vp[0] * n[0] + vp[1] * n[1], wnm = vm[0] * n[0] + vm[1] * n[1];
+    const double dwnp = vp[2] * n[0] + vp[3] * n[1], dwnm = vm[2] * n[0] + vm[3] * n[1];
+    const bool own = fabs(wnp) >= fabs(wnm);
+    const double sg = own ? (wnp > 0.0 ? 1.0 : (wnp < 0.0 ? -1.0 : 0.0)) : (wnm > 0.0 ? 1.0 : (wnm < 0.0 ? -1.0 : 0.0));
+    const double dlam = sg * (own ? dwnp : dwnm);
+    flux[0] = prm.cdt * (0.5 * prm.gg * (vp[4] * dwnp + vm[4] * dwnm) + 0.5 * dlam * prm.g1 * (vp[4] - vm[4]));
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
+};
+
+// Its transpose: wbar = J_C(w)^T pbar.
+//   cell:  wbar = -cdt gg p_f grad(pbar_h) (tested with phi)
+//   face:  own-side derivative applied to the cotangent jump:
+//          wbar+ += cdt (gg/2 p_f+ n + g1/2 (p_f+ - p_f-) dlambda/dw+) (pbar+ - pbar-)
+// One group: w (2), p_f, pbar (gradient field).  Output: wbar (2).
+struct CTPhys {
+  static constexpr int NG = 1;
+  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = 2;
+  using Params = CParams;
+  using real = double;
+  static constexpr int out_ncomp(int) { return 2; }
+  static constexpr bool has_val(int) { return true; }
+  static constexpr bool has_grad(int) { return false; }
+  static constexpr int narr_of(int) { return 3; }
+  static constexpr int nf_of(int) { return 4; }
+  static constexpr int nfc_of(int) { return 4; }
+  static constexpr int nfg_of(int) { return 1; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = 3;
+    static constexpr bool FACE = true;
+    static constexpr int ncomp(int a) { return a == 0 ? 2 : 1; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const double* deta,
+                                               const PointGeo& pg, double* val, double (*)[2]) {
+    const double J00 = pg.J[0], J01 = pg.J[1], J10 = pg.J[2], J11 = pg.J[3];
+    const double idet = 1.0 / (J00 * J11 - J01 * J10);
+    const double gx = (J11 * v[4] - J10 * deta[0]) * idet, gz = (J00 * deta[0] - J01 * v[4]) * idet;
+    const double s = -prm.cdt * prm.gg * v[2];
+    val[0] += s * gx;
+    val[1] += s * gz;
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    const double wnp = vp[0] * n[0] + vp[1] * n[1], wnm = vm[0] * n[0] + vm[1] * n[1];
+    const bool own = fabs(wnp) >= fabs(wnm);
+    const double sg = own ? (wnp > 0.0 ? 1.0 : (wnp < 0.0 ? -1.0 : 0.0)) : 0.0;
+    const double jump = vp[3] - vm[3];
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+      flux[k] = prm.cdt * (0.5 * prm.gg * vp[2] * n[k] + 0.5 * prm.g1 * (vp[2] - vm[2]) * sg * n[k]) * jump;
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
+};
+
 }  // namespace af

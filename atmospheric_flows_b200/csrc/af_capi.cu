@@ -548,6 +548,85 @@ int af_launch_count(const af_operator* o, long long* n) {
   return AF_OK;
 }
 
+
+// ------------------------------------------------------------- tangents and transposes
+// of the implicit operators (no counterpart in the reference): the pieces of an adjoint
+// pressure solve.  A^{-1} is always the exact cell-wise inverse here.
+
+int af_vmult_pressure_transpose(af_operator* o, double* pbar, const double* ubar) {
+  if (!o || !pbar || !ubar) return fail(AF_BAD_ARG, "null argument");
+  if (!aligned16(pbar) || !aligned16(ubar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
+  AF_CU(cudaSetDevice(o->device));
+  AF_CU(o->ops->op_BT(o->mesh, ubar, coeff_BC(o) * o->dt / (o->Ma * o->Ma), pbar, o->ncell, o->stream));
+  o->launches += 1;
+  return AF_OK;
+}
+
+int af_vmult_enthalpy_tangent(af_operator* o, double* dst, const double* w, const double* dw) {
+  if (!o || !dst || !w || !dw) return fail(AF_BAD_ARG, "null argument");
+  if (!o->pres_fixed_set) return fail(AF_BAD_ARG, "set_pres_fixed first");
+  if (!aligned16(dst) || !aligned16(w) || !aligned16(dw)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
+  AF_CU(cudaSetDevice(o->device));
+  AF_CU(o->ops->op_C_tangent(o->mesh, w, dw, o->d_pres_fixed, c_params(o), dst, o->ncell, o->stream));
+  o->launches += 1;
+  return AF_OK;
+}
+
+int af_vmult_enthalpy_transpose(af_operator* o, double* wbar, const double* w, const double* pbar) {
+  if (!o || !wbar || !w || !pbar) return fail(AF_BAD_ARG, "null argument");
+  if (!o->pres_fixed_set) return fail(AF_BAD_ARG, "set_pres_fixed first");
+  if (!aligned16(wbar) || !aligned16(w) || !aligned16(pbar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
+  AF_CU(cudaSetDevice(o->device));
+  AF_CU(o->ops->op_CT(o->mesh, w, o->d_pres_fixed, pbar, c_params(o), wbar, o->ncell, o->stream));
+  o->launches += 1;
+  return AF_OK;
+}
+
+// w = A^{-1} B p into the workspace (2 ns), exact inverse
+static int schur_w(af_operator* o, const double* p, double* w, double* t) {
+  AF_CU(o->ops->op_B(o->mesh, p, coeff_BC(o) * o->dt / (o->Ma * o->Ma), t, o->ncell, o->stream));
+  int r = ensure_factor(o, true);
+  if (r != AF_OK) return r;
+  AF_CU(o->ops->mass_solve(o->d_La, 2, t, 1.0, w, o->ncell, o->stream));
+  o->launches += 2;
+  return AF_OK;
+}
+
+int af_schur_tangent(af_operator* o, double* dst, const double* p, const double* dp) {
+  if (!o || !dst || !p || !dp) return fail(AF_BAD_ARG, "null argument");
+  if (!o->rho_fixed_set || !o->pres_fixed_set) return fail(AF_BAD_ARG, "set rho_for_fixed and pres_fixed first");
+  if (!aligned16(dst) || !aligned16(p) || !aligned16(dp)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
+  AF_CU(cudaSetDevice(o->device));
+  const long n = o->n_scalar();
+  double *w = o->d_ws, *z = o->d_ws + 2 * n, *t = o->d_ws + 4 * n, *c = o->d_ws + 6 * n;
+  int r = schur_w(o, p, w, t);
+  if (r == AF_OK) r = schur_w(o, dp, z, t);
+  if (r != AF_OK) return r;
+  AF_CU(o->ops->op_C_tangent(o->mesh, w, z, o->d_pres_fixed, c_params(o), c, o->ncell, o->stream));
+  AF_CU(o->ops->mass(o->mesh, 1, dp, nullptr, 1.0 / (1.4 - 1.0), dst, o->ncell, o->stream));  // D dp
+  AF_CU(axpby(-1.0, c, 1.0, dst, n, o->stream));
+  o->launches += 3;
+  return AF_OK;
+}
+
+int af_schur_transpose(af_operator* o, double* dst, const double* p, const double* pbar) {
+  if (!o || !dst || !p || !pbar) return fail(AF_BAD_ARG, "null argument");
+  if (!o->rho_fixed_set || !o->pres_fixed_set) return fail(AF_BAD_ARG, "set rho_for_fixed and pres_fixed first");
+  if (!aligned16(dst) || !aligned16(p) || !aligned16(pbar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
+  AF_CU(cudaSetDevice(o->device));
+  const long n = o->n_scalar();
+  double *w = o->d_ws, *t = o->d_ws + 2 * n, *t2 = o->d_ws + 4 * n, *q = o->d_ws + 6 * n;
+  int r = schur_w(o, p, w, t);
+  if (r != AF_OK) return r;
+  AF_CU(o->ops->op_CT(o->mesh, w, o->d_pres_fixed, pbar, c_params(o), t, o->ncell, o->stream));  // J_C^T pbar
+  AF_CU(o->ops->mass_solve(o->d_La, 2, t, 1.0, t2, o->ncell, o->stream));                        // A^{-1} (A = A^T)
+  AF_CU(o->ops->op_BT(o->mesh, t2, coeff_BC(o) * o->dt / (o->Ma * o->Ma), q, o->ncell, o->stream));
+  AF_CU(o->ops->mass(o->mesh, 1, pbar, nullptr, 1.0 / (1.4 - 1.0), dst, o->ncell, o->stream));    // D = D^T
+  AF_CU(axpby(-1.0, q, 1.0, dst, n, o->stream));
+  o->launches += 5;
+  return AF_OK;
+}
+
 }  // extern "C"
 
 namespace af {

@@ -79,6 +79,12 @@ struct DegreeOps {
   // its tangent-linear: dy (rho, u, p) = J(in) din
   cudaError_t (*rhs_tangent1)(const MeshDev&, const double* const* in, const double* const* din, double* const* dy,
                               const RhsParams&, int ncell, cudaStream_t);
+  // implicit operators: pbar = B^T ubar;  dst = J_C(w) dw;  wbar = J_C(w)^T pbar
+  cudaError_t (*op_BT)(const MeshDev&, const double* ubar, double c, double* pbar, int ncell, cudaStream_t);
+  cudaError_t (*op_C_tangent)(const MeshDev&, const double* w, const double* dw, const double* pf, const CParams&,
+                              double* dst, int ncell, cudaStream_t);
+  cudaError_t (*op_CT)(const MeshDev&, const double* w, const double* pf, const double* pbar, const CParams&,
+                       double* wbar, int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

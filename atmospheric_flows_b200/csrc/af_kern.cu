@@ -521,6 +521,21 @@ cudaError_t rhs_tangent1(const MeshDev& mesh, const double* const* in, const dou
   return launch_cellop<P, RhsTlm1Phys, kAdjCells, 2>(mesh, a, prm, ncell, st);
 }
 
+cudaError_t op_BT(const MeshDev& mesh, const double* ubar, double c, double* pbar, int ncell, cudaStream_t st) {
+  ArgPtrs<1, 1> a{{ubar}, {pbar}};
+  return launch_cellop<P, BTPhys>(mesh, a, BParams{c}, ncell, st);
+}
+cudaError_t op_C_tangent(const MeshDev& mesh, const double* w, const double* dw, const double* pf,
+                         const CParams& prm, double* dst, int ncell, cudaStream_t st) {
+  ArgPtrs<3, 1> a{{w, dw, pf}, {dst}};
+  return launch_cellop<P, CTlmPhys>(mesh, a, prm, ncell, st);
+}
+cudaError_t op_CT(const MeshDev& mesh, const double* w, const double* pf, const double* pbar, const CParams& prm,
+                  double* wbar, int ncell, cudaStream_t st) {
+  ArgPtrs<3, 1> a{{w, pf, pbar}, {wbar}};
+  return launch_cellop<P, CTPhys>(mesh, a, prm, ncell, st);
+}
+
 constexpr int kTransferThreads = 256;
 
 template <class R>
@@ -552,7 +567,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         prolong<double>,   prolong<float>,
                         restrict_<double>, restrict_<float>,
                         inject,            rhs_adjoint1,
-                        rhs_tangent1};
+                        rhs_tangent1,      op_BT,
+                        op_C_tangent,      op_CT};
 
 }  // namespace
 

@@ -561,18 +561,18 @@ int af_schur_solver_precondition(af_schur_solver* s, double* dst, const double* 
   return precondition(s, dst, src);
 }
 
+}  // extern "C"
+
+namespace {
+
 // Flexible GMRES (right preconditioning, the preconditioned directions kept), classical
 // Gram-Schmidt applied twice, Givens rotations; converged when the true residual
-// |b - S x| <= rel_tol |b| (the Arnoldi estimate is checked first, the true residual is
-// recomputed at every restart).
-int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_tol, int max_iterations,
-                   af_schur_stats* stats) {
-  if (!s || !x || !b) return merr(AF_BAD_ARG, "null argument");
-  if (!s->setup_done) return merr(AF_BAD_ARG, "af_schur_solver_setup first");
-  if (!(rel_tol > 0.0) || max_iterations < 1) return merr(AF_BAD_ARG, "af_schur_solve: invalid tolerance or cap");
+// |b - A x| <= rel_tol |b| (the Arnoldi estimate is checked first, the true residual is
+// recomputed at every restart).  A is the Schur operator or its transpose.
+template <class Apply>
+int fgmres(af_schur_solver* s, const Apply& A, double* x, const double* b, double rel_tol, int max_iterations,
+           af_schur_stats* stats) {
   af_operator* o = s->op;
-  MG_CU(cudaSetDevice(o->device));
-  MG_AF(af_set_NS_stage(o, 2));
   cudaStream_t st = o->stream;
   const long n = o->n_scalar();
   const int m = s->opt.restart;
@@ -595,7 +595,7 @@ int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_to
   double res = 0.0, res0 = -1.0;
   bool converged = false;
   while (true) {
-    MG_AF(af_vmult(o, s->gw, x));
+    MG_AF(A(s->gw, x));
     MG_CU(sub(b, s->gw, s->gw, n, st));
     MG_CU(dot(s->gw, nullptr, n, s->part, s->scal, st));
     double beta2 = 0.0;
@@ -615,7 +615,7 @@ int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_to
       double* zj = s->Z + (long)j * n;
       double* w = s->V + (long)(j + 1) * n;
       MG_AF(precondition(s, zj, s->V + (long)j * n));
-      MG_AF(af_vmult(o, w, zj));
+      MG_AF(A(w, zj));
       MG_CU(mdot(s->V, n, j + 1, w, n, s->part, s->dh, st));
       MG_CU(maxpy(s->V, n, j + 1, s->dh, w, n, st));
       MG_CU(mdot(s->V, n, j + 1, w, n, s->part, s->dh + (m + 1), st));
@@ -671,6 +671,36 @@ int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_to
   if (stats) *stats = s->stats;
   if (!converged) return merr(AF_NO_CONVERGENCE, "Schur FGMRES: no convergence within max_iterations");
   return AF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_tol, int max_iterations,
+                   af_schur_stats* stats) {
+  if (!s || !x || !b) return merr(AF_BAD_ARG, "null argument");
+  if (!s->setup_done) return merr(AF_BAD_ARG, "af_schur_solver_setup first");
+  if (!(rel_tol > 0.0) || max_iterations < 1) return merr(AF_BAD_ARG, "af_schur_solve: invalid tolerance or cap");
+  af_operator* o = s->op;
+  MG_CU(cudaSetDevice(o->device));
+  MG_AF(af_set_NS_stage(o, 2));
+  auto A = [o](double* out, const double* in) { return af_vmult(o, out, in); };
+  return fgmres(s, A, x, b, rel_tol, max_iterations, stats);
+}
+
+// Adjoint pressure solve: J_S(p)^T x = b at the linearisation point p, with the solver's
+// preconditioner (a preconditioner of S serves its transpose: the flexible method needs no
+// exact correspondence).
+int af_schur_solve_transpose(af_schur_solver* s, const double* p, double* x, const double* b, double rel_tol,
+                             int max_iterations, af_schur_stats* stats) {
+  if (!s || !p || !x || !b) return merr(AF_BAD_ARG, "null argument");
+  if (!s->setup_done) return merr(AF_BAD_ARG, "af_schur_solver_setup first");
+  if (!(rel_tol > 0.0) || max_iterations < 1) return merr(AF_BAD_ARG, "af_schur_solve_transpose: invalid tolerance or cap");
+  af_operator* o = s->op;
+  MG_CU(cudaSetDevice(o->device));
+  auto A = [o, p](double* out, const double* in) { return af_schur_transpose(o, out, p, in); };
+  return fgmres(s, A, x, b, rel_tol, max_iterations, stats);
 }
 
 }  // extern "C"

@@ -58,6 +58,11 @@ def lib():
         L.af_last_inner_iterations.argtypes = [vp, ctypes.POINTER(ip)]
         L.af_n_dofs.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_longlong)]
         L.af_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        for name in ("af_vmult_pressure_transpose",):
+            getattr(L, name).argtypes = [vp, dp, dp]
+        for name in ("af_vmult_enthalpy_tangent", "af_vmult_enthalpy_transpose", "af_schur_tangent",
+                     "af_schur_transpose"):
+            getattr(L, name).argtypes = [vp, dp, dp, dp]
         L.af_compute_diagnostics.argtypes = [vp, dp, dp, dp, dp, ctypes.POINTER(Diagnostics)]
         L.af_l2_norm.argtypes = [vp, ip, dp, ctypes.POINTER(ctypes.c_double)]
         L.af_error_string.restype = ctypes.c_char_p
@@ -127,7 +132,13 @@ class EULEROperator:
 
     # --- plumbing ---
     def set_stream(self, stream):
-        check(lib().af_set_stream(self._h, ctypes.c_void_p(stream.cuda_stream if stream is not None else 0)))
+        """Run on a torch stream (None: the handle's own stream).  torch's default stream has
+        handle 0, which the C ABI reads as "own stream"; it is passed as cudaStreamLegacy (0x1)."""
+        if stream is None:
+            h = 0
+        else:
+            h = stream.cuda_stream or 1  # cudaStreamLegacy
+        check(lib().af_set_stream(self._h, ctypes.c_void_p(h)))
 
     def synchronize(self):
         check(lib().af_synchronize(self._h))
@@ -217,6 +228,27 @@ class EULEROperator:
 
     def compute_diagonal(self, dst):
         check(lib().af_compute_diagonal(self._h, _ptr(dst)))
+
+    # --- tangents and transposes of the implicit operators ---
+    def vmult_pressure_transpose(self, pbar, ubar):
+        """pbar = B^T ubar"""
+        check(lib().af_vmult_pressure_transpose(self._h, _ptr(pbar), _ptr(ubar)))
+
+    def vmult_enthalpy_tangent(self, dst, w, dw):
+        """dst = J_C(w) dw"""
+        check(lib().af_vmult_enthalpy_tangent(self._h, _ptr(dst), _ptr(w), _ptr(dw)))
+
+    def vmult_enthalpy_transpose(self, wbar, w, pbar):
+        """wbar = J_C(w)^T pbar"""
+        check(lib().af_vmult_enthalpy_transpose(self._h, _ptr(wbar), _ptr(w), _ptr(pbar)))
+
+    def schur_tangent(self, dst, p, dp):
+        """dst = J_S(p) dp"""
+        check(lib().af_schur_tangent(self._h, _ptr(dst), _ptr(p), _ptr(dp)))
+
+    def schur_transpose(self, dst, p, pbar):
+        """dst = J_S(p)^T pbar"""
+        check(lib().af_schur_transpose(self._h, _ptr(dst), _ptr(p), _ptr(pbar)))
 
     # --- diagnostics (Atmospheric_Flow.cc:925-1087) ---
     def compute_diagnostics(self, rho, u, p, rho_stage=None):

@@ -41,6 +41,7 @@ def _bind():
     L.af_schur_solver_levels.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     L.af_schur_solver_precondition.argtypes = [vp, vp, vp]
     L.af_schur_solve.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(Stats)]
+    L.af_schur_solve_transpose.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(Stats)]
     L._schur_bound = True
     return L
 
@@ -88,10 +89,20 @@ class SchurSolver:
     def precondition(self, dst, src):
         check(_bind().af_schur_solver_precondition(self._h, _ptr(dst), _ptr(src)))
 
+    def solve_transpose(self, p, x, b, rel_tol=1e-10, max_iterations=1000, raise_on_failure=True):
+        """Adjoint solve J_S(p)^T x = b (x: initial guess in, solution out)."""
+        st = Stats()
+        r = _bind().af_schur_solve_transpose(self._h, _ptr(p), _ptr(x), _ptr(b), rel_tol, max_iterations,
+                                             ctypes.byref(st))
+        return self._result(r, st, raise_on_failure)
+
     def solve(self, x, b, rel_tol=1e-10, max_iterations=1000, raise_on_failure=True):
         """x: initial guess in, solution out.  Returns the stats dict."""
         st = Stats()
         r = _bind().af_schur_solve(self._h, _ptr(x), _ptr(b), rel_tol, max_iterations, ctypes.byref(st))
+        return self._result(r, st, raise_on_failure)
+
+    def _result(self, r, st, raise_on_failure):
         out = {"iterations": st.iterations, "initial_residual": st.initial_residual,
                "final_residual": st.final_residual, "seconds": st.seconds, "status": r}
         if r != 0 and raise_on_failure:

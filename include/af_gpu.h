@@ -52,7 +52,9 @@ typedef struct {
 int af_create(const af_mesh_desc* mesh, int degree, int n_q_points_1d, double Mach, double Froude, double dt,
               af_operator** out);
 int af_destroy(af_operator* op);
-/* Use an external stream (cudaStream_t passed as void*); NULL restores the own stream. */
+/* Use an external stream (cudaStream_t passed as void*); NULL restores the handle's own
+ * (non-blocking) stream.  To run on the legacy default stream pass cudaStreamLegacy
+ * ((void*)0x1), not NULL. */
 int af_set_stream(af_operator* op, void* stream);
 int af_synchronize(af_operator* op);
 
@@ -186,6 +188,10 @@ int af_schur_solver_precondition(af_schur_solver* s, double* dst, const double* 
 /* x (initial guess in, solution out) for S x = b; returns AF_NO_CONVERGENCE at the cap. */
 int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_tol, int max_iterations,
                    af_schur_stats* stats);
+/* Adjoint pressure solve (no counterpart in the reference): J_S(p)^T x = b, J_S(p) the Jacobian
+ * of the Schur apply at p (see af_schur_transpose), same FGMRES and preconditioner. */
+int af_schur_solve_transpose(af_schur_solver* s, const double* p, double* x, const double* b, double rel_tol,
+                             int max_iterations, af_schur_stats* stats);
 
 /* ---------------------------------------------------------------- IMEX time stepping
  * One IMEX-DG step of the reference's EulerSolver::run (Atmospheric_Flow.cc:1110-1251):
@@ -278,6 +284,23 @@ int af_io_read_state_header(const char* path, af_state_header* header);
 int af_io_read_state(const char* path, double* vertices, double* rho, double* u, double* p);
 int af_io_write_vtu(const char* path, const af_mesh_desc* mesh, int degree, const double* rho, const double* u,
                     const double* p);
+
+/* ---------------------------------------------------------------- tangents and transposes
+ * of the implicit operators (no counterpart in the reference; the pieces of an adjoint IMEX
+ * stage).  DEVICE vectors; the operator's HYPERBOLIC_stage coefficient, dt, Mach,
+ * rho_for_fixed and pres_fixed as in the forward.  C is nonlinear in w through the wave
+ * speed lambda(w); its Jacobian differentiates lambda along the branch the forward takes.
+ *   af_vmult_pressure_transpose:  pbar = B^T ubar
+ *   af_vmult_enthalpy_tangent:    dst = J_C(w) dw
+ *   af_vmult_enthalpy_transpose:  wbar = J_C(w)^T pbar
+ *   af_schur_tangent:             dst = J_S(p) dp = D dp - J_C(w) A^{-1} B dp,  w = A^{-1} B p
+ *   af_schur_transpose:           dst = J_S(p)^T pbar = D pbar - B^T A^{-1} J_C(w)^T pbar
+ * (A^{-1}: the exact cell-wise inverse.) */
+int af_vmult_pressure_transpose(af_operator* op, double* pbar, const double* ubar);
+int af_vmult_enthalpy_tangent(af_operator* op, double* dst, const double* w, const double* dw);
+int af_vmult_enthalpy_transpose(af_operator* op, double* wbar, const double* w, const double* pbar);
+int af_schur_tangent(af_operator* op, double* dst, const double* p, const double* dp);
+int af_schur_transpose(af_operator* op, double* dst, const double* p, const double* pbar);
 
 /* Measures the FP64 FMA throughput of the current device (TFLOP/s) with a short
  * dependent-chain kernel; the denominator of the FP64 roofline the benchmark reports.

@@ -91,3 +91,111 @@ def test_tangent_matches_oracle_differences(P, name):
     got = np.concatenate([t.cpu().numpy() for t in dy])
     err = np.linalg.norm(got - fd) / np.linalg.norm(fd)
     assert err < 1e-8, err
+
+
+# ------------------------------------------------------------------ implicit operators
+def _implicit_setup(name, P):
+    from atmospheric_flows_b200.operator import EULEROperator
+    m, Ma, Fr, src = _case(name, P, True)
+    op = EULEROperator(m, P, Ma, Fr, 2.0)
+    op.set_stream(torch.cuda.current_stream())
+    op.set_schur_mode(1)
+    op.set_HYPERBOLIC_stage(1)
+    op.set_rho_for_fixed(_d(src[0]))
+    op.set_pres_fixed(_d(src[2]))
+    return m, op, src
+
+
+def _dot(a, b):
+    return float(torch.dot(a, b))
+
+
+@pytest.mark.parametrize("P", [2, 4])
+@pytest.mark.parametrize("name", ["hill", "hill_periodic"])
+def test_implicit_dot_products(P, name):
+    """B^T, J_C^T and J_S^T against B, J_C and J_S: dot-product tests to 1e-12."""
+    m, op, src = _implicit_setup(name, P)
+    ns = m.n_cells * (P + 1) ** 2
+    rng = np.random.default_rng(21)
+    rnd = lambda n: _d(rng.standard_normal(n))
+    q, pbar, p = rnd(ns), rnd(ns), _d(src[2])
+    ubar, w, dw = rnd(2 * ns), _d(src[1]), rnd(2 * ns)
+    Bq = torch.empty(2 * ns, dtype=torch.float64, device="cuda")
+    op.vmult_pressure(Bq, q)
+    BTu = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.vmult_pressure_transpose(BTu, ubar)
+    Jdw = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.vmult_enthalpy_tangent(Jdw, w, dw)
+    JTp = torch.empty(2 * ns, dtype=torch.float64, device="cuda")
+    op.vmult_enthalpy_transpose(JTp, w, pbar)
+    Sq = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.schur_tangent(Sq, p, q)
+    STp = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.schur_transpose(STp, p, pbar)
+    torch.cuda.synchronize()
+    for lhs, rhs, scale in ((_dot(ubar, Bq), _dot(BTu, q), float((ubar.abs() * Bq.abs()).sum())),
+                            (_dot(pbar, Jdw), _dot(JTp, dw), float((pbar.abs() * Jdw.abs()).sum())),
+                            (_dot(pbar, Sq), _dot(STp, q), float((pbar.abs() * Sq.abs()).sum()))):
+        assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
+
+
+@pytest.mark.parametrize("P", [2, 3])
+def test_implicit_tangents_match_differences(P):
+    """J_C and J_S against 5-point differences of the forward C and Schur applies (rough
+    states, no wave-speed kink inside the stencil; C is piecewise linear in w, S in p)."""
+    m, op, src = _implicit_setup("hill", P)
+    ns = m.n_cells * (P + 1) ** 2
+    rng = np.random.default_rng(5)
+    w, p = _d(src[1]), _d(src[2])
+    dw = _d(1e-4 * float(w.abs().mean()) * rng.standard_normal(2 * ns))
+    # the wave speed of C acts on w = A^{-1} B p, whose face traces on rough data are closer
+    # together than those of u: a smaller step keeps the branches of the stencil fixed
+    dp = _d(1e-7 * float(p.abs().mean()) * rng.standard_normal(ns))
+
+    def fd(F, x, dx):
+        out = []
+        for t in (1.0, -1.0, 2.0, -2.0):
+            y = torch.empty(ns, dtype=torch.float64, device="cuda")
+            F(y, x + t * dx)
+            out.append(y)
+        torch.cuda.synchronize()
+        return (8.0 * (out[0] - out[1]) - (out[2] - out[3])) / 12.0
+    want = fd(op.vmult_enthalpy, w, dw)
+    got = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.vmult_enthalpy_tangent(got, w, dw)
+    torch.cuda.synchronize()
+    assert float(torch.linalg.norm(got - want) / torch.linalg.norm(want)) < 1e-8
+    op.set_NS_stage(2)
+    want = fd(op.vmult, p, dp)
+    op.schur_tangent(got, p, dp)
+    torch.cuda.synchronize()
+    assert float(torch.linalg.norm(got - want) / torch.linalg.norm(want)) < 1e-7
+
+
+@pytest.mark.parametrize("pc", ["jacobi", "cheb_fp32"])
+def test_adjoint_pressure_solve(pc):
+    """J_S(p)^T x = b solved to 1e-12 (checked with the transpose apply); and J_S(p) p = S p
+    (the Schur apply is positively homogeneous of degree 1 in p, Euler's identity), which ties
+    the linearisation to the forward operator."""
+    from atmospheric_flows_b200.schur import SchurSolver
+    P = 3
+    m, op, src = _implicit_setup("hill", P)
+    op.set_NS_stage(2)
+    ns = m.n_cells * (P + 1) ** 2
+    rng = np.random.default_rng(8)
+    p = _d(src[2])
+    b = _d(rng.standard_normal(ns))
+    s = SchurSolver(op, pc)
+    s.setup()
+    x = torch.zeros(ns, dtype=torch.float64, device="cuda")
+    out = s.solve_transpose(p, x, b, rel_tol=1e-12, max_iterations=5000)
+    assert out["iterations"] > 0
+    r = torch.empty_like(x)
+    op.schur_transpose(r, p, x)
+    torch.cuda.synchronize()
+    assert float(torch.linalg.norm(r - b) / torch.linalg.norm(b)) < 1e-11
+    Sp, Jp = torch.empty_like(x), torch.empty_like(x)
+    op.vmult(Sp, p)
+    op.schur_tangent(Jp, p, p)
+    torch.cuda.synchronize()
+    assert float(torch.linalg.norm(Jp - Sp) / torch.linalg.norm(Sp)) < 1e-12
