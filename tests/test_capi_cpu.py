@@ -50,3 +50,14 @@ def test_create_rejects_bad_arguments_on_host():
     bad = O._MeshDesc(0, 2, 0, v.ctypes.data, 0, 0.0)
     assert L.af_create(ctypes.byref(bad), 4, 9, 1.0, 1.0, 1.0, ctypes.byref(h)) == O.AF_BAD_ARG
     assert L.af_set_NS_stage(None, 7) == O.AF_BAD_ARG
+
+
+def test_cpp_header_compiles():
+    """include/af_euler_operator.hpp is self-contained C++17 over af_gpu.h."""
+    import subprocess
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = "#include \"af_euler_operator.hpp\"\nint main() { return 0; }\n"
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
+                        "-x", "c++", "-"], input=src, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
