@@ -303,34 +303,38 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   const int ncb = min(CB, ncell - c0);  // valid cells in this block
   const int c = c0 + (cl < ncb ? cl : ncb - 1);
 
-  // ---- per-cell geometry and neighbours (member 0), basis copy for runtime indexing
+  // ---- per-cell geometry and neighbours, spread over the cell's threads (task f < 4: face f,
+  //      task 4: the bilinear map and the neighbour indices); basis copy for runtime indexing
   for (int k = tid; k < NQ * P1; k += NT) s_S[k] = tb.S[k / P1][k % P1];
   for (int k = tid; k < NQ; k += NT) s_w[k] = tb.w[k];
-  if (m == 0) {
+  for (int task = m; task < 5; task += NQ) {
     const int i = c % mesh.nx, j = c / mesh.nx, W = mesh.nx + 1;
-    const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
-    const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
     R* g = s_geo + cl * 24;
-    g[0] = v1.x - v0.x; g[1] = v1.y - v0.y;                        // A = x_xi at eta = 0
-    g[2] = v3.x - v2.x - v1.x + v0.x; g[3] = v3.y - v2.y - v1.y + v0.y;  // B (bilinear term)
-    g[4] = v2.x - v0.x; g[5] = v2.y - v0.y;                        // C = x_eta at xi = 0
-    g[6] = v0.x; g[7] = v0.y;
-    // faces: 0 (xi=0, edge v0->v2), 1 (xi=1, v1->v3), 2 (eta=0, v0->v1), 3 (eta=1, v2->v3);
-    // a face's normal is formed from its two vertices the same way by both cells
-    double tx, tz, len;
-    tx = v2.x - v0.x; tz = v2.y - v0.y; len = sqrt(tx * tx + tz * tz);
-    g[8] = -tz / len; g[9] = tx / len; g[10] = len;
-    tx = v3.x - v1.x; tz = v3.y - v1.y; len = sqrt(tx * tx + tz * tz);
-    g[11] = tz / len; g[12] = -tx / len; g[13] = len;
-    tx = v1.x - v0.x; tz = v1.y - v0.y; len = sqrt(tx * tx + tz * tz);
-    g[14] = tz / len; g[15] = -tx / len; g[16] = len;
-    tx = v3.x - v2.x; tz = v3.y - v2.y; len = sqrt(tx * tx + tz * tz);
-    g[17] = -tz / len; g[18] = tx / len; g[19] = len;
-    int nb0 = i > 0 ? c - 1 : (mesh.periodic_x ? c + mesh.nx - 1 : -1);
-    int nb1 = i < mesh.nx - 1 ? c + 1 : (mesh.periodic_x ? c - mesh.nx + 1 : -1);
-    int nb2 = j > 0 ? c - mesh.nx : -1;
-    int nb3 = j < mesh.nz - 1 ? c + mesh.nx : -1;
-    g[20] = (R)nb0; g[21] = (R)nb1; g[22] = (R)nb2; g[23] = (R)nb3;
+    if (task == 4) {
+      const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
+      const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
+      g[0] = v1.x - v0.x; g[1] = v1.y - v0.y;                        // A = x_xi at eta = 0
+      g[2] = v3.x - v2.x - v1.x + v0.x; g[3] = v3.y - v2.y - v1.y + v0.y;  // B (bilinear term)
+      g[4] = v2.x - v0.x; g[5] = v2.y - v0.y;                        // C = x_eta at xi = 0
+      g[6] = v0.x; g[7] = v0.y;
+      const int nb0 = i > 0 ? c - 1 : (mesh.periodic_x ? c + mesh.nx - 1 : -1);
+      const int nb1 = i < mesh.nx - 1 ? c + 1 : (mesh.periodic_x ? c - mesh.nx + 1 : -1);
+      const int nb2 = j > 0 ? c - mesh.nx : -1;
+      const int nb3 = j < mesh.nz - 1 ? c + mesh.nx : -1;
+      g[20] = (R)nb0; g[21] = (R)nb1; g[22] = (R)nb2; g[23] = (R)nb3;
+    } else {
+      // faces: 0 (xi=0, edge v0->v2), 1 (xi=1, v1->v3), 2 (eta=0, v0->v1), 3 (eta=1, v2->v3);
+      // a face's normal is formed from its two vertices the same way by both cells
+      const int f = task;
+      const int ia = (f == 1) ? i + 1 : i, ja = (f == 3) ? j + 1 : j;                       // first vertex
+      const int ib = (f == 0) ? i : i + 1, jb = (f == 2) ? j : j + 1;                       // second vertex
+      const double2 a = mesh.vtx[ja * W + ia], b = mesh.vtx[jb * W + ib];
+      const double tx = b.x - a.x, tz = b.y - a.y, len = sqrt(tx * tx + tz * tz);
+      const double sg = (f == 0 || f == 3) ? 1.0 : -1.0;  // outward: (-tz, tx) on faces 0 and 3
+      g[8 + 3 * f] = sg * (-tz / len);
+      g[9 + 3 * f] = sg * (tx / len);
+      g[10 + 3 * f] = len;
+    }
   }
   if (Phys::FACES) {
     for (int k = tid; k < L::R_FLUX; k += NT) s_flux[k] = 0.0;
