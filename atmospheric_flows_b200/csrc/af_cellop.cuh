@@ -94,6 +94,30 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 constexpr int odd(int n) { return n | 1; }
 
+// Own-cell staging by bulk copies (1) or per-element cp.async (0); see Layout::BULK.
+#ifndef AF_BULK_STAGING
+#define AF_BULK_STAGING 1
+#endif
+constexpr bool kBulkStaging = AF_BULK_STAGING != 0;
+
+// Bounded wait on a shared-memory mbarrier phase; false when the bound was reached.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned phase) {
+  for (int it = 0; it < (1 << 20); ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// Set when a kernel of this translation unit gave up waiting for its bulk copies (never
+// expected; the kernel then returns without writing its outputs).
+static __device__ int g_af_stage_timeout = 0;
+
 // Unroll factor of the z-pass loop over quadrature-point pairs (see the kernel).
 #ifndef AF_Z_UNROLL
 #define AF_Z_UNROLL 1
@@ -197,7 +221,12 @@ struct Layout {
   // region A: x-contracted rows of every cell field, later the z-accumulators
   static constexpr int R_EO = NFC * CB * EOS;
   static constexpr int R_ACC = NOUT * 2 * CB * EOS;
-  static constexpr int RA = R_EO > R_ACC ? R_EO : R_ACC;
+  static constexpr int ALIGN = 16 / (int)sizeof(R);  // region B starts on a 16-byte boundary
+  static constexpr int RA = ((R_EO > R_ACC ? R_EO : R_ACC) + ALIGN - 1) / ALIGN * ALIGN;
+  // Own-cell staging by bulk asynchronous copies (TMA, one per array and CTA): needs the
+  // shared-memory image of an array to equal its global chunk (no padding: ND odd) and chunk
+  // sizes that are multiples of 16 bytes (CB even); arrays are then laid out [cell][comp][node].
+  static constexpr bool BULK = kBulkStaging && (ND % 2 == 1) && (CB % 2 == 0);
   // region B: one group's nodal values and neighbour face nodes, later the outputs
   static constexpr int R_IN = NF * CB * NDP;
   static constexpr int R_NB = Phys::FACES ? 4 * NF * CB * P1P : 0;
@@ -296,6 +325,17 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   R* s_S = s_geo + L::R_GEO;
   R* s_w = s_S + NQ * P1;
 
+  __shared__ alignas(8) unsigned long long s_bar;  // bulk-copy completion (Layout::BULK)
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_bar);
+  if constexpr (L::BULK) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+  }
+  unsigned bar_phase = 0;
+  bool abort = false;
+
   const int tid = threadIdx.x;
   const int m = tid / CB;   // member: row / column / face point
   const int cl = tid % CB;  // cell within the block
@@ -349,18 +389,60 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     constexpr int EOFF = PhysInfo<Phys>::eo_offset(G);
     constexpr bool GFACE = Phys::FACES && Gr::FACE;
 
+    if (abort) return;
     __syncthreads();  // region B free (previous group done) / geometry visible
-    // own cells: contiguous chunk per array, coalesced asynchronous copies
-    sfor<Gi::NARR>([&](auto ac) {
-      constexpr int A = decltype(ac)::value;
-      constexpr int NC = Gr::ncomp(A);
-      constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
-      const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
-      for (int e = tid; e < ncb * NC * ND; e += NT) {
-        const int cc = e / (NC * ND), r = e % (NC * ND);
-        cp_async_el(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
+    // own cells: the contiguous chunk of each array, by one bulk copy per array (TMA) when
+    // the layout allows, otherwise by coalesced per-element asynchronous copies
+    const bool bulk = L::BULK && ((size_t)ncb * ND * sizeof(R)) % 16 == 0;
+    if (bulk) {
+      if (tid == 0) {
+        unsigned bytes = 0;
+        sfor<Gi::NARR>([&](auto ac) { bytes += (unsigned)(ncb * Gr::ncomp(decltype(ac)::value) * ND * sizeof(R)); });
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+        sfor<Gi::NARR>([&](auto ac) {
+          constexpr int A = decltype(ac)::value;
+          constexpr int NC = Gr::ncomp(A);
+          constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+          const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(s_in + fb * CB * ND);
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+              "l"(src), "r"((unsigned)(ncb * NC * ND * sizeof(R))), "r"(bar)
+              : "memory");
+        });
       }
-    });
+    } else {
+      sfor<Gi::NARR>([&](auto ac) {
+        constexpr int A = decltype(ac)::value;
+        constexpr int NC = Gr::ncomp(A);
+        constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+        const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+        for (int e = tid; e < ncb * NC * ND; e += NT) {
+          if constexpr (L::BULK) {
+            cp_async_el(&s_in[fb * CB * ND + e], src + e);  // [cell][comp][node], as the bulk copy
+          } else {
+            const int cc = e / (NC * ND), r = e % (NC * ND);
+            cp_async_el(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
+          }
+        }
+      });
+    }
+    // shared-memory offset of field fi (group-local) of cell cl
+    auto foff = [&](int fi, int cl_) -> int {
+      if constexpr (!L::BULK) {
+        return (fi * CB + cl_) * L::NDP;
+      } else {
+        int off = 0, fb = 0;
+#pragma unroll
+        for (int a = 0; a < Gi::NARR; ++a) {
+          const int nc = Gr::ncomp(a);
+          if (fi >= fb && fi < fb + nc) off = fb * CB * ND + cl_ * nc * ND + (fi - fb) * ND;
+          fb += nc;
+        }
+        return off;
+      }
+    };
     // neighbours' face nodes (L2-resident), ordered along the face parameter;
     // one element per thread for each (face, field): CB * P1 <= NT for every degree
     if constexpr (GFACE) {
@@ -388,7 +470,17 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     }
     cp_async_wait_all();
-    __syncthreads();
+    if (bulk) {
+      const bool ok = mbar_wait(bar, bar_phase);
+      bar_phase ^= 1u;
+      if (!ok) atomicExch(&g_af_stage_timeout, 1);
+      if (__syncthreads_or(!ok)) {  // every thread leaves together, nothing waits on a barrier
+        abort = true;
+        return;
+      }
+    } else {
+      __syncthreads();
+    }
     // ---- X pass: rows (k, P-k) even/odd, contracted along x, for the cell fields (S) and
     //      again for the gradient fields (D, slots NFC..NFC+NFG-1)
     {
@@ -398,7 +490,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         const int fi = task / NPR, k = task % NPR;
         const bool dxi = NFG > 0 && fi >= NFC;
         const int src = dxi ? fi - NFG : fi;  // gradient fields are the last NFG cell fields
-        const R* cell = s_in + (src * CB + cl) * L::NDP;
+        const R* cell = s_in + foff(src, cl);
         R* eo = s_eo + ((EOFF + fi) * CB + cl) * L::EOS;
         R r[P1], y[NQ];
         auto contract = [&]() {
@@ -439,7 +531,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         R vp[NF], vm[NF];
 #pragma unroll
         for (int fi = 0; fi < NF; ++fi) {
-          const R* cell = s_in + (fi * CB + cl) * L::NDP;
+          const R* cell = s_in + foff(fi, cl);
           const R* nbv = s_nb + ((f * NF + fi) * CB + cl) * L::P1P;
           R a = 0.0, b = 0.0;
 #pragma unroll
@@ -463,6 +555,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     }
   });
+  if (abort) return;
   __syncthreads();
 
   // ================= merged z pass: member = quadrature column qx =================
