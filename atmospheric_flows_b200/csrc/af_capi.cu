@@ -449,6 +449,7 @@ static int ensure_factor(af_operator* o, bool weighted) {
   return AF_OK;
 }
 
+
 int af_vmult_inverse(af_operator* o, double* dst, const double* src) {
   if (!o || !dst || !src) return fail(AF_BAD_ARG, "null argument");
   const int ns = o->ns;
@@ -632,4 +633,15 @@ int af_schur_transpose(af_operator* o, double* dst, const double* p, const doubl
 namespace af {
 // Lets other translation units of the library report through af_last_error_message().
 void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace af
+
+namespace af {
+// The operator's packed cell inverses of A (rho_for_fixed) or M, built if needed; used by the
+// pressure solver's finest level instead of factorising the same matrices again.
+int mass_inverse(af_operator* o, bool weighted, const double** out) {
+  const int r = ensure_factor(o, weighted);
+  if (r != AF_OK) return r;
+  *out = weighted ? o->d_La : o->d_Lm;
+  return AF_OK;
+}
 }  // namespace af

@@ -48,3 +48,6 @@ struct af_operator {
   long n_scalar() const { return (long)ncell * nd; }
 };
 
+namespace af {
+int mass_inverse(af_operator* o, bool weighted, const double** out);
+}

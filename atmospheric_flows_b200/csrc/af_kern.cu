@@ -202,122 +202,124 @@ cudaError_t inv_diag(const MeshDev& mesh, int ncomp, const double* weight, doubl
 
 // ---------------------------------------------------------------- exact cell inverse
 // Cell mass matrix  M_K[I][J] = sum_q w(q) JxW(q) phi_I(q) phi_J(q)  (w = 1 or a density),
-// assembled by sum factorisation, factored by Cholesky and inverted (M^{-1} = L^{-T} L^{-1}),
-// one thread per cell.  The packed lower triangle of the symmetric inverse (row-major) is
-// stored cell-major, Minv[c * NPK + k], so that one warp of the apply kernel reads a cell's
-// inverse as one contiguous block.
-// Per-thread work arrays live in shared memory, interleaved by thread (conflict-free).
+// its Cholesky factor and its inverse, one warp per cell:
+//   F(q) = w(q) JxW(q) at the Gauss points (lanes over points);
+//   T(qz)[ix][jx] = sum_qx S[qx][ix] S[qx][jx] F(qz, qx),
+//   M[I][J] = sum_qz S[qz][iz] S[qz][jz] T(qz)[ix][jx]   (lanes over entries, packed lower);
+//   Cholesky M = L L^T in place (lanes over rows, one column at a time);
+//   X = L^{-1}: lane j solves L x = e_j for its column in registers;  M^{-1} = X^T X.
+// The packed lower triangle of the inverse (row-major) is stored cell-major,
+// Minv[c * NPK + k], so that one warp of the apply kernel reads a cell's inverse as one
+// contiguous block.
 constexpr int kND = (P + 1) * (P + 1);
 constexpr int kNPK = kND * (kND + 1) / 2;
-constexpr int kFactorThreads = P <= 2 ? 64 : (P <= 4 ? 32 : 16);
+constexpr int kFactorWarps = P <= 4 ? 4 : (P == 5 ? 2 : 1);  // static shared memory <= 48 KB
 
-__global__ void __launch_bounds__(kFactorThreads)
+__global__ void __launch_bounds__(32 * kFactorWarps)
     k_mass_factor(const MeshDev mesh, const double* __restrict__ weight, double* __restrict__ Lg, const int ncell) {
   using T = Tab<P>;
-  constexpr int P1 = T::P1, NQ = T::NQ, ND = kND, NPK = kNPK, NTH = kFactorThreads;
-  extern __shared__ double sm[];
-  const int t = threadIdx.x;
-  const int c = blockIdx.x * NTH + t;
-  double* A = sm;                  // [NPK][NTH]
-  double* F = sm + NPK * NTH;      // [NQ*NQ][NTH]
+  constexpr int P1 = T::P1, NQ = T::NQ, ND = kND, NPK = kNPK;
+  constexpr int NT = NQ * P1 * (P1 + 1) / 2;  // T(qz)[ix >= jx]
+  __shared__ double sA[kFactorWarps][NPK];
+  __shared__ double sX[kFactorWarps][NPK];
+  __shared__ double sF[kFactorWarps][NQ * NQ];
+  __shared__ double sT[kFactorWarps][NT];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kFactorWarps + warp;
+  if (c >= ncell) return;  // whole warps; no block-wide barrier below
   const Tab<P>& tb = c_tab;
-  const bool valid = c < ncell;
-  const int cc = valid ? c : ncell - 1;
-  const int i = cc % mesh.nx, j = cc / mesh.nx, W = mesh.nx + 1;
+  double* A = sA[warp];
+  double* X = sX[warp];
+  double* F = sF[warp];
+  double* Tm = sT[warp];
+  const int i = c % mesh.nx, j = c / mesh.nx, W = mesh.nx + 1;
   const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
   const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
   const double Ax = v1.x - v0.x, Az = v1.y - v0.y, Cx = v2.x - v0.x, Cz = v2.y - v0.y;
   const double Bx = v3.x - v2.x - v1.x + v0.x, Bz = v3.y - v2.y - v1.y + v0.y;
-  // f(q) = w(q) JxW(q)
-  for (int qx = 0; qx < NQ; ++qx) {
-    double tx[P1];
+  // F(q) = w(q) JxW(q)
+  for (int q = lane; q < NQ * NQ; q += 32) {
+    const int qx = q % NQ, qz = q / NQ;
+    const double xi = tb.x[qx], eta = tb.x[qz];
+    const double J00 = fma(Bx, eta, Ax), J10 = fma(Bz, eta, Az), J01 = fma(Bx, xi, Cx), J11 = fma(Bz, xi, Cz);
+    double f = (J00 * J11 - J01 * J10) * tb.w[qx] * tb.w[qz];
     if (weight) {
+      const double* wc = weight + (size_t)c * ND;
+      double wv = 0.0;
 #pragma unroll
       for (int iz = 0; iz < P1; ++iz) {
-        double s = 0.0;
+        double t = 0.0;
 #pragma unroll
-        for (int ix = 0; ix < P1; ++ix) s = fma(tb.S[qx][ix], weight[(size_t)cc * ND + iz * P1 + ix], s);
-        tx[iz] = s;
+        for (int ix = 0; ix < P1; ++ix) t = fma(tb.S[qx][ix], wc[iz * P1 + ix], t);
+        wv = fma(tb.S[qz][iz], t, wv);
       }
+      f *= wv;
     }
-    const double xi = tb.x[qx];
-    const double J01 = fma(Bx, xi, Cx), J11 = fma(Bz, xi, Cz);
-    for (int qz = 0; qz < NQ; ++qz) {
-      const double eta = tb.x[qz];
-      const double J00 = fma(Bx, eta, Ax), J10 = fma(Bz, eta, Az);
-      double f = (J00 * J11 - J01 * J10) * tb.w[qx] * tb.w[qz];
-      if (weight) {
-        double wv = 0.0;
+    F[q] = f;
+  }
+  __syncwarp();
+  // T(qz)[ix][jx], ix >= jx
+  for (int e = lane; e < NT; e += 32) {
+    const int qz = e / (P1 * (P1 + 1) / 2);
+    int r = e % (P1 * (P1 + 1) / 2), ix = 0;
+    while (r > ix) { r -= ix + 1; ++ix; }
+    const int jx = r;
+    double s = 0.0;
 #pragma unroll
-        for (int iz = 0; iz < P1; ++iz) wv = fma(tb.S[qz][iz], tx[iz], wv);
-        f *= wv;
-      }
-      F[(qz * NQ + qx) * NTH + t] = f;
+    for (int qx = 0; qx < NQ; ++qx) s = fma(tb.S[qx][ix] * tb.S[qx][jx], F[qz * NQ + qx], s);
+    Tm[e] = s;
+  }
+  __syncwarp();
+  // M[I][J], I >= J (packed row-major)
+  for (int e = lane; e < NPK; e += 32) {
+    int I = 0, r = e;
+    while (r > I) { r -= I + 1; ++I; }
+    const int J = r;
+    const int iz = I / P1, ix = I % P1, jz = J / P1, jx = J % P1;
+    const int a = ix >= jx ? ix : jx, b = ix >= jx ? jx : ix;
+    const int tix = a * (a + 1) / 2 + b;
+    double s = 0.0;
+#pragma unroll
+    for (int qz = 0; qz < NQ; ++qz)
+      s = fma(tb.S[qz][iz] * tb.S[qz][jz], Tm[qz * (P1 * (P1 + 1) / 2) + tix], s);
+    A[e] = s;
+  }
+  __syncwarp();
+  // Cholesky, one column at a time: L_kk = sqrt(A_kk); L_ik = A_ik / L_kk; A_ij -= L_ik L_jk
+  for (int k = 0; k < ND; ++k) {
+    const double lkk = sqrt(A[k * (k + 1) / 2 + k]);
+    const double inv = 1.0 / lkk;
+    for (int r = k + 1 + lane; r < ND; r += 32) A[r * (r + 1) / 2 + k] *= inv;
+    __syncwarp();
+    if (lane == 0) A[k * (k + 1) / 2 + k] = lkk;
+    for (int r = k + 1 + lane; r < ND; r += 32) {
+      const double lrk = A[r * (r + 1) / 2 + k];
+      for (int q = k + 1; q <= r; ++q) A[r * (r + 1) / 2 + q] -= lrk * A[q * (q + 1) / 2 + k];
+    }
+    __syncwarp();
+  }
+  // X = L^{-1}: lane jc solves L x = e_jc (x_i = 0 for i < jc) in registers and stores the
+  // column into the packed lower X; then M^{-1}[I][J] = sum_{k >= I} X[k][I] X[k][J]
+  for (int jc = lane; jc < ND; jc += 32) {
+    double x[ND];
+#pragma unroll
+    for (int ii = 0; ii < ND; ++ii) {
+      double s = (ii == jc) ? 1.0 : 0.0;
+#pragma unroll
+      for (int kk = 0; kk < ii; ++kk) s = fma(-A[ii * (ii + 1) / 2 + kk], x[kk], s);
+      x[ii] = ii >= jc ? s / A[ii * (ii + 1) / 2 + ii] : 0.0;
+      if (ii >= jc) X[ii * (ii + 1) / 2 + jc] = x[ii];
     }
   }
-  for (int k = 0; k < NPK; ++k) A[k * NTH + t] = 0.0;
-  // A[I][J] += S[qz][iz] S[qz][jz] * T[ix][jx],  T[ix][jx] = sum_qx S[qx][ix] S[qx][jx] f(qz, qx)
-  for (int qz = 0; qz < NQ; ++qz) {
-    double Tm[P1][P1];
-#pragma unroll
-    for (int ix = 0; ix < P1; ++ix)
-#pragma unroll
-      for (int jx = 0; jx <= ix; ++jx) {
-        double s = 0.0;
-        for (int qx = 0; qx < NQ; ++qx) s = fma(tb.S[qx][ix] * tb.S[qx][jx], F[(qz * NQ + qx) * NTH + t], s);
-        Tm[ix][jx] = s;
-        Tm[jx][ix] = s;
-      }
-    for (int I = 0; I < ND; ++I) {
-      const int iz = I / P1, ix = I % P1;
-      const double si = tb.S[qz][iz];
-      for (int J = 0; J <= I; ++J) {
-        const int jz = J / P1, jx = J % P1;
-        A[(I * (I + 1) / 2 + J) * NTH + t] += si * tb.S[qz][jz] * Tm[ix][jx];
-      }
-    }
-  }
-  // Cholesky, packed row-major lower; the diagonal stores 1/L_jj
-  for (int jj = 0; jj < ND; ++jj) {
-    double d = A[(jj * (jj + 1) / 2 + jj) * NTH + t];
-    for (int k = 0; k < jj; ++k) {
-      const double l = A[(jj * (jj + 1) / 2 + k) * NTH + t];
-      d -= l * l;
-    }
-    const double inv = 1.0 / sqrt(d);
-    A[(jj * (jj + 1) / 2 + jj) * NTH + t] = inv;
-    for (int ii = jj + 1; ii < ND; ++ii) {
-      double a = A[(ii * (ii + 1) / 2 + jj) * NTH + t];
-      for (int k = 0; k < jj; ++k) a -= A[(ii * (ii + 1) / 2 + k) * NTH + t] * A[(jj * (jj + 1) / 2 + k) * NTH + t];
-      A[(ii * (ii + 1) / 2 + jj) * NTH + t] = a * inv;
-    }
-  }
-  // X = L^{-1} (lower), row by row: X_ii = 1/L_ii, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj; the
-  // row is formed in scratch (the quadrature region F) because it still reads L_i.
-  double* Xr = F;
-  for (int ii = 0; ii < ND; ++ii) {
-    const double di = A[(ii * (ii + 1) / 2 + ii) * NTH + t];
-    for (int jj = 0; jj < ii; ++jj) {
-      double s = 0.0;
-      for (int k = jj; k < ii; ++k) s += A[(ii * (ii + 1) / 2 + k) * NTH + t] * A[(k * (k + 1) / 2 + jj) * NTH + t];
-      Xr[jj * NTH + t] = -s * di;
-    }
-    for (int jj = 0; jj < ii; ++jj) A[(ii * (ii + 1) / 2 + jj) * NTH + t] = Xr[jj * NTH + t];
-  }
-  // M^{-1} = X^T X, (i, j <= i) = sum_{k >= i} X_ki X_kj, in place: rows ascending, j
-  // ascending (row i's own X_ii is overwritten last; rows k > i are still X)
-  for (int ii = 0; ii < ND; ++ii)
-    for (int jj = 0; jj <= ii; ++jj) {
-      double s = 0.0;
-      for (int k = ii; k < ND; ++k) s += A[(k * (k + 1) / 2 + ii) * NTH + t] * A[(k * (k + 1) / 2 + jj) * NTH + t];
-      A[(ii * (ii + 1) / 2 + jj) * NTH + t] = s;
-    }
-  // cell-major output, written cooperatively (coalesced): Minv[c * NPK + k]
-  __syncthreads();
-  const int c0 = blockIdx.x * NTH;
-  for (int e = t; e < NTH * NPK; e += NTH) {
-    const int cl = e / NPK, k = e % NPK;
-    if (c0 + cl < ncell) Lg[(size_t)(c0 + cl) * NPK + k] = A[k * NTH + cl];
+  __syncwarp();
+  double* out = Lg + (size_t)c * NPK;
+  for (int e = lane; e < NPK; e += 32) {
+    int I = 0, r = e;
+    while (r > I) { r -= I + 1; ++I; }
+    const int J = r;
+    double s = 0.0;
+    for (int k = I; k < ND; ++k) s = fma(X[k * (k + 1) / 2 + I], X[k * (k + 1) / 2 + J], s);
+    out[e] = s;
   }
 }
 
@@ -376,14 +378,7 @@ cudaError_t launch_mass_solve(const R* L, int ncomp, const R* b, R scale, R* x, 
 }
 
 cudaError_t mass_factor(const MeshDev& mesh, const double* weight, double* L, int ncell, cudaStream_t st) {
-  const size_t bytes = sizeof(double) * (size_t)(kNPK + (2 * P + 1) * (2 * P + 1)) * kFactorThreads;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_mass_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  k_mass_factor<<<(ncell + kFactorThreads - 1) / kFactorThreads, kFactorThreads, bytes, st>>>(mesh, weight, L, ncell);
+  k_mass_factor<<<(ncell + kFactorWarps - 1) / kFactorWarps, 32 * kFactorWarps, 0, st>>>(mesh, weight, L, ncell);
   return cudaGetLastError();
 }
 

@@ -344,7 +344,15 @@ int setup_levels(af_schur_solver* s, bool estimate) {
       o->launches += 2;
     }
     k_convert<double, R><<<nblocks(L.ns), kThreads, 0, o->stream>>>(L.pf, (R*)L.pfR, L.ns);
-    if (sizeof(R) == sizeof(double)) {
+    if (l == 0) {  // the operator's own inverse of A (built once per rho_for_fixed)
+      const double* La = nullptr;
+      MG_AF(mass_inverse(o, true, &La));
+      const long nf = (long)L.ncell * k->factor_len;
+      if (sizeof(R) == sizeof(double))
+        MG_CU(cudaMemcpyAsync(L.LA, La, sizeof(double) * nf, cudaMemcpyDeviceToDevice, o->stream));
+      else
+        k_convert<double, R><<<nblocks(nf), kThreads, 0, o->stream>>>(La, (R*)L.LA, nf);
+    } else if (sizeof(R) == sizeof(double)) {
       MG_CU(k->mass_factor(L.mesh, L.rho, (double*)L.LA, L.ncell, o->stream));
     } else {
       const long nf = (long)L.ncell * k->factor_len;

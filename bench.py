@@ -432,12 +432,22 @@ def run_ours(args, rank, world, local_rank):
 def run_profile_case(kind):
     """A short run of one workload for ncu captures (no timing, no JSON): 'rhs' the fused
     stage-1 apply, 'adjoint' its tangent and backward, 'schur' the FP32 multigrid setup and
-    one V-cycle on the 1024x256 pressure system."""
+    one V-cycle on the 1024x256 pressure system, 'imex' two mixed-precision IMEX steps on the
+    periodic 512x256 hill."""
     import torch
     from atmospheric_flows_b200 import mesh as M
     from atmospheric_flows_b200.operator import EULEROperator
     sc = M.Scaling()
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    if kind == "imex":
+        from atmospheric_flows_b200.imex import IMEXStepper
+        m = M.hill_mesh(512, 256, periodic_x=True)
+        st = M.hill_state(m, DEGREE, seed=SEED, modes=4)
+        g = IMEXStepper(m, DEGREE, sc.Ma, sc.Fr, 0.5, schur_preconditioner="cheb_fp32")
+        g.set_state(d(st.rho), d(st.u), d(st.p))
+        g.step(2)
+        torch.cuda.synchronize()
+        return
     if kind in ("rhs", "adjoint"):
         m, src_h = workload(DEGREE, modes=2)
         op = EULEROperator(m, DEGREE, sc.Ma, sc.Fr, 2.0)
@@ -479,7 +489,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-solvers", action="store_true", help="skip the Schur-solve and IMEX-step measurements")
-    ap.add_argument("--profile", choices=["rhs", "adjoint", "schur"],
+    ap.add_argument("--profile", choices=["rhs", "adjoint", "schur", "imex"],
                     help="run one workload briefly for an ncu capture and exit (no measurement)")
     args = ap.parse_args()
     if args.profile:
