@@ -1,6 +1,7 @@
 // af_kern.cu -- per-degree kernel instantiations.  Compiled once per polynomial degree
 // with -DAF_P=<p>; each object registers its entry points in the degree table used by
 // the C ABI (af_capi.cu).
+#include <cstdint>
 #include <cstdio>
 
 #include "af_adjoint.cuh"
@@ -335,27 +336,58 @@ __global__ void __launch_bounds__(32 * kSolveWarps)
     k_mass_solve(const R* __restrict__ Minv, const R* __restrict__ b, R* __restrict__ x, R* __restrict__ dv,
                  const R scale, const R alpha, const int first, const int ncomp, const int ncell) {
   constexpr int ND = kND, NPK = kNPK;
-  __shared__ R sM[kSolveWarps][NPK];
-  __shared__ R sb[kSolveWarps][2 * ND];
+  __shared__ alignas(16) R sM[kSolveWarps * NPK];
+  __shared__ alignas(16) R sb[kSolveWarps * 2 * ND];
+  __shared__ alignas(8) unsigned long long s_bar;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * kSolveWarps + warp;
-  if (c >= ncell) return;  // whole warps only; no block-wide barrier below
-  // asynchronous copies: every load of the warp is in flight before the single wait
-  const R* mp = Minv + (size_t)c * NPK;
-  for (int k = lane; k < NPK; k += 32) cp_async_el(&sM[warp][k], mp + k);
-  const R* bp = b + (size_t)c * ncomp * ND;
-  for (int k = lane; k < ncomp * ND; k += 32) cp_async_el(&sb[warp][k], bp + k);
-  cp_async_wait_all();
-  __syncwarp();
+  const int c0 = blockIdx.x * kSolveWarps, c = c0 + warp;
+  // A full block's inverses and right-hand sides are contiguous: one bulk copy (TMA) each when
+  // the chunks are 16-byte multiples, else per-element asynchronous copies per warp.
+  const size_t mbytes = sizeof(R) * (size_t)kSolveWarps * NPK, bbytes = sizeof(R) * (size_t)kSolveWarps * ncomp * ND;
+  const bool bulk = c0 + kSolveWarps <= ncell && mbytes % 16 == 0 && bbytes % 16 == 0 &&
+                    (reinterpret_cast<uintptr_t>(Minv + (size_t)c0 * NPK) & 15) == 0 &&
+                    (reinterpret_cast<uintptr_t>(b + (size_t)c0 * ncomp * ND) & 15) == 0;
+  if (bulk) {
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_bar);
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"((unsigned)(mbytes + bbytes))
+                   : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                       (unsigned)__cvta_generic_to_shared(sM)),
+                   "l"(Minv + (size_t)c0 * NPK), "r"((unsigned)mbytes), "r"(bar)
+                   : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                       (unsigned)__cvta_generic_to_shared(sb)),
+                   "l"(b + (size_t)c0 * ncomp * ND), "r"((unsigned)bbytes), "r"(bar)
+                   : "memory");
+    }
+    __syncthreads();  // barrier initialised before anyone waits on it
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) return;  // never expected; every thread leaves together
+  } else {
+    if (c >= ncell) return;  // whole warps only; no block-wide barrier on this path
+    const R* mp = Minv + (size_t)c * NPK;
+    for (int k = lane; k < NPK; k += 32) cp_async_el(&sM[warp * NPK + k], mp + k);
+    const R* bp = b + (size_t)c * ncomp * ND;
+    for (int k = lane; k < ncomp * ND; k += 32) cp_async_el(&sb[warp * ncomp * ND + k], bp + k);
+    cp_async_wait_all();
+    __syncwarp();
+  }
+  const R* M = sM + warp * NPK;
+  const R* bb = sb + warp * ncomp * ND;
   for (int i = lane; i < ND; i += 32) {
     const int ri = i * (i + 1) / 2;
-    for (int d = 0; d < ncomp; ++d) {
-      R y = R(0);
+    R y0 = R(0), y1 = R(0);  // both components share each matrix load
 #pragma unroll
-      for (int j = 0; j < ND; ++j) {
-        const int idx = j <= i ? ri + j : j * (j + 1) / 2 + i;
-        y = fmaR(sM[warp][idx], sb[warp][d * ND + j], y);
-      }
+    for (int j = 0; j < ND; ++j) {
+      const R m = M[j <= i ? ri + j : j * (j + 1) / 2 + i];
+      y0 = fmaR(m, bb[j], y0);
+      if (ncomp == 2) y1 = fmaR(m, bb[ND + j], y1);
+    }
+    for (int d = 0; d < ncomp; ++d) {
+      const R y = d == 0 ? y0 : y1;
       const size_t o = ((size_t)c * ncomp + d) * ND + i;
       if constexpr (MODE == 0) {
         x[o] = scale * y;
