@@ -13,7 +13,8 @@ from .schur import NAMES as SCHUR_NAMES
 class Options(ctypes.Structure):
     _fields_ = [("eps", ctypes.c_double), ("max_iterations", ctypes.c_int), ("fixed_point_tol", ctypes.c_double),
                 ("fixed_point_max_iterations", ctypes.c_int), ("gmres_restart", ctypes.c_int),
-                ("mass_solver", ctypes.c_int), ("schur_inner", ctypes.c_int), ("schur_preconditioner", ctypes.c_int)]
+                ("mass_solver", ctypes.c_int), ("schur_inner", ctypes.c_int), ("schur_preconditioner", ctypes.c_int),
+                ("schur_poly_degree", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -45,7 +46,7 @@ class IMEXStepper:
 
     def __init__(self, mesh, degree, Ma, Fr, dt, eps=None, max_iterations=None, fixed_point_tol=None,
                  fixed_point_max_iterations=None, gmres_restart=None, mass_solver=None, schur_inner=None,
-                 schur_preconditioner=None):
+                 schur_preconditioner=None, schur_poly_degree=None):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("IMEXStepper needs a CUDA device (no CPU fallback)")
@@ -56,7 +57,8 @@ class IMEXStepper:
         for k, v in (("eps", eps), ("max_iterations", max_iterations), ("fixed_point_tol", fixed_point_tol),
                      ("fixed_point_max_iterations", fixed_point_max_iterations), ("gmres_restart", gmres_restart),
                      ("mass_solver", mass_solver), ("schur_inner", schur_inner),
-                     ("schur_preconditioner", SCHUR_NAMES.get(schur_preconditioner, schur_preconditioner))):
+                     ("schur_preconditioner", SCHUR_NAMES.get(schur_preconditioner, schur_preconditioner)),
+                     ("schur_poly_degree", schur_poly_degree)):
             if v is not None:
                 setattr(opt, k, v)
         self.mesh, self.degree = mesh, degree
