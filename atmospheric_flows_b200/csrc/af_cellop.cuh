@@ -55,6 +55,22 @@ struct NfgOf<Phys, std::void_t<decltype(Phys::nfg_of(0))>> {
   static constexpr int get(int g) { return Phys::nfg_of(g); }
 };
 
+// Policies may declare a cell-local epilogue (Phys::EPI) that replaces the plain store:
+//   1: out = scale * M_K^{-1} y per cell and component (prm.Minv: packed cell inverses,
+//      cell-major, as written by the factor kernel);
+//   2: the Chebyshev step on a residual increment y:  r += y;  d' = alpha d + s M_K^{-1} r;
+//      x = d' (first) or x += d'   (prm.r, prm.din, prm.dout, prm.x, prm.Minv).  d' goes to
+//      its own array: other CTAs still read d's face nodes when the operator's input is d.
+// The CTA's inverse blocks are brought in by a bulk copy issued at kernel start.
+template <class Phys, class = void>
+struct EpiOf {
+  static constexpr int value = 0;
+};
+template <class Phys>
+struct EpiOf<Phys, std::void_t<decltype(Phys::EPI)>> {
+  static constexpr int value = Phys::EPI;
+};
+
 template <int N, class F, int... I>
 __device__ __forceinline__ void sfor_impl(F& f, std::integer_sequence<int, I...>) {
   (f(std::integral_constant<int, I>{}), ...);
@@ -235,7 +251,11 @@ struct Layout {
   static constexpr int R_FLUX = Phys::FACES ? 4 * NOUT * CB * NQ : 0;
   static constexpr int R_GEO = CB * 24;  // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb
   static constexpr int R_S = NQ * P1 + NQ;
-  static constexpr int TOTAL = RA + RB + R_FLUX + R_GEO + R_S;
+  // region E (epilogue policies): the CTA's packed cell inverses, 16-byte aligned
+  static constexpr int EPI = EpiOf<Phys>::value;
+  static constexpr int NPK = ND * (ND + 1) / 2;
+  static constexpr int OE = (RA + RB + R_FLUX + R_GEO + R_S + ALIGN - 1) / ALIGN * ALIGN;
+  static constexpr int TOTAL = EPI ? OE + CB * NPK : RA + RB + R_FLUX + R_GEO + R_S;
   static constexpr size_t BYTES = sizeof(R) * TOTAL;
 };
 
@@ -335,6 +355,31 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   }
   unsigned bar_phase = 0;
   bool abort = false;
+  // epilogue policies: the CTA's inverse blocks, copied from kernel start on
+  __shared__ alignas(8) unsigned long long s_bar_e;
+  const unsigned bar_e = (unsigned)__cvta_generic_to_shared(&s_bar_e);
+  R* s_minv = smem + L::OE;
+  bool epi_bulk = false;
+  if constexpr (L::EPI != 0) {
+    const int c0e = blockIdx.x * CB, ncbe = min(CB, ncell - c0e);
+    const size_t bytes = sizeof(R) * (size_t)ncbe * L::NPK;
+    const R* srcm = prm.Minv + (size_t)c0e * L::NPK;
+    epi_bulk = bytes % 16 == 0 && (reinterpret_cast<size_t>(srcm) & 15) == 0;
+    if (epi_bulk) {
+      if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_e) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar_e), "r"((unsigned)bytes)
+                     : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                         (unsigned)__cvta_generic_to_shared(s_minv)),
+                     "l"(srcm), "r"((unsigned)bytes), "r"(bar_e)
+                     : "memory");
+      }
+    } else {
+      for (int e = threadIdx.x; e < ncbe * L::NPK; e += L::NT) cp_async_el(&s_minv[e], srcm + e);
+    }
+  }
 
   const int tid = threadIdx.x;
   const int m = tid / CB;   // member: row / column / face point
@@ -555,7 +600,13 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     }
   });
-  if (abort) return;
+  if (abort) {  // a staging wait gave up: wait (bounded) for this CTA's copies before leaving
+    if (tid == 0) {
+      if (L::BULK) mbar_wait(bar, bar_phase ^ 1u);
+      if (epi_bulk) mbar_wait(bar_e, 0);
+    }
+    return;
+  }
   __syncthreads();
 
   // ================= merged z pass: member = quadrature column qx =================
@@ -740,19 +791,76 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     for (int ix = 0; ix < P1; ++ix) dst[ix] = out[ix];
   }
   __syncthreads();
-  // ---- store (coalesced)
-  sfor<Phys::NOUT_ARR>([&](auto oc) {
-    constexpr int OA = decltype(oc)::value;
-    constexpr int NC = Phys::out_ncomp(OA);
-    constexpr int ob = [] { int b = 0; for (int a = 0; a < OA; ++a) b += Phys::out_ncomp(a); return b; }();
-    R* dst = ptr.out[OA] + (size_t)c0 * NC * ND;
-    for (int e = tid; e < ncb * NC * ND; e += NT) {
-      const int cc = e / (NC * ND), r = e % (NC * ND);
-      const R v = s_out[((ob + r / ND) * CB + cc) * L::NDP + r % ND];
-      if (Phys::ACCUMULATE) dst[e] += v;
-      else dst[e] = v;
+  if constexpr (L::EPI == 0) {
+    // ---- store (coalesced)
+    sfor<Phys::NOUT_ARR>([&](auto oc) {
+      constexpr int OA = decltype(oc)::value;
+      constexpr int NC = Phys::out_ncomp(OA);
+      constexpr int ob = [] { int b = 0; for (int a = 0; a < OA; ++a) b += Phys::out_ncomp(a); return b; }();
+      R* dst = ptr.out[OA] + (size_t)c0 * NC * ND;
+      for (int e = tid; e < ncb * NC * ND; e += NT) {
+        const int cc = e / (NC * ND), r = e % (NC * ND);
+        const R v = s_out[((ob + r / ND) * CB + cc) * L::NDP + r % ND];
+        if (Phys::ACCUMULATE) dst[e] += v;
+        else dst[e] = v;
+      }
+    });
+  } else {
+    // ---- cell-local epilogue: the inverse blocks (copied since kernel start)
+    if (epi_bulk) {
+      const bool ok = mbar_wait(bar_e, 0);
+      if (!ok) atomicExch(&g_af_stage_timeout, 1);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) mbar_wait(bar_e, 0);
+        return;
+      }
+    } else {
+      cp_async_wait_all();
+      __syncthreads();
     }
-  });
+    R* s_y = smem;  // region A is free after the x-transpose pass
+    constexpr int NPK = L::NPK;
+    if constexpr (L::EPI == 2) {
+      // r += y (stored), kept in s_y for the inverse
+      R* r = prm.r + (size_t)c0 * ND;
+      for (int e = tid; e < ncb * ND; e += NT) {
+        const int cc = e / ND, k = e % ND;
+        const R rn = r[e] + s_out[cc * L::NDP + k];
+        r[e] = rn;
+        s_y[cc * ND + k] = rn;
+      }
+      __syncthreads();
+    }
+    // tasks (cell, row i): all components of the cell's row share each inverse entry
+    for (int e = tid; e < ncb * ND; e += NT) {
+      const int cc = e / ND, i = e % ND;
+      const R* M = s_minv + cc * NPK;
+      const int ri = i * (i + 1) / 2;
+      R y[NOUT];
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) y[o] = R(0);
+#pragma unroll
+      for (int j = 0; j < ND; ++j) {
+        const R m = M[j <= i ? ri + j : j * (j + 1) / 2 + i];
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) {
+          const R v = L::EPI == 2 ? s_y[cc * ND + j] : s_out[(o * CB + cc) * L::NDP + j];
+          y[o] = fmaR(m, v, y[o]);
+        }
+      }
+      if constexpr (L::EPI == 1) {
+        // one output array, NOUT components, [cell][comp][node]
+        R* dst = ptr.out[0] + (size_t)(c0 + cc) * NOUT * ND;
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) dst[o * ND + i] = prm.scale * y[o];
+      } else {
+        const size_t g = (size_t)(c0 + cc) * ND + i;
+        const R nd = (prm.alpha != R(0) ? prm.alpha * prm.din[g] : R(0)) + prm.s * y[0];
+        prm.dout[g] = nd;
+        prm.x[g] = prm.first ? nd : prm.x[g] + nd;
+      }
+    }
+  }
 }
 
 template <int P, class Phys, int CB_ = cells_per_block<P>(), int MINB = min_blocks_per_sm<P>()>

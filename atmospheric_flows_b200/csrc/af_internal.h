@@ -85,6 +85,18 @@ struct DegreeOps {
                               double* dst, int ncell, cudaStream_t);
   cudaError_t (*op_CT)(const MeshDev&, const double* w, const double* pf, const double* pbar, const CParams&,
                        double* wbar, int ncell, cudaStream_t);
+
+  // ---- fused cell-kernel epilogues in FP32 (packed inverses LA / LM from mass_factor) ----
+  // w = scale A^{-1} (B p) with B's coefficient c: one launch for B and the cell-wise solve
+  cudaError_t (*b_inv_f)(const MeshDev&, const float* p, float c, const float* LA, float scale, float* w, int ncell,
+                         cudaStream_t);
+  // the smoother step:  r += C0 w - D din;  dout = alpha din + s M^{-1} r;  x = dout (first) or
+  // x += dout.  prm.g1 carries +1/(gamma-1) as for mg_res; din and dout are distinct arrays.
+  // (FP64 counterparts measured slower than the separate launches: twice the inverse bytes in
+  // shared memory halve the occupancy of the FP64 kernels.)
+  cudaError_t (*res_cheb_f)(const MeshDev&, const float* w, const float* pf, const float* din,
+                            const CParamsT<float>&, const float* LM, float alpha, float s, float* r, float* dout,
+                            float* x, int first, int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

@@ -563,6 +563,36 @@ cudaError_t op_CT(const MeshDev& mesh, const double* w, const double* pf, const 
   return launch_cellop<P, CTPhys>(mesh, a, prm, ncell, st);
 }
 
+// ------------------------------------------------------------------ fused epilogues
+template <class R>
+cudaError_t b_inv(const MeshDev& mesh, const R* p, R c, const R* LA, R scale, R* w, int ncell, cudaStream_t st) {
+  ArgPtrs<1, 1, R> a{{p}, {w}};
+  BInvParams<R> q;
+  q.c = c;
+  q.Minv = LA;
+  q.scale = scale;
+  return launch_cellop<P, BInvPhys<R>>(mesh, a, q, ncell, st);
+}
+
+template <class R>
+cudaError_t res_cheb(const MeshDev& mesh, const R* w, const R* pf, const R* din, const CParamsT<R>& prm, const R* LM,
+                     R alpha, R s, R* r, R* dout, R* x, int first, int ncell, cudaStream_t st) {
+  if (din == dout) return cudaErrorInvalidValue;
+  ArgPtrs<3, 1, R> a{{din, w, pf}, {r}};
+  ResChebParams<R> q;
+  static_cast<CParamsT<R>&>(q) = prm;
+  q.g1 = -prm.g1;
+  q.Minv = LM;
+  q.alpha = alpha;
+  q.s = s;
+  q.r = r;
+  q.din = din;
+  q.dout = dout;
+  q.x = x;
+  q.first = first;
+  return launch_cellop<P, ResChebPhys<R>>(mesh, a, q, ncell, st);
+}
+
 constexpr int kTransferThreads = 256;
 
 template <class R>
@@ -595,7 +625,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         restrict_<double>, restrict_<float>,
                         inject,            rhs_adjoint1,
                         rhs_tangent1,      op_BT,
-                        op_C_tangent,      op_CT};
+                        op_C_tangent,      op_CT,
+                        b_inv<float>,      res_cheb<float>};
 
 }  // namespace
 

@@ -30,6 +30,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/af_gpu.h"
@@ -184,8 +185,15 @@ int alloc(af_schur_solver* s, void** p, size_t bytes) {
 
 template <class R>
 struct Prec;
+// kFused: the level's smoother runs B with the cell-wise A^{-1} in its epilogue, and the
+// residual update with the Chebyshev step in its epilogue (two launches per smoothing step
+// instead of four).  FP32 only: the FP64 kernels hold twice the inverse bytes in shared
+// memory, which halves their occupancy, and their extra FP64 epilogue work costs more than
+// the saved vector traffic (504 vs 417 us for B + A^{-1}, 704 vs 518 us for the residual and
+// Chebyshev step, 1024x256, p = 4).
 template <>
 struct Prec<double> {
+  static constexpr bool kFused = false;
   static cudaError_t B(const DegreeOps* k, const MeshDev& m, const double* p, double c, double* u, int nc,
                        cudaStream_t st) {
     return k->op_B(m, p, c, u, nc, st);
@@ -212,6 +220,7 @@ struct Prec<double> {
 };
 template <>
 struct Prec<float> {
+  static constexpr bool kFused = true;
   static cudaError_t B(const DegreeOps* k, const MeshDev& m, const float* p, double c, float* u, int nc,
                        cudaStream_t st) {
     return k->mg_B_f(m, p, (float)c, u, nc, st);
@@ -229,6 +238,16 @@ struct Prec<float> {
                           int first, int nc, cudaStream_t st) {
     return k->cheb_f(L, r, (float)a, (float)s, d, x, first, nc, st);
   }
+  static cudaError_t b_inv(const DegreeOps* k, const MeshDev& m, const float* p, double c, const float* LA, float* w,
+                           int nc, cudaStream_t st) {
+    return k->b_inv_f(m, p, (float)c, LA, 1.0f, w, nc, st);
+  }
+  static cudaError_t res_cheb(const DegreeOps* k, const MeshDev& m, const float* w, const float* pf, const float* din,
+                              double cdt, const float* LM, double a, double s, float* r, float* dout, float* x, int nc,
+                              cudaStream_t st) {
+    CParamsT<float> q{(float)cdt, (float)kG1, (float)kGG};
+    return k->res_cheb_f(m, w, pf, din, q, LM, (float)a, (float)s, r, dout, x, 0, nc, st);
+  }
   static cudaError_t prolong(const DegreeOps* k, const float* xc, float* xf, int nxc, int nzc, cudaStream_t st) {
     return k->prolong_f(xc, xf, nxc, nzc, st);
   }
@@ -242,10 +261,16 @@ template <class R>
 int residual_update(af_schur_solver* s, Level& L, const R* v, R* r) {
   af_operator* o = s->op;
   const DegreeOps* k = o->ops;
-  MG_CU(Prec<R>::B(k, L.mesh, v, s->cB, (R*)L.u, L.ncell, o->stream));
-  MG_CU(Prec<R>::solve(k, (const R*)L.LA, 2, (const R*)L.u, 1.0, (R*)L.w, L.ncell, o->stream));
+  if constexpr (Prec<R>::kFused) {  // w = A^{-1} B v in one launch
+    MG_CU(Prec<R>::b_inv(k, L.mesh, v, s->cB, (const R*)L.LA, (R*)L.w, L.ncell, o->stream));
+    o->launches += 1;
+  } else {
+    MG_CU(Prec<R>::B(k, L.mesh, v, s->cB, (R*)L.u, L.ncell, o->stream));
+    MG_CU(Prec<R>::solve(k, (const R*)L.LA, 2, (const R*)L.u, 1.0, (R*)L.w, L.ncell, o->stream));
+    o->launches += 2;
+  }
   MG_CU(Prec<R>::res(k, L.mesh, (const R*)L.w, (const R*)L.pfR, v, s->cdt, r, L.ncell, o->stream));
-  o->launches += 3;
+  o->launches += 1;
   return AF_OK;
 }
 
@@ -259,6 +284,7 @@ int chebyshev(af_schur_solver* s, Level& L, int degree, double lo, double hi, bo
   R* x = (R*)L.x;
   R* r = (R*)L.r;
   R* d = (R*)L.d;
+  R* dn = (R*)L.u;  // the next d: the fused step reads d's face nodes from other CTAs
   const R* b = (const R*)L.b;
   const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
   const double ginv = 1.0 / kG1;  // D^{-1} = (gamma-1) M^{-1}
@@ -268,10 +294,20 @@ int chebyshev(af_schur_solver* s, Level& L, int degree, double lo, double hi, bo
   o->launches += 1;
   double rho_old = 1.0 / sigma;
   for (int it = 1; it < degree; ++it) {
-    MG_AF(residual_update<R>(s, L, d, r));
     const double rho = 1.0 / (2.0 * sigma - rho_old);
-    MG_CU(Prec<R>::cheb(k, (const R*)L.LM, r, rho * rho_old, ginv * 2.0 * rho / delta, d, x, 0, L.ncell, o->stream));
-    o->launches += 1;
+    const double a = rho * rho_old, sc = ginv * 2.0 * rho / delta;
+    if constexpr (Prec<R>::kFused) {
+      // w = A^{-1} B d;  r += C0 w - D d;  dn = a d + sc M^{-1} r;  x += dn  (two launches)
+      MG_CU(Prec<R>::b_inv(k, L.mesh, d, s->cB, (const R*)L.LA, (R*)L.w, L.ncell, o->stream));
+      MG_CU(Prec<R>::res_cheb(k, L.mesh, (const R*)L.w, (const R*)L.pfR, d, s->cdt, (const R*)L.LM, a, sc, r, dn, x,
+                              L.ncell, o->stream));
+      o->launches += 2;
+      std::swap(d, dn);
+    } else {
+      MG_AF(residual_update<R>(s, L, d, r));
+      MG_CU(Prec<R>::cheb(k, (const R*)L.LM, r, a, sc, d, x, 0, L.ncell, o->stream));
+      o->launches += 1;
+    }
     rho_old = rho;
   }
   if (final_residual) MG_AF(residual_update<R>(s, L, d, r));

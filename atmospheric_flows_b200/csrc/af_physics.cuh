@@ -249,6 +249,18 @@ struct BPhysT {
 };
 using BPhys = BPhysT<double>;
 
+// B followed by the cell-wise A^{-1} in the kernel's epilogue: w = scale A^{-1} B p.
+template <class R>
+struct BInvParams : BParamsT<R> {
+  const R* Minv;  // packed cell inverses of A (cell-major)
+  R scale;
+};
+template <class R = double>
+struct BInvPhys : BPhysT<R> {
+  using Params = BInvParams<R>;
+  static constexpr int EPI = 1;
+};
+
 // ------------------------------------------- C (u -> p), optionally D p - C w (Schur)
 template <class R>
 struct CParamsT {
@@ -308,6 +320,25 @@ struct CPhys {
   }
   template <int G>
   __device__ __forceinline__ static void boundary(const Params&, const R*, const R*, R*) {}
+};
+
+// The multigrid smoother's residual update followed by its Chebyshev step in the kernel's
+// epilogue (the linearised Schur operator: r += C0 w - D d, then d' = alpha d + s M^{-1} r,
+// x += d').  Inputs as CPhys<true, +1>: d (the D term), w, p_fixed; g1 carries -1/(gamma-1).
+template <class R>
+struct ResChebParams : CParamsT<R> {
+  const R* Minv;  // packed cell inverses of M
+  R alpha, s;
+  R* r;
+  const R* din;  // the operator's input d (own cells read again for alpha d)
+  R* dout;
+  R* x;
+  int first;
+};
+template <class R>
+struct ResChebPhys : CPhys<true, 1, R, false, true> {
+  using Params = ResChebParams<R>;
+  static constexpr int EPI = 2;
 };
 
 // ---------------------------------------------------------------- mass-type operators
