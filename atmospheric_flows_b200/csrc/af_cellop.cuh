@@ -55,13 +55,14 @@ struct NfgOf<Phys, std::void_t<decltype(Phys::nfg_of(0))>> {
   static constexpr int get(int g) { return Phys::nfg_of(g); }
 };
 
-// Policies may declare a cell-local epilogue (Phys::EPI) that replaces the plain store:
-//   1: out = scale * M_K^{-1} y per cell and component (prm.Minv: packed cell inverses,
-//      cell-major, as written by the factor kernel);
+// Policies may declare a cell-local epilogue (Phys::EPI) that replaces the plain store.  Both
+// apply a cell-wise inverse mass matrix by the change of basis to the Gauss points (CobT):
+//   M_K^{-1} y = Vi (W_K (Vi^T y)),  W_K = prm.inv[cell][q] = 1 / (rho(g_q) JxW(g_q)),
+//   1: out = scale * M_K^{-1} y per cell and component;
 //   2: the Chebyshev step on a residual increment y:  r += y;  d' = alpha d + s M_K^{-1} r;
-//      x = d' (first) or x += d'   (prm.r, prm.din, prm.dout, prm.x, prm.Minv).  d' goes to
-//      its own array: other CTAs still read d's face nodes when the operator's input is d.
-// The CTA's inverse blocks are brought in by a bulk copy issued at kernel start.
+//      x = d' (first) or x += d'   (prm.r, prm.din, prm.dout, prm.x).  d' goes to its own
+//      array: other CTAs still read d's face nodes when the operator's input is d.
+// The CTA's weights are brought in by a bulk copy issued at kernel start.
 template <class Phys, class = void>
 struct EpiOf {
   static constexpr int value = 0;
@@ -88,6 +89,9 @@ template <int P>
 __device__ __forceinline__ const Tab<P>& tab() {
   return tabr<P, double>();
 }
+// change-of-basis tables (cell-wise inverse mass matrices without stored matrices)
+template <int P, class R>
+__device__ __forceinline__ const CobT<P, R>& cobr();
 
 // Fused multiply-add in the working precision (no silent promotion of float operands).
 __device__ __forceinline__ double fmaR(double a, double b, double c) { return __fma_rn(a, b, c); }
@@ -251,11 +255,12 @@ struct Layout {
   static constexpr int R_FLUX = Phys::FACES ? 4 * NOUT * CB * NQ : 0;
   static constexpr int R_GEO = CB * 24;  // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb
   static constexpr int R_S = NQ * P1 + NQ;
-  // region E (epilogue policies): the CTA's packed cell inverses, 16-byte aligned
+  // region E (epilogue policies): the CTA's Gauss-point inverse weights, 16-byte aligned
   static constexpr int EPI = EpiOf<Phys>::value;
-  static constexpr int NPK = ND * (ND + 1) / 2;
   static constexpr int OE = (RA + RB + R_FLUX + R_GEO + R_S + ALIGN - 1) / ALIGN * ALIGN;
-  static constexpr int TOTAL = EPI ? OE + CB * NPK : RA + RB + R_FLUX + R_GEO + R_S;
+  static constexpr int TOTAL = EPI ? OE + CB * ND : RA + RB + R_FLUX + R_GEO + R_S;
+  // the epilogue's scratch (input rows and half-transformed values) lives in region A
+  static_assert(EPI == 0 || RA >= (NOUT + 1) * CB * ND, "region A too small for the epilogue");
   static constexpr size_t BYTES = sizeof(R) * TOTAL;
 };
 
@@ -355,15 +360,15 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   }
   unsigned bar_phase = 0;
   bool abort = false;
-  // epilogue policies: the CTA's inverse blocks, copied from kernel start on
+  // epilogue policies: the CTA's inverse weights, copied from kernel start on
   __shared__ alignas(8) unsigned long long s_bar_e;
   const unsigned bar_e = (unsigned)__cvta_generic_to_shared(&s_bar_e);
   R* s_minv = smem + L::OE;
   bool epi_bulk = false;
   if constexpr (L::EPI != 0) {
     const int c0e = blockIdx.x * CB, ncbe = min(CB, ncell - c0e);
-    const size_t bytes = sizeof(R) * (size_t)ncbe * L::NPK;
-    const R* srcm = prm.Minv + (size_t)c0e * L::NPK;
+    const size_t bytes = sizeof(R) * (size_t)ncbe * ND;
+    const R* srcm = prm.inv + (size_t)c0e * ND;
     epi_bulk = bytes % 16 == 0 && (reinterpret_cast<size_t>(srcm) & 15) == 0;
     if (epi_bulk) {
       if (threadIdx.x == 0) {
@@ -377,7 +382,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
                      : "memory");
       }
     } else {
-      for (int e = threadIdx.x; e < ncbe * L::NPK; e += L::NT) cp_async_el(&s_minv[e], srcm + e);
+      for (int e = threadIdx.x; e < ncbe * ND; e += L::NT) cp_async_el(&s_minv[e], srcm + e);
     }
   }
 
@@ -806,7 +811,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     });
   } else {
-    // ---- cell-local epilogue: the inverse blocks (copied since kernel start)
+    // ---- cell-local epilogue: the inverse weights (copied since kernel start)
     if (epi_bulk) {
       const bool ok = mbar_wait(bar_e, 0);
       if (!ok) atomicExch(&g_af_stage_timeout, 1);
@@ -818,10 +823,13 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       cp_async_wait_all();
       __syncthreads();
     }
-    R* s_y = smem;  // region A is free after the x-transpose pass
-    constexpr int NPK = L::NPK;
+    // region A is free after the x-transpose pass: s_y = the (cell, component) input rows
+    // (EPI 2: the updated residual), s_u = the values between the passes
+    constexpr int NC = L::EPI == 1 ? NOUT : 1;
+    R* s_y = smem;
+    R* s_u = smem + CB * ND;
+    const CobT<P, R>& cb = cobr<P, R>();
     if constexpr (L::EPI == 2) {
-      // r += y (stored), kept in s_y for the inverse
       R* r = prm.r + (size_t)c0 * ND;
       for (int e = tid; e < ncb * ND; e += NT) {
         const int cc = e / ND, k = e % ND;
@@ -831,33 +839,69 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
       __syncthreads();
     }
-    // tasks (cell, row i): all components of the cell's row share each inverse entry
-    for (int e = tid; e < ncb * ND; e += NT) {
-      const int cc = e / ND, i = e % ND;
-      const R* M = s_minv + cc * NPK;
-      const int ri = i * (i + 1) / 2;
-      R y[NOUT];
+    auto yin = [&](int o, int cc, int k) -> R {
+      if constexpr (L::EPI == 2) return s_y[cc * ND + k];
+      else return s_out[(o * CB + cc) * L::NDP + k];
+    };
+    // pass 1 (along x): u[iz][qx] = sum_ix Vi[ix][qx] y[iz][ix]; task (component, cell, row)
+    for (int e = tid; e < NC * ncb * P1; e += NT) {
+      const int o = e / (ncb * P1), cc = (e / P1) % ncb, iz = e % P1;
+      R yr[P1];
 #pragma unroll
-      for (int o = 0; o < NOUT; ++o) y[o] = R(0);
+      for (int ix = 0; ix < P1; ++ix) yr[ix] = yin(o, cc, iz * P1 + ix);
 #pragma unroll
-      for (int j = 0; j < ND; ++j) {
-        const R m = M[j <= i ? ri + j : j * (j + 1) / 2 + i];
+      for (int qx = 0; qx < P1; ++qx) {
+        R t = R(0);
 #pragma unroll
-        for (int o = 0; o < NOUT; ++o) {
-          const R v = L::EPI == 2 ? s_y[cc * ND + j] : s_out[(o * CB + cc) * L::NDP + j];
-          y[o] = fmaR(m, v, y[o]);
-        }
+        for (int ix = 0; ix < P1; ++ix) t = fmaR(cb.Vi[ix][qx], yr[ix], t);
+        s_u[(o * CB + cc) * ND + iz * P1 + qx] = t;
       }
-      if constexpr (L::EPI == 1) {
-        // one output array, NOUT components, [cell][comp][node]
-        R* dst = ptr.out[0] + (size_t)(c0 + cc) * NOUT * ND;
+    }
+    __syncthreads();
+    // pass 2 (along z, per column qx): to the Gauss points, times the weights, and back
+    for (int e = tid; e < NC * ncb * P1; e += NT) {
+      const int o = e / (ncb * P1), cc = (e / P1) % ncb, qx = e % P1;
+      R* col = s_u + (o * CB + cc) * ND + qx;
+      R u[P1], t[P1];
 #pragma unroll
-        for (int o = 0; o < NOUT; ++o) dst[o * ND + i] = prm.scale * y[o];
-      } else {
-        const size_t g = (size_t)(c0 + cc) * ND + i;
-        const R nd = (prm.alpha != R(0) ? prm.alpha * prm.din[g] : R(0)) + prm.s * y[0];
-        prm.dout[g] = nd;
-        prm.x[g] = prm.first ? nd : prm.x[g] + nd;
+      for (int iz = 0; iz < P1; ++iz) u[iz] = col[iz * P1];
+#pragma unroll
+      for (int qz = 0; qz < P1; ++qz) {
+        R a = R(0);
+#pragma unroll
+        for (int iz = 0; iz < P1; ++iz) a = fmaR(cb.Vi[iz][qz], u[iz], a);
+        t[qz] = a * s_minv[cc * ND + qz * P1 + qx];
+      }
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) {
+        R a = R(0);
+#pragma unroll
+        for (int qz = 0; qz < P1; ++qz) a = fmaR(cb.Vi[iz][qz], t[qz], a);
+        col[iz * P1] = a;
+      }
+    }
+    __syncthreads();
+    // pass 3 (along x): x[iz][ix] = sum_qx Vi[ix][qx] v[iz][qx], then the store or update
+    for (int e = tid; e < NC * ncb * P1; e += NT) {
+      const int o = e / (ncb * P1), cc = (e / P1) % ncb, iz = e % P1;
+      const R* row = s_u + (o * CB + cc) * ND + iz * P1;
+      R v[P1];
+#pragma unroll
+      for (int qx = 0; qx < P1; ++qx) v[qx] = row[qx];
+#pragma unroll
+      for (int ix = 0; ix < P1; ++ix) {
+        R y = R(0);
+#pragma unroll
+        for (int qx = 0; qx < P1; ++qx) y = fmaR(cb.Vi[ix][qx], v[qx], y);
+        if constexpr (L::EPI == 1) {
+          // one output array, NOUT components, [cell][comp][node]
+          ptr.out[0][((size_t)(c0 + cc) * NOUT + o) * ND + iz * P1 + ix] = prm.scale * y;
+        } else {
+          const size_t g = (size_t)(c0 + cc) * ND + iz * P1 + ix;
+          const R nd = (prm.alpha != R(0) ? prm.alpha * prm.din[g] : R(0)) + prm.s * y;
+          prm.dout[g] = nd;
+          prm.x[g] = prm.first ? nd : prm.x[g] + nd;
+        }
       }
     }
   }

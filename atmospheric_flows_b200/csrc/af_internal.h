@@ -47,22 +47,15 @@ struct DegreeOps {
   int factor_len;  // (p+1)^2 ((p+1)^2 + 1) / 2
 
   // ---- h-multigrid level kernels, in FP64 (_d) and FP32 (_f) ----
-  // u = B p (BPhys, coefficient c = coeff dt / Ma^2)
-  cudaError_t (*mg_B_f)(const MeshDev&, const float* p, float c, float* u, int ncell, cudaStream_t);
   // r += C0 w - D p: the residual update of the linearised Schur complement (C0 = C
   // without the wave-speed term); prm.g1 carries +1/(gamma-1)
   cudaError_t (*mg_res_d)(const MeshDev&, const double* w, const double* pf, const double* p, const CParams&,
                           double* r, int ncell, cudaStream_t);
   cudaError_t (*mg_res_f)(const MeshDev&, const float* w, const float* pf, const float* p, const CParamsT<float>&,
                           float* r, int ncell, cudaStream_t);
-  // x = M_K^{-1} b per cell with the packed inverses in FP32
-  cudaError_t (*mass_solve_f)(const float* L, int ncomp, const float* b, float scale, float* x, int ncell,
-                              cudaStream_t);
-  // Chebyshev update with the cell-wise inverse D^{-1} = s M^{-1}:
+  // Chebyshev update with the packed cell-wise inverse D^{-1} = s M^{-1} (FP64 levels):
   //   d = alpha d + s M^{-1} r  (alpha == 0: d not read);  x = d (first) or x += d
   cudaError_t (*cheb_d)(const double* L, const double* r, double alpha, double s, double* d, double* x, int first,
-                        int ncell, cudaStream_t);
-  cudaError_t (*cheb_f)(const float* L, const float* r, float alpha, float s, float* d, float* x, int first,
                         int ncell, cudaStream_t);
   // xf += P xc (coarse nx_c x nz_c cells, fine 2nx_c x 2nz_c); rc = P^T rf
   cudaError_t (*prolong_d)(const double* xc, double* xf, int nxc, int nzc, cudaStream_t);
@@ -86,16 +79,22 @@ struct DegreeOps {
   cudaError_t (*op_CT)(const MeshDev&, const double* w, const double* pf, const double* pbar, const CParams&,
                        double* wbar, int ncell, cudaStream_t);
 
-  // ---- fused cell-kernel epilogues in FP32 (packed inverses LA / LM from mass_factor) ----
-  // w = scale A^{-1} (B p) with B's coefficient c: one launch for B and the cell-wise solve
-  cudaError_t (*b_inv_f)(const MeshDev&, const float* p, float c, const float* LA, float scale, float* w, int ncell,
+  // ---- FP32 level kernels with cell-wise inverses by the change of basis to the Gauss points
+  // (no stored matrices): W = 1 / (rho JxW) at the (P+1)^2 Gauss points, rho = 1 when null
+  cudaError_t (*cob_weights_f)(const MeshDev&, const double* rho, float* W, int ncell, cudaStream_t);
+  // x = scale M_W^{-1} b (ncomp 1 or 2)
+  cudaError_t (*cob_solve_f)(const float* W, int ncomp, const float* b, float scale, float* x, int ncell,
+                             cudaStream_t);
+  // d = alpha d + s M_W^{-1} r;  x = d (first) or x += d
+  cudaError_t (*cob_cheb_f)(const float* W, const float* r, float alpha, float s, float* d, float* x, int first,
+                            int ncell, cudaStream_t);
+  // w = scale A_W^{-1} (B p) with B's coefficient c: one launch for B and the cell-wise solve
+  cudaError_t (*b_inv_f)(const MeshDev&, const float* p, float c, const float* WA, float scale, float* w, int ncell,
                          cudaStream_t);
-  // the smoother step:  r += C0 w - D din;  dout = alpha din + s M^{-1} r;  x = dout (first) or
-  // x += dout.  prm.g1 carries +1/(gamma-1) as for mg_res; din and dout are distinct arrays.
-  // (FP64 counterparts measured slower than the separate launches: twice the inverse bytes in
-  // shared memory halve the occupancy of the FP64 kernels.)
+  // the smoother step:  r += C0 w - D din;  dout = alpha din + s M_W^{-1} r;  x = dout (first)
+  // or x += dout.  prm.g1 carries +1/(gamma-1) as for mg_res; din and dout are distinct arrays.
   cudaError_t (*res_cheb_f)(const MeshDev&, const float* w, const float* pf, const float* din,
-                            const CParamsT<float>&, const float* LM, float alpha, float s, float* r, float* dout,
+                            const CParamsT<float>&, const float* WM, float alpha, float s, float* r, float* dout,
                             float* x, int first, int ncell, cudaStream_t);
 };
 

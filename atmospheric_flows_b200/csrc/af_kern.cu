@@ -17,6 +17,8 @@ static __constant__ Tab<AF_P> c_tab;
 static __constant__ TabT<AF_P, float> c_tabf;
 static __constant__ TransT<AF_P, double> c_tr;
 static __constant__ TransT<AF_P, float> c_trf;
+static __constant__ CobT<AF_P, double> c_cob;
+static __constant__ CobT<AF_P, float> c_cobf;
 
 template <>
 __device__ __forceinline__ const Tab<AF_P>& tabr<AF_P, double>() {
@@ -25,6 +27,14 @@ __device__ __forceinline__ const Tab<AF_P>& tabr<AF_P, double>() {
 template <>
 __device__ __forceinline__ const TabT<AF_P, float>& tabr<AF_P, float>() {
   return c_tabf;
+}
+template <>
+__device__ __forceinline__ const CobT<AF_P, double>& cobr<AF_P, double>() {
+  return c_cob;
+}
+template <>
+__device__ __forceinline__ const CobT<AF_P, float>& cobr<AF_P, float>() {
+  return c_cobf;
 }
 
 namespace {
@@ -36,7 +46,11 @@ cudaError_t upload_tables() {
   static const TabT<P, float> tf = host::make_tab<P, float>();
   static const TransT<P, double> tr = host::make_trans<P, double>();
   static const TransT<P, float> trf = host::make_trans<P, float>();
+  static const CobT<P, double> cob = host::make_cob<P, double>();
+  static const CobT<P, float> cobf = host::make_cob<P, float>();
   cudaError_t e = cudaMemcpyToSymbol(c_tab, &t, sizeof(t));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cob, &cob, sizeof(cob));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cobf, &cobf, sizeof(cobf));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tabf, &tf, sizeof(tf));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tr, &tr, sizeof(tr));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_trf, &trf, sizeof(trf));
@@ -420,11 +434,6 @@ cudaError_t mass_solve(const double* L, int ncomp, const double* b, double scale
 }
 
 // ------------------------------------------------------------------ multigrid kernels
-cudaError_t mg_B_f(const MeshDev& mesh, const float* p, float c, float* u, int ncell, cudaStream_t st) {
-  ArgPtrs<1, 1, float> a{{p}, {u}};
-  return launch_cellop<P, BPhysT<float>>(mesh, a, BParamsT<float>{c}, ncell, st);
-}
-
 // r += C0 w - D p: CPhys with SIGN +1 gives +C0 w; the D term enters with -g1
 template <class R>
 cudaError_t mg_res(const MeshDev& mesh, const R* w, const R* pf, const R* p, const CParamsT<R>& prm, R* r, int ncell,
@@ -433,11 +442,6 @@ cudaError_t mg_res(const MeshDev& mesh, const R* w, const R* pf, const R* p, con
   CParamsT<R> q = prm;
   q.g1 = -prm.g1;
   return launch_cellop<P, CPhys<true, 1, R, false, true>>(mesh, a, q, ncell, st);
-}
-
-cudaError_t mass_solve_f(const float* L, int ncomp, const float* b, float scale, float* x, int ncell,
-                         cudaStream_t st) {
-  return launch_mass_solve<float, 0>(L, ncomp, b, scale, x, nullptr, 0.0f, 0, ncell, st);
 }
 
 template <class R>
@@ -563,26 +567,154 @@ cudaError_t op_CT(const MeshDev& mesh, const double* w, const double* pf, const 
   return launch_cellop<P, CTPhys>(mesh, a, prm, ncell, st);
 }
 
+// ------------------------------------------------------------------ change-of-basis inverses
+// Gauss-point inverse weights of a cell's mass matrix: W[c][qz (P+1) + qx] = 1 / (rho JxW) at
+// the (P+1)-point Gauss points (rho = 1 when null), for the sum-factorised inverse
+// M_K^{-1} = Vi diag(W) Vi^T of CobT (exact for the plain mass matrix on bilinear cells).
+template <class R>
+__global__ void k_cob_weights(const MeshDev mesh, const double* __restrict__ rho, R* __restrict__ W, const int ncell) {
+  constexpr int P1 = P + 1, ND = P1 * P1;
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long)ncell * ND) return;
+  const int c = (int)(e / ND), q = (int)(e % ND), qx = q % P1, qz = q / P1;
+  const CobT<P, double>& cb = c_cob;
+  const int i = c % mesh.nx, j = c / mesh.nx, Wd = mesh.nx + 1;
+  const double2 v0 = mesh.vtx[j * Wd + i], v1 = mesh.vtx[j * Wd + i + 1];
+  const double2 v2 = mesh.vtx[(j + 1) * Wd + i], v3 = mesh.vtx[(j + 1) * Wd + i + 1];
+  const double Ax = v1.x - v0.x, Az = v1.y - v0.y, Cx = v2.x - v0.x, Cz = v2.y - v0.y;
+  const double Bx = v3.x - v2.x - v1.x + v0.x, Bz = v3.y - v2.y - v1.y + v0.y;
+  const double xi = cb.g[qx], eta = cb.g[qz];
+  const double J00 = fma(Bx, eta, Ax), J10 = fma(Bz, eta, Az), J01 = fma(Bx, xi, Cx), J11 = fma(Bz, xi, Cz);
+  double f = (J00 * J11 - J01 * J10) * cb.w[qx] * cb.w[qz];
+  if (rho) {
+    const double* rc = rho + (size_t)c * ND;
+    double rv = 0.0;
+#pragma unroll
+    for (int iz = 0; iz < P1; ++iz) {
+      double t = 0.0;
+#pragma unroll
+      for (int ix = 0; ix < P1; ++ix) t = fma(cb.V[qx][ix], rc[iz * P1 + ix], t);
+      rv = fma(cb.V[qz][iz], t, rv);
+    }
+    f *= rv;
+  }
+  W[e] = (R)(1.0 / f);
+}
+
+// x = scale M_K^{-1} b per cell and component by the change of basis (MODE 0), or the
+// Chebyshev update d = alpha d + scale M_K^{-1} b, x = d (first) or x += d (MODE 1, ncomp 1).
+// Tasks are (component, cell, line) over three passes in shared memory.
+constexpr int kCobCells = 32;
+template <class R, int MODE>
+__global__ void __launch_bounds__(128)
+    k_cob_solve(const R* __restrict__ W, const R* __restrict__ b, R* __restrict__ x, R* __restrict__ dv,
+                const R scale, const R alpha, const int first, const int ncomp, const int ncell) {
+  constexpr int P1 = P + 1, ND = P1 * P1;
+  __shared__ R sy[kCobCells * 2 * ND];
+  __shared__ R sw[kCobCells * ND];
+  const CobT<P, R>& cb = cobr<P, R>();
+  const int c0 = blockIdx.x * kCobCells, ncb = min(kCobCells, ncell - c0);
+  for (int e = threadIdx.x; e < ncb * ncomp * ND; e += blockDim.x) sy[e] = b[(size_t)c0 * ncomp * ND + e];
+  for (int e = threadIdx.x; e < ncb * ND; e += blockDim.x) sw[e] = W[(size_t)c0 * ND + e];
+  __syncthreads();
+  const int nt = ncomp * ncb * P1;  // tasks (cell, component, line); sy is [cell][comp][node]
+  for (int e = threadIdx.x; e < nt; e += blockDim.x) {  // along x, in place per row
+    R* row = sy + (e / P1) * ND + (e % P1) * P1;
+    R y[P1];
+#pragma unroll
+    for (int ix = 0; ix < P1; ++ix) y[ix] = row[ix];
+#pragma unroll
+    for (int qx = 0; qx < P1; ++qx) {
+      R t = R(0);
+#pragma unroll
+      for (int ix = 0; ix < P1; ++ix) t = fmaR(cb.Vi[ix][qx], y[ix], t);
+      row[qx] = t;
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nt; e += blockDim.x) {  // along z per column, weights, back
+    const int cc = e / (ncomp * P1), qx = e % P1;
+    R* col = sy + (e / P1) * ND + qx;
+    R u[P1], t[P1];
+#pragma unroll
+    for (int iz = 0; iz < P1; ++iz) u[iz] = col[iz * P1];
+#pragma unroll
+    for (int qz = 0; qz < P1; ++qz) {
+      R a = R(0);
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) a = fmaR(cb.Vi[iz][qz], u[iz], a);
+      t[qz] = a * sw[cc * ND + qz * P1 + qx];
+    }
+#pragma unroll
+    for (int iz = 0; iz < P1; ++iz) {
+      R a = R(0);
+#pragma unroll
+      for (int qz = 0; qz < P1; ++qz) a = fmaR(cb.Vi[iz][qz], t[qz], a);
+      col[iz * P1] = a;
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nt; e += blockDim.x) {  // along x, then the store or update
+    const R* row = sy + (e / P1) * ND + (e % P1) * P1;
+    R v[P1];
+#pragma unroll
+    for (int qx = 0; qx < P1; ++qx) v[qx] = row[qx];
+#pragma unroll
+    for (int ix = 0; ix < P1; ++ix) {
+      R y = R(0);
+#pragma unroll
+      for (int qx = 0; qx < P1; ++qx) y = fmaR(cb.Vi[ix][qx], v[qx], y);
+      const size_t g = (size_t)c0 * ncomp * ND + (size_t)(e / P1) * ND + (e % P1) * P1 + ix;
+      if constexpr (MODE == 0) {
+        x[g] = scale * y;
+      } else {
+        const R nd = (alpha != R(0) ? alpha * dv[g] : R(0)) + scale * y;
+        dv[g] = nd;
+        x[g] = first ? nd : x[g] + nd;
+      }
+    }
+  }
+}
+
+template <class R>
+cudaError_t cob_weights(const MeshDev& mesh, const double* rho, R* W, int ncell, cudaStream_t st) {
+  const long n = (long)ncell * kND;
+  k_cob_weights<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(mesh, rho, W, ncell);
+  return cudaGetLastError();
+}
+template <class R>
+cudaError_t cob_solve(const R* W, int ncomp, const R* b, R scale, R* x, int ncell, cudaStream_t st) {
+  if (ncomp < 1 || ncomp > 2) return cudaErrorInvalidValue;
+  k_cob_solve<R, 0><<<(ncell + kCobCells - 1) / kCobCells, 128, 0, st>>>(W, b, x, nullptr, scale, R(0), 0, ncomp,
+                                                                         ncell);
+  return cudaGetLastError();
+}
+template <class R>
+cudaError_t cob_cheb(const R* W, const R* r, R alpha, R s, R* d, R* x, int first, int ncell, cudaStream_t st) {
+  k_cob_solve<R, 1><<<(ncell + kCobCells - 1) / kCobCells, 128, 0, st>>>(W, r, x, d, s, alpha, first, 1, ncell);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ fused epilogues
 template <class R>
-cudaError_t b_inv(const MeshDev& mesh, const R* p, R c, const R* LA, R scale, R* w, int ncell, cudaStream_t st) {
+cudaError_t b_inv(const MeshDev& mesh, const R* p, R c, const R* WA, R scale, R* w, int ncell, cudaStream_t st) {
   ArgPtrs<1, 1, R> a{{p}, {w}};
   BInvParams<R> q;
   q.c = c;
-  q.Minv = LA;
+  q.inv = WA;
   q.scale = scale;
   return launch_cellop<P, BInvPhys<R>>(mesh, a, q, ncell, st);
 }
 
 template <class R>
-cudaError_t res_cheb(const MeshDev& mesh, const R* w, const R* pf, const R* din, const CParamsT<R>& prm, const R* LM,
+cudaError_t res_cheb(const MeshDev& mesh, const R* w, const R* pf, const R* din, const CParamsT<R>& prm, const R* WM,
                      R alpha, R s, R* r, R* dout, R* x, int first, int ncell, cudaStream_t st) {
   if (din == dout) return cudaErrorInvalidValue;
   ArgPtrs<3, 1, R> a{{din, w, pf}, {r}};
   ResChebParams<R> q;
   static_cast<CParamsT<R>&>(q) = prm;
   q.g1 = -prm.g1;
-  q.Minv = LM;
+  q.inv = WM;
   q.alpha = alpha;
   q.s = s;
   q.r = r;
@@ -618,15 +750,16 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         op_C,              inv_diag,
                         mass_factor,       mass_solve,
                         cells_per_block<P>(), kNPK,
-                        mg_B_f,            mg_res<double>,
-                        mg_res<float>,     mass_solve_f,
-                        cheb<double>,      cheb<float>,
+                        mg_res<double>,    mg_res<float>,
+                        cheb<double>,
                         prolong<double>,   prolong<float>,
                         restrict_<double>, restrict_<float>,
                         inject,            rhs_adjoint1,
                         rhs_tangent1,      op_BT,
                         op_C_tangent,      op_CT,
-                        b_inv<float>,      res_cheb<float>};
+                        cob_weights<float>, cob_solve<float>,
+                        cob_cheb<float>,   b_inv<float>,
+                        res_cheb<float>};
 
 }  // namespace
 

@@ -149,8 +149,10 @@ struct Level {
   double* rho = nullptr;       // rho_for_fixed (owned on coarse levels)
   double* pf = nullptr;        // pres_fixed (owned on coarse levels)
   void* pfR = nullptr;         // pres_fixed in the level precision
-  void* LA = nullptr;          // cell inverses of A (rho-weighted vector mass)
-  void* LM = nullptr;          // cell inverses of M
+  // cell-wise inverses of A (rho-weighted vector mass) and M: packed inverse matrices on FP64
+  // levels; Gauss-point inverse weights (change of basis, no stored matrices) on FP32 levels
+  void* LA = nullptr;
+  void* LM = nullptr;
   void *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *u = nullptr, *w = nullptr;
   double lmax = 0.0;
 };
@@ -165,7 +167,6 @@ struct af_schur_solver {
   bool fp32 = false;
   bool setup_done = false, eig_done = false;
   double cB = 0, cdt = 0;       // B and C coefficients of the last setup
-  double* dtmp = nullptr;       // FP64 inverse scratch (FP32 levels)
   double* part = nullptr;       // reductions
   double* scal = nullptr;
   double* invd = nullptr;       // Jacobi: inverse diagonal of D
@@ -185,12 +186,14 @@ int alloc(af_schur_solver* s, void** p, size_t bytes) {
 
 template <class R>
 struct Prec;
-// kFused: the level's smoother runs B with the cell-wise A^{-1} in its epilogue, and the
-// residual update with the Chebyshev step in its epilogue (two launches per smoothing step
-// instead of four).  FP32 only: the FP64 kernels hold twice the inverse bytes in shared
-// memory, which halves their occupancy, and their extra FP64 epilogue work costs more than
-// the saved vector traffic (504 vs 417 us for B + A^{-1}, 704 vs 518 us for the residual and
-// Chebyshev step, 1024x256, p = 4).
+// FP32 levels (kFused): B runs with the cell-wise A^{-1} in its epilogue and the residual
+// update with the Chebyshev step in its epilogue (two launches per smoothing step instead of
+// four), and both inverses are applied by the change of basis to the Gauss points: exact for
+// M on bilinear cells, the (P+1)-point approximation of A (a preconditioner may differ from
+// the operator), with no stored matrices and no factorisation.  FP64 levels keep the exact
+// packed inverses and separate launches: a fused FP64 kernel holding the CTA's packed
+// inverses in shared memory measured slower (504 vs 417 us for B + A^{-1}, 704 vs 518 us for
+// the residual and Chebyshev step, 1024x256, p = 4).
 template <>
 struct Prec<double> {
   static constexpr bool kFused = false;
@@ -221,22 +224,18 @@ struct Prec<double> {
 template <>
 struct Prec<float> {
   static constexpr bool kFused = true;
-  static cudaError_t B(const DegreeOps* k, const MeshDev& m, const float* p, double c, float* u, int nc,
-                       cudaStream_t st) {
-    return k->mg_B_f(m, p, (float)c, u, nc, st);
-  }
   static cudaError_t res(const DegreeOps* k, const MeshDev& m, const float* w, const float* pf, const float* p,
                          double cdt, float* r, int nc, cudaStream_t st) {
     CParamsT<float> q{(float)cdt, (float)kG1, (float)kGG};
     return k->mg_res_f(m, w, pf, p, q, r, nc, st);
   }
-  static cudaError_t solve(const DegreeOps* k, const float* L, int ncomp, const float* b, double s, float* x, int nc,
+  static cudaError_t solve(const DegreeOps* k, const float* W, int ncomp, const float* b, double s, float* x, int nc,
                            cudaStream_t st) {
-    return k->mass_solve_f(L, ncomp, b, (float)s, x, nc, st);
+    return k->cob_solve_f(W, ncomp, b, (float)s, x, nc, st);
   }
-  static cudaError_t cheb(const DegreeOps* k, const float* L, const float* r, double a, double s, float* d, float* x,
+  static cudaError_t cheb(const DegreeOps* k, const float* W, const float* r, double a, double s, float* d, float* x,
                           int first, int nc, cudaStream_t st) {
-    return k->cheb_f(L, r, (float)a, (float)s, d, x, first, nc, st);
+    return k->cob_cheb_f(W, r, (float)a, (float)s, d, x, first, nc, st);
   }
   static cudaError_t b_inv(const DegreeOps* k, const MeshDev& m, const float* p, double c, const float* LA, float* w,
                            int nc, cudaStream_t st) {
@@ -380,20 +379,15 @@ int setup_levels(af_schur_solver* s, bool estimate) {
       o->launches += 2;
     }
     k_convert<double, R><<<nblocks(L.ns), kThreads, 0, o->stream>>>(L.pf, (R*)L.pfR, L.ns);
-    if (l == 0) {  // the operator's own inverse of A (built once per rho_for_fixed)
+    if (sizeof(R) == sizeof(float)) {  // Gauss-point inverse weights of A
+      MG_CU(k->cob_weights_f(L.mesh, L.rho, (float*)L.LA, L.ncell, o->stream));
+    } else if (l == 0) {  // the operator's own inverse of A (built once per rho_for_fixed)
       const double* La = nullptr;
       MG_AF(mass_inverse(o, true, &La));
       const long nf = (long)L.ncell * k->factor_len;
-      if (sizeof(R) == sizeof(double))
-        MG_CU(cudaMemcpyAsync(L.LA, La, sizeof(double) * nf, cudaMemcpyDeviceToDevice, o->stream));
-      else
-        k_convert<double, R><<<nblocks(nf), kThreads, 0, o->stream>>>(La, (R*)L.LA, nf);
-    } else if (sizeof(R) == sizeof(double)) {
-      MG_CU(k->mass_factor(L.mesh, L.rho, (double*)L.LA, L.ncell, o->stream));
+      MG_CU(cudaMemcpyAsync(L.LA, La, sizeof(double) * nf, cudaMemcpyDeviceToDevice, o->stream));
     } else {
-      const long nf = (long)L.ncell * k->factor_len;
-      MG_CU(k->mass_factor(L.mesh, L.rho, s->dtmp, L.ncell, o->stream));
-      k_convert<double, R><<<nblocks(nf), kThreads, 0, o->stream>>>(s->dtmp, (R*)L.LA, nf);
+      MG_CU(k->mass_factor(L.mesh, L.rho, (double*)L.LA, L.ncell, o->stream));
     }
     MG_CU(cudaGetLastError());
     o->launches += 3;
@@ -415,15 +409,11 @@ int build_mass_inverses(af_schur_solver* s) {
   af_operator* o = s->op;
   const DegreeOps* k = o->ops;
   for (auto& L : s->lv) {
-    if (sizeof(R) == sizeof(double)) {
+    if (sizeof(R) == sizeof(double))
       MG_CU(k->mass_factor(L.mesh, nullptr, (double*)L.LM, L.ncell, o->stream));
-    } else {
-      const long nf = (long)L.ncell * k->factor_len;
-      MG_CU(k->mass_factor(L.mesh, nullptr, s->dtmp, L.ncell, o->stream));
-      k_convert<double, R><<<nblocks(nf), kThreads, 0, o->stream>>>(s->dtmp, (R*)L.LM, nf);
-    }
-    MG_CU(cudaGetLastError());
-    o->launches += 2;
+    else
+      MG_CU(k->cob_weights_f(L.mesh, nullptr, (float*)L.LM, L.ncell, o->stream));
+    o->launches += 1;
   }
   return AF_OK;
 }
@@ -533,11 +523,10 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
     nx /= 2;
     nz /= 2;
   }
-  size_t maxf = 0;
   for (size_t l = 0; l < s->lv.size(); ++l) {
     Level& L = s->lv[l];
-    const size_t nf = (size_t)L.ncell * op->ops->factor_len;
-    maxf = std::max(maxf, nf);
+    // packed inverses (FP64) or Gauss-point weights (FP32, one value per node)
+    const size_t nf = s->fp32 ? (size_t)L.ns : (size_t)L.ncell * op->ops->factor_len;
     if (l > 0) {
       const Level& F = s->lv[l - 1];
       if ((r = alloc(s, (void**)&L.vtx, sizeof(double2) * (L.nx + 1) * (L.nz + 1))) != AF_OK) return cleanup(r);
@@ -555,7 +544,6 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
       if ((r = alloc(s, p, rs * 2 * L.ns)) != AF_OK) return cleanup(r);
   }
   s->nact = (int)s->lv.size();
-  if (s->fp32 && (r = alloc(s, (void**)&s->dtmp, sizeof(double) * maxf)) != AF_OK) return cleanup(r);
   r = s->fp32 ? build_mass_inverses<float>(s) : build_mass_inverses<double>(s);
   if (r != AF_OK) return cleanup(r);
   *out = s;

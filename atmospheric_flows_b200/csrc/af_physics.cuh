@@ -249,10 +249,11 @@ struct BPhysT {
 };
 using BPhys = BPhysT<double>;
 
-// B followed by the cell-wise A^{-1} in the kernel's epilogue: w = scale A^{-1} B p.
+// B followed by the cell-wise A^{-1} in the kernel's epilogue: w = scale A^{-1} B p, with A^{-1}
+// by the change of basis to the Gauss points (inv = 1 / (rho JxW) there; cellop epilogue 1).
 template <class R>
 struct BInvParams : BParamsT<R> {
-  const R* Minv;  // packed cell inverses of A (cell-major)
+  const R* inv;  // [cell][(P+1)^2] Gauss-point inverse weights
   R scale;
 };
 template <class R = double>
@@ -327,7 +328,7 @@ struct CPhys {
 // x += d').  Inputs as CPhys<true, +1>: d (the D term), w, p_fixed; g1 carries -1/(gamma-1).
 template <class R>
 struct ResChebParams : CParamsT<R> {
-  const R* Minv;  // packed cell inverses of M
+  const R* inv;  // [cell][(P+1)^2] Gauss-point inverse weights of M (1 / JxW)
   R alpha, s;
   R* r;
   const R* din;  // the operator's input d (own cells read again for alpha d)

@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cmath>
+#include <utility>
 #include <vector>
 
 namespace af {
@@ -43,6 +44,21 @@ struct TransT {
   R Pm[2][P + 1][P + 1];
   R E[P + 1][P + 1];
   int ch[P + 1];
+};
+
+// Change of basis between the nodal basis and the (P+1) x (P+1) Gauss points.  With
+// V[q][i] = l_i(g_q) (square and invertible), the mass matrix of a bilinear cell is exactly
+// (V x V)^T diag(JxW) (V x V) over the P+1 Gauss points -- its integrand l_i l_j det J has
+// degree <= 2P+1 per direction, which (P+1)-point Gauss integrates exactly -- so
+//   M_K^{-1} = (V x V)^{-1} diag(1 / JxW) (V x V)^{-T},
+// applied by sum factorisation with Vi = V^{-1} and no stored matrices.  A density weight
+// rho (degree P) makes the integrand degree 3P+1: the same formula with rho(g_q) JxW is then
+// the inverse of the (P+1)-point approximation of the weighted mass matrix.
+template <int P, class R = double>
+struct CobT {
+  R Vi[P + 1][P + 1];  // Vi[i][q] = (V^{-1})[i][q]
+  R V[P + 1][P + 1];   // V[q][i] = l_i(g_q)
+  R g[P + 1], w[P + 1];  // Gauss points and weights on [0, 1]
 };
 
 namespace host {
@@ -148,6 +164,43 @@ inline TabT<P, R> make_tab() {
   for (int q = 0; q < T::NQ; ++q) {
     t.w[q] = (R)w[q];
     t.x[q] = (R)x[q];
+  }
+  return t;
+}
+
+template <int P, class R = double>
+inline CobT<P, R> make_cob() {
+  constexpr int P1 = P + 1;
+  CobT<P, R> t{};
+  std::vector<LD> nd = gll(P), x, w;
+  gauss(P1, x, w);
+  LD V[P1][P1], Vi[P1][2 * P1];
+  for (int q = 0; q < P1; ++q)
+    for (int i = 0; i < P1; ++i) V[q][i] = lag(nd, i, x[q]);
+  // Gauss-Jordan with partial pivoting on [V | I]
+  for (int r = 0; r < P1; ++r)
+    for (int c = 0; c < 2 * P1; ++c) Vi[r][c] = c < P1 ? V[r][c] : (c - P1 == r ? 1 : 0);
+  for (int c = 0; c < P1; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < P1; ++r)
+      if (fabsl(Vi[r][c]) > fabsl(Vi[piv][c])) piv = r;
+    for (int k = 0; k < 2 * P1; ++k) std::swap(Vi[c][k], Vi[piv][k]);
+    const LD d = Vi[c][c];
+    for (int k = 0; k < 2 * P1; ++k) Vi[c][k] /= d;
+    for (int r = 0; r < P1; ++r)
+      if (r != c) {
+        const LD f = Vi[r][c];
+        for (int k = 0; k < 2 * P1; ++k) Vi[r][k] -= f * Vi[c][k];
+      }
+  }
+  for (int i = 0; i < P1; ++i)
+    for (int q = 0; q < P1; ++q) {
+      t.Vi[i][q] = (R)Vi[i][P1 + q];
+      t.V[q][i] = (R)V[q][i];
+    }
+  for (int q = 0; q < P1; ++q) {
+    t.g[q] = (R)x[q];
+    t.w[q] = (R)w[q];
   }
   return t;
 }
