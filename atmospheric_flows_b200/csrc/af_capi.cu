@@ -164,7 +164,7 @@ int af_destroy(af_operator* o) {
   cudaFree(o->d_part);
   cudaFree(o->d_kst);
   cudaFree(o->d_stage);
-  cudaFree(o->d_Lm);
+  cudaFree(o->d_Wm);
   cudaFree(o->d_La);
   if (o->own_stream) cudaStreamDestroy(o->own_stream);
   delete o;
@@ -437,29 +437,42 @@ static int solve_A(af_operator* o, double* x, const double* b) {
 }
 
 // Packed inverses of the cell mass matrices (built on first use)
-static int ensure_factor(af_operator* o, bool weighted) {
-  double** L = weighted ? &o->d_La : &o->d_Lm;
-  bool* valid = weighted ? &o->La_valid : &o->Lm_valid;
-  if (*valid) return AF_OK;
-  if (weighted && !o->rho_fixed_set) return fail(AF_BAD_ARG, "set_rho_for_fixed first");
-  if (!*L) AF_CU(cudaMalloc(L, sizeof(double) * (size_t)o->ncell * o->ops->factor_len));
-  AF_CU(o->ops->mass_factor(o->mesh, weighted ? o->d_rho_fixed : nullptr, *L, o->ncell, o->stream));
+// packed exact inverses of A (rho_for_fixed); M uses the change of basis instead
+static int ensure_factor(af_operator* o) {
+  if (o->La_valid) return AF_OK;
+  if (!o->rho_fixed_set) return fail(AF_BAD_ARG, "set_rho_for_fixed first");
+  if (!o->d_La) AF_CU(cudaMalloc(&o->d_La, sizeof(double) * (size_t)o->ncell * o->ops->factor_len));
+  AF_CU(o->ops->mass_factor(o->mesh, o->d_rho_fixed, o->d_La, o->ncell, o->stream));
   o->launches += 1;
-  *valid = true;
+  o->La_valid = true;
   return AF_OK;
 }
 
+// Gauss-point weights of M for its inverse by the change of basis (exact on bilinear cells:
+// M_K = (V x V)^T diag(JxW) (V x V) with V the nodal basis at the P+1 Gauss points)
+static int ensure_mass_weights(af_operator* o) {
+  if (o->Wm_valid) return AF_OK;
+  if (!o->d_Wm) AF_CU(cudaMalloc(&o->d_Wm, sizeof(double) * (size_t)o->n_scalar()));
+  AF_CU(o->ops->cob_weights_d(o->mesh, nullptr, o->d_Wm, o->ncell, o->stream));
+  o->launches += 1;
+  o->Wm_valid = true;
+  return AF_OK;
+}
 
 int af_vmult_inverse(af_operator* o, double* dst, const double* src) {
   if (!o || !dst || !src) return fail(AF_BAD_ARG, "null argument");
   const int ns = o->ns;
   if (ns == 2) return fail(AF_BAD_ARG, "af_vmult_inverse: NS_stage 2 (Schur complement) has no cell-wise inverse");
   AF_CU(cudaSetDevice(o->device));
-  const bool weighted = (ns == 3 || ns == 5);
-  int r = ensure_factor(o, weighted);
-  if (r != AF_OK) return r;
-  const double scale = ns == 6 ? (1.4 - 1.0) : 1.0;  // D = M/(gamma-1)
-  AF_CU(o->ops->mass_solve(weighted ? o->d_La : o->d_Lm, weighted ? 2 : 1, src, scale, dst, o->ncell, o->stream));
+  if (ns == 3 || ns == 5) {  // A: packed exact inverses (rho-weighted, rebuilt per rho_for_fixed)
+    const int r = ensure_factor(o);
+    if (r != AF_OK) return r;
+    AF_CU(o->ops->mass_solve(o->d_La, 2, src, 1.0, dst, o->ncell, o->stream));
+  } else {  // M (NS 1/4) and D = M/(gamma-1) (NS 6): change of basis, no stored matrices
+    const int r = ensure_mass_weights(o);
+    if (r != AF_OK) return r;
+    AF_CU(o->ops->cob_solve_d(o->d_Wm, 1, src, ns == 6 ? (1.4 - 1.0) : 1.0, dst, o->ncell, o->stream));
+  }
   o->launches += 1;
   return AF_OK;
 }
@@ -496,7 +509,7 @@ int af_vmult(af_operator* o, double* dst, const double* src) {
   o->launches += 1;
   int r;
   if (o->schur_mode == 1) {  // exact cell-wise A^{-1}
-    r = ensure_factor(o, true);
+    r = ensure_factor(o);
     if (r != AF_OK) return r;
     AF_CU(o->ops->mass_solve(o->d_La, 2, t1, 1.0, t2, o->ncell, o->stream));
     o->launches += 1;
@@ -588,7 +601,7 @@ int af_vmult_enthalpy_transpose(af_operator* o, double* wbar, const double* w, c
 // w = A^{-1} B p into the workspace (2 ns), exact inverse
 static int schur_w(af_operator* o, const double* p, double* w, double* t) {
   AF_CU(o->ops->op_B(o->mesh, p, coeff_BC(o) * o->dt / (o->Ma * o->Ma), t, o->ncell, o->stream));
-  int r = ensure_factor(o, true);
+  int r = ensure_factor(o);
   if (r != AF_OK) return r;
   AF_CU(o->ops->mass_solve(o->d_La, 2, t, 1.0, w, o->ncell, o->stream));
   o->launches += 2;
@@ -638,12 +651,12 @@ void set_last_error(const char* msg) { g_last_error = msg; }
 }  // namespace af
 
 namespace af {
-// The operator's packed cell inverses of A (rho_for_fixed) or M, built if needed; used by the
+// The operator's packed cell inverses of A (rho_for_fixed), built if needed; used by the FP64
 // pressure solver's finest level instead of factorising the same matrices again.
-int mass_inverse(af_operator* o, bool weighted, const double** out) {
-  const int r = ensure_factor(o, weighted);
+int mass_inverse_A(af_operator* o, const double** out) {
+  const int r = ensure_factor(o);
   if (r != AF_OK) return r;
-  *out = weighted ? o->d_La : o->d_Lm;
+  *out = o->d_La;
   return AF_OK;
 }
 }  // namespace af

@@ -37,10 +37,11 @@ struct af_operator {
   int last_inner_its = 0;
   long long launches = 0;
   const DegreeOps* ops = nullptr;
-  // exact cell-wise inverses: packed Cholesky factors of M (fixed) and of A (rho_for_fixed)
-  double* d_Lm = nullptr;
+  // exact cell-wise inverses: Gauss-point weights of M (fixed mesh; change of basis) and the
+  // packed inverses of A (rho_for_fixed)
+  double* d_Wm = nullptr;
   double* d_La = nullptr;
-  bool Lm_valid = false, La_valid = false;
+  bool Wm_valid = false, La_valid = false;
   // host-buffer entry points: device staging
   double* d_stage = nullptr;
   size_t stage_len = 0;
@@ -49,5 +50,5 @@ struct af_operator {
 };
 
 namespace af {
-int mass_inverse(af_operator* o, bool weighted, const double** out);
+int mass_inverse_A(af_operator* o, const double** out);
 }

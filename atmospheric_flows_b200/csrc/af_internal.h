@@ -79,11 +79,16 @@ struct DegreeOps {
   cudaError_t (*op_CT)(const MeshDev&, const double* w, const double* pf, const double* pbar, const CParams&,
                        double* wbar, int ncell, cudaStream_t);
 
-  // ---- FP32 level kernels with cell-wise inverses by the change of basis to the Gauss points
-  // (no stored matrices): W = 1 / (rho JxW) at the (P+1)^2 Gauss points, rho = 1 when null
+  // ---- cell-wise inverses by the change of basis to the Gauss points (no stored matrices):
+  // W = 1 / (rho JxW) at the (P+1)^2 Gauss points, rho = 1 when null.  Exact for the plain
+  // mass matrix on bilinear cells (FP64: the operator's M and D inverses); the FP32 levels
+  // of the pressure preconditioner also use it for A
   cudaError_t (*cob_weights_f)(const MeshDev&, const double* rho, float* W, int ncell, cudaStream_t);
+  cudaError_t (*cob_weights_d)(const MeshDev&, const double* rho, double* W, int ncell, cudaStream_t);
   // x = scale M_W^{-1} b (ncomp 1 or 2)
   cudaError_t (*cob_solve_f)(const float* W, int ncomp, const float* b, float scale, float* x, int ncell,
+                             cudaStream_t);
+  cudaError_t (*cob_solve_d)(const double* W, int ncomp, const double* b, double scale, double* x, int ncell,
                              cudaStream_t);
   // d = alpha d + s M_W^{-1} r;  x = d (first) or x += d
   cudaError_t (*cob_cheb_f)(const float* W, const float* r, float alpha, float s, float* d, float* x, int first,

@@ -757,7 +757,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         inject,            rhs_adjoint1,
                         rhs_tangent1,      op_BT,
                         op_C_tangent,      op_CT,
-                        cob_weights<float>, cob_solve<float>,
+                        cob_weights<float>, cob_weights<double>,
+                        cob_solve<float>,  cob_solve<double>,
                         cob_cheb<float>,   b_inv<float>,
                         res_cheb<float>};
 

@@ -383,7 +383,7 @@ int setup_levels(af_schur_solver* s, bool estimate) {
       MG_CU(k->cob_weights_f(L.mesh, L.rho, (float*)L.LA, L.ncell, o->stream));
     } else if (l == 0) {  // the operator's own inverse of A (built once per rho_for_fixed)
       const double* La = nullptr;
-      MG_AF(mass_inverse(o, true, &La));
+      MG_AF(mass_inverse_A(o, &La));
       const long nf = (long)L.ncell * k->factor_len;
       MG_CU(cudaMemcpyAsync(L.LA, La, sizeof(double) * nf, cudaMemcpyDeviceToDevice, o->stream));
     } else {
