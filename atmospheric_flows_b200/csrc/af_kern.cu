@@ -423,8 +423,114 @@ cudaError_t launch_mass_solve(const R* L, int ncomp, const R* b, R scale, R* x, 
   return cudaGetLastError();
 }
 
+// Degrees <= 4 ((P+1)^2 <= 32 rows): the same cell matrix and its inverse with lane i owning
+// row i in registers, which removes the shared-memory traffic and index decoding of the
+// kernel above (instruction-bound: about 11.5 k warp instructions per cell at p = 4):
+//   rows: M[i][j] = sum_qz S[qz][iz] S[qz][jz] T(qz)[ix][jx], T as above (full, not packed);
+//   in-place Gauss-Jordan without pivoting (M is symmetric positive definite): for each
+//   pivot k, row k is scaled by 1/M_kk and broadcast by warp shuffles, every other row r
+//   takes a_rj -= a_rk a_kj and a_rk = -a_rk / M_kk, leaving M^{-1} in the rows;
+//   the lower triangle is staged in shared memory and stored coalesced.
+constexpr int kGJWarps = 4;
+template <int ND_ = kND>
+__global__ void __launch_bounds__(32 * kGJWarps)
+    k_mass_inverse_rows(const MeshDev mesh, const double* __restrict__ weight, double* __restrict__ Lg,
+                        const int ncell) {
+  static_assert(ND_ <= 32, "one row per lane");
+  using T = Tab<P>;
+  constexpr int P1 = T::P1, NQ = T::NQ, ND = ND_, NPK = ND * (ND + 1) / 2;
+  __shared__ double sS[NQ * P1];
+  __shared__ double sF[kGJWarps][NQ * NQ];
+  __shared__ double sT[kGJWarps][NQ * P1 * P1];
+  __shared__ double sO[kGJWarps][NPK];
+  const Tab<P>& tb = c_tab;
+  for (int k = threadIdx.x; k < NQ * P1; k += blockDim.x) sS[k] = tb.S[k / P1][k % P1];
+  __syncthreads();  // the only block-wide barrier; warps past the last cell leave after it
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kGJWarps + warp;
+  if (c >= ncell) return;
+  double* F = sF[warp];
+  double* Tm = sT[warp];
+  double* O = sO[warp];
+  const int i = c % mesh.nx, j = c / mesh.nx, W = mesh.nx + 1;
+  const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
+  const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
+  const double Ax = v1.x - v0.x, Az = v1.y - v0.y, Cx = v2.x - v0.x, Cz = v2.y - v0.y;
+  const double Bx = v3.x - v2.x - v1.x + v0.x, Bz = v3.y - v2.y - v1.y + v0.y;
+  // F(q) = w(q) JxW(q)
+  for (int q = lane; q < NQ * NQ; q += 32) {
+    const int qx = q % NQ, qz = q / NQ;
+    const double xi = tb.x[qx], eta = tb.x[qz];
+    const double J00 = fma(Bx, eta, Ax), J10 = fma(Bz, eta, Az), J01 = fma(Bx, xi, Cx), J11 = fma(Bz, xi, Cz);
+    double f = (J00 * J11 - J01 * J10) * tb.w[qx] * tb.w[qz];
+    if (weight) {
+      const double* wc = weight + (size_t)c * ND;
+      double wv = 0.0;
+#pragma unroll
+      for (int iz = 0; iz < P1; ++iz) {
+        double t = 0.0;
+#pragma unroll
+        for (int ix = 0; ix < P1; ++ix) t = fma(sS[qx * P1 + ix], wc[iz * P1 + ix], t);
+        wv = fma(sS[qz * P1 + iz], t, wv);
+      }
+      f *= wv;
+    }
+    F[q] = f;
+  }
+  __syncwarp();
+  // T(qz)[ix][jx]
+  for (int e = lane; e < NQ * P1 * P1; e += 32) {
+    const int qz = e / (P1 * P1), ix = (e / P1) % P1, jx = e % P1;
+    double s = 0.0;
+#pragma unroll
+    for (int qx = 0; qx < NQ; ++qx) s = fma(sS[qx * P1 + ix] * sS[qx * P1 + jx], F[qz * NQ + qx], s);
+    Tm[e] = s;
+  }
+  __syncwarp();
+  // row r = lane of the cell matrix (lanes >= ND duplicate the last row and store nothing)
+  const int r = lane < ND ? lane : ND - 1, rz = r / P1, rx = r % P1;
+  double siz[NQ];
+#pragma unroll
+  for (int qz = 0; qz < NQ; ++qz) siz[qz] = sS[qz * P1 + rz];
+  double a[ND];
+#pragma unroll
+  for (int jj = 0; jj < ND; ++jj) {
+    const int jz = jj / P1, jx = jj % P1;
+    double s = 0.0;
+#pragma unroll
+    for (int qz = 0; qz < NQ; ++qz) s = fma(siz[qz] * tb.S[qz][jz], Tm[qz * P1 * P1 + rx * P1 + jx], s);
+    a[jj] = s;
+  }
+  // Gauss-Jordan in place
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    const double piv = 1.0 / __shfl_sync(0xffffffffu, a[k], k);
+    if (lane == k) {
+#pragma unroll
+      for (int jj = 0; jj < ND; ++jj) a[jj] = jj == k ? piv : a[jj] * piv;
+    }
+    const double f = a[k];
+#pragma unroll
+    for (int jj = 0; jj < ND; ++jj) {
+      const double rkj = __shfl_sync(0xffffffffu, a[jj], k);
+      if (lane != k) a[jj] = jj == k ? -f * rkj : fma(-f, rkj, a[jj]);
+    }
+  }
+  // lower triangle of row r, packed row-major, then coalesced
+#pragma unroll
+  for (int jj = 0; jj < ND; ++jj)
+    if (lane < ND && jj <= lane) O[lane * (lane + 1) / 2 + jj] = a[jj];
+  __syncwarp();
+  double* out = Lg + (size_t)c * NPK;
+  for (int e = lane; e < NPK; e += 32) out[e] = O[e];
+}
+
 cudaError_t mass_factor(const MeshDev& mesh, const double* weight, double* L, int ncell, cudaStream_t st) {
-  k_mass_factor<<<(ncell + kFactorWarps - 1) / kFactorWarps, 32 * kFactorWarps, 0, st>>>(mesh, weight, L, ncell);
+  if constexpr (kND <= 32) {
+    k_mass_inverse_rows<<<(ncell + kGJWarps - 1) / kGJWarps, 32 * kGJWarps, 0, st>>>(mesh, weight, L, ncell);
+  } else {
+    k_mass_factor<<<(ncell + kFactorWarps - 1) / kFactorWarps, 32 * kFactorWarps, 0, st>>>(mesh, weight, L, ncell);
+  }
   return cudaGetLastError();
 }
 
