@@ -802,6 +802,12 @@ cudaError_t cob_cheb(const R* W, const R* r, R alpha, R s, R* d, R* x, int first
 }
 
 // ------------------------------------------------------------------ fused epilogues
+// Launch shapes of the two FP32 smoother kernels at p = 4 (1024x256, us per launch):
+// cells per CTA / CTAs per SM  16/2: B+A^-1 190.6, residual+Chebyshev 258.2;  32/2: 176.4,
+// 237.7;  32/3: 172.5, 240.5;  8/8: 215.1, 314.7;  64/1: 209.1, 372.2.
+constexpr int kFusedCB = P == 4 ? 32 : cells_per_block<P>();
+constexpr int kBInvMinB = P == 4 ? 3 : min_blocks_per_sm<P>();
+constexpr int kResChebMinB = min_blocks_per_sm<P>();
 template <class R>
 cudaError_t b_inv(const MeshDev& mesh, const R* p, R c, const R* WA, R scale, R* w, int ncell, cudaStream_t st) {
   ArgPtrs<1, 1, R> a{{p}, {w}};
@@ -809,7 +815,7 @@ cudaError_t b_inv(const MeshDev& mesh, const R* p, R c, const R* WA, R scale, R*
   q.c = c;
   q.inv = WA;
   q.scale = scale;
-  return launch_cellop<P, BInvPhys<R>>(mesh, a, q, ncell, st);
+  return launch_cellop<P, BInvPhys<R>, kFusedCB, kBInvMinB>(mesh, a, q, ncell, st);
 }
 
 template <class R>
@@ -828,7 +834,7 @@ cudaError_t res_cheb(const MeshDev& mesh, const R* w, const R* pf, const R* din,
   q.dout = dout;
   q.x = x;
   q.first = first;
-  return launch_cellop<P, ResChebPhys<R>>(mesh, a, q, ncell, st);
+  return launch_cellop<P, ResChebPhys<R>, kFusedCB, kResChebMinB>(mesh, a, q, ncell, st);
 }
 
 constexpr int kTransferThreads = 256;
