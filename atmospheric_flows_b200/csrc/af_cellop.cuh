@@ -83,8 +83,8 @@ __device__ __forceinline__ void sfor(F&& f) {
 
 // 1D tables of degree P in precision R; each kernel translation unit defines the
 // specialisations it uses (constant memory is per module).
-template <int P, class R>
-__device__ __forceinline__ const TabT<P, R>& tabr();
+template <int P, class R, int NQ = 2 * P + 1>
+__device__ __forceinline__ const TabT<P, R, NQ>& tabr();
 template <int P>
 __device__ __forceinline__ const Tab<P>& tab() {
   return tabr<P, double>();
@@ -225,10 +225,21 @@ struct PhysInfo {
   }
 };
 
+// Gauss points per direction of a policy: the operator's 2P+1, or P+1 for a policy that
+// declares REDUCED_Q (preconditioner operators; exact for B, M and D on bilinear cells).
+template <int P, class Phys, class = void>
+struct NQOf {
+  static constexpr int value = 2 * P + 1;
+};
+template <int P, class Phys>
+struct NQOf<P, Phys, std::void_t<decltype(Phys::REDUCED_Q)>> {
+  static constexpr int value = Phys::REDUCED_Q ? P + 1 : 2 * P + 1;
+};
+
 template <int P, class Phys, int CB_ = cells_per_block<P>()>
 struct Layout {
   using R = RealOf<Phys>;
-  using T = TabT<P, R>;
+  using T = TabT<P, R, NQOf<P, Phys>::value>;
   static constexpr int P1 = T::P1, NQ = T::NQ, ND = P1 * P1;
   static constexpr int CB = CB_;
   static constexpr int NT = CB * NQ;
@@ -265,10 +276,10 @@ struct Layout {
 };
 
 // even/odd contraction of a P1-vector r along one direction to NQ values
-template <int P, class R>
+template <int P, class R, int NQ>
 __device__ __forceinline__ void contract_eo(const R* r, R* y) {
-  using T = TabT<P, R>;
-  const T& t = tabr<P, R>();
+  using T = TabT<P, R, NQ>;
+  const T& t = tabr<P, R, NQ>();
   R re[T::H > 0 ? T::H : 1], ro[T::H > 0 ? T::H : 1];
 #pragma unroll
   for (int i = 0; i < T::H; ++i) {
@@ -277,7 +288,7 @@ __device__ __forceinline__ void contract_eo(const R* r, R* y) {
   }
   const R rm = T::MIDN ? r[P / 2] : 0.0;
 #pragma unroll
-  for (int k = 0; k < P; ++k) {
+  for (int k = 0; k < T::QH; ++k) {
     R e = 0.0, o = 0.0;
 #pragma unroll
     for (int i = 0; i < T::H; ++i) {
@@ -288,18 +299,20 @@ __device__ __forceinline__ void contract_eo(const R* r, R* y) {
     y[k] = e + o;
     y[T::NQ - 1 - k] = e - o;
   }
-  R e = 0.0;
+  if constexpr (T::QMID) {  // the middle point sees the even part only
+    R e = 0.0;
 #pragma unroll
-  for (int i = 0; i < T::H; ++i) e = fmaR(t.Se[P][i], re[i], e);
-  if (T::MIDN) e = fmaR(t.Sm[P], rm, e);
-  y[P] = e;
+    for (int i = 0; i < T::H; ++i) e = fmaR(t.Se[T::QH][i], re[i], e);
+    if (T::MIDN) e = fmaR(t.Sm[T::QH], rm, e);
+    y[T::QH] = e;
+  }
 }
 
 // derivative counterpart: y[q] = sum_i D[q][i] r[i] with D[NQ-1-q][i] = -D[q][P-i]
-template <int P, class R>
+template <int P, class R, int NQ>
 __device__ __forceinline__ void contract_eo_D(const R* r, R* y) {
-  using T = TabT<P, R>;
-  const T& t = tabr<P, R>();
+  using T = TabT<P, R, NQ>;
+  const T& t = tabr<P, R, NQ>();
   R re[T::H > 0 ? T::H : 1], ro[T::H > 0 ? T::H : 1];
 #pragma unroll
   for (int i = 0; i < T::H; ++i) {
@@ -308,7 +321,7 @@ __device__ __forceinline__ void contract_eo_D(const R* r, R* y) {
   }
   const R rm = T::MIDN ? r[P / 2] : R(0);
 #pragma unroll
-  for (int k = 0; k <= P; ++k) {
+  for (int k = 0; k < T::QE; ++k) {
     R e = 0.0, o = 0.0;
 #pragma unroll
     for (int i = 0; i < T::H; ++i) {
@@ -317,7 +330,7 @@ __device__ __forceinline__ void contract_eo_D(const R* r, R* y) {
     }
     if (T::MIDN) e = fmaR(t.Dm[k], rm, e);
     y[k] = e + o;
-    if (k < P) y[T::NQ - 1 - k] = o - e;
+    if (k < T::QH) y[T::NQ - 1 - k] = o - e;
   }
 }
 
@@ -330,13 +343,14 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
              const typename Phys::Params prm, const int ncell) {
   using L = Layout<P, Phys, CB_>;
   using R = RealOf<Phys>;
-  using T = TabT<P, R>;
+  using T = typename L::T;
   constexpr int P1 = L::P1, NQ = L::NQ, ND = L::ND, CB = L::CB, NT = L::NT;
   constexpr int H = T::H;
   constexpr bool MIDN = T::MIDN;
+  constexpr int QH = T::QH;  // quadrature point pairs (q, NQ-1-q); middle point QH if T::QMID
   constexpr int NOUT = Phys::NOUT;
   constexpr int NFC_ALL = L::NFC;
-  const T& tb = tabr<P, R>();
+  const T& tb = tabr<P, R, NQ>();
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* smem = reinterpret_cast<R*>(smem_raw);
@@ -544,8 +558,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         R* eo = s_eo + ((EOFF + fi) * CB + cl) * L::EOS;
         R r[P1], y[NQ];
         auto contract = [&]() {
-          if (NFG > 0 && dxi) contract_eo_D<P>(r, y);
-          else contract_eo<P>(r, y);
+          if (NFG > 0 && dxi) contract_eo_D<P, R, NQ>(r, y);
+          else contract_eo<P, R, NQ>(r, y);
         };
         if (k < H) {
 #pragma unroll
@@ -673,8 +687,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     };
 #pragma unroll kZUnroll
-    for (int k = 0; k <= P; ++k) {
-      const bool pair = k < P;
+    for (int k = 0; k < T::QE; ++k) {
+      const bool pair = k < QH;
       R v1[NFC_ALL], v2[NFC_ALL];
 #pragma unroll
       for (int fi = 0; fi < NFC_ALL; ++fi) {
@@ -740,7 +754,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
 #pragma unroll
     for (int i = 0; i < H; ++i) oE[i] = oO[i] = 0.0;
 #pragma unroll
-    for (int k = 0; k < P; ++k) {
+    for (int k = 0; k < QH; ++k) {
       const R a1 = A[k], a2 = A[NQ - 1 - k], b1 = B[k], b2 = B[NQ - 1 - k];
       const R As = a1 + a2, Ad = a1 - a2, Bs = b1 + b2, Bd = b1 - b2;
 #pragma unroll
@@ -752,14 +766,14 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
       if (MIDN) { oM = fmaR(tb.Sm[k], As, oM); oM = fmaR(tb.Dm[k], Bd, oM); }
     }
-    {
-      const R am = A[P], bm = B[P];
+    if constexpr (T::QMID) {  // the middle point: even part of S, odd part of D
+      const R am = A[QH], bm = B[QH];
 #pragma unroll
       for (int i = 0; i < H; ++i) {
-        oE[i] = fmaR(tb.Se[P][i], am, oE[i]);
-        oO[i] = fmaR(tb.Do[P][i], bm, oO[i]);
+        oE[i] = fmaR(tb.Se[QH][i], am, oE[i]);
+        oO[i] = fmaR(tb.Do[QH][i], bm, oO[i]);
       }
-      if (MIDN) oM = fmaR(tb.Sm[P], am, oM);
+      if (MIDN) oM = fmaR(tb.Sm[QH], am, oM);
     }
     R out[P1];
 #pragma unroll

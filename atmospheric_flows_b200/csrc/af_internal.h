@@ -101,6 +101,15 @@ struct DegreeOps {
   cudaError_t (*res_cheb_f)(const MeshDev&, const float* w, const float* pf, const float* din,
                             const CParamsT<float>&, const float* WM, float alpha, float s, float* r, float* dout,
                             float* x, int first, int ncell, cudaStream_t);
+  // the same three FP32 level operators with P+1 Gauss points per direction (exact for B and
+  // D on bilinear cells, approximate for C0 and A): the reduced-quadrature preconditioner
+  cudaError_t (*mg_res_fr)(const MeshDev&, const float* w, const float* pf, const float* p,
+                           const CParamsT<float>&, float* r, int ncell, cudaStream_t);
+  cudaError_t (*b_inv_fr)(const MeshDev&, const float* p, float c, const float* WA, float scale, float* w,
+                          int ncell, cudaStream_t);
+  cudaError_t (*res_cheb_fr)(const MeshDev&, const float* w, const float* pf, const float* din,
+                             const CParamsT<float>&, const float* WM, float alpha, float s, float* r, float* dout,
+                             float* x, int first, int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

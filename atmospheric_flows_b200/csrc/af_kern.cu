@@ -15,6 +15,7 @@ namespace af {
 
 static __constant__ Tab<AF_P> c_tab;
 static __constant__ TabT<AF_P, float> c_tabf;
+static __constant__ TabT<AF_P, float, AF_P + 1> c_tabfr;  // reduced quadrature (preconditioner)
 static __constant__ TransT<AF_P, double> c_tr;
 static __constant__ TransT<AF_P, float> c_trf;
 static __constant__ CobT<AF_P, double> c_cob;
@@ -27,6 +28,10 @@ __device__ __forceinline__ const Tab<AF_P>& tabr<AF_P, double>() {
 template <>
 __device__ __forceinline__ const TabT<AF_P, float>& tabr<AF_P, float>() {
   return c_tabf;
+}
+template <>
+__device__ __forceinline__ const TabT<AF_P, float, AF_P + 1>& tabr<AF_P, float, AF_P + 1>() {
+  return c_tabfr;
 }
 template <>
 __device__ __forceinline__ const CobT<AF_P, double>& cobr<AF_P, double>() {
@@ -44,6 +49,7 @@ constexpr int P = AF_P;
 cudaError_t upload_tables() {
   static const Tab<P> t = host::make_tab<P>();
   static const TabT<P, float> tf = host::make_tab<P, float>();
+  static const TabT<P, float, P + 1> tfr = host::make_tab<P, float, P + 1>();
   static const TransT<P, double> tr = host::make_trans<P, double>();
   static const TransT<P, float> trf = host::make_trans<P, float>();
   static const CobT<P, double> cob = host::make_cob<P, double>();
@@ -52,6 +58,7 @@ cudaError_t upload_tables() {
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cob, &cob, sizeof(cob));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cobf, &cobf, sizeof(cobf));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tabf, &tf, sizeof(tf));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tabfr, &tfr, sizeof(tfr));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tr, &tr, sizeof(tr));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_trf, &trf, sizeof(trf));
   return e;
@@ -837,6 +844,42 @@ cudaError_t res_cheb(const MeshDev& mesh, const R* w, const R* pf, const R* din,
   return launch_cellop<P, ResChebPhys<R>, kFusedCB, kResChebMinB>(mesh, a, q, ncell, st);
 }
 
+// reduced-quadrature (P+1 Gauss points) counterparts of mg_res, b_inv and res_cheb in FP32
+cudaError_t mg_res_fr(const MeshDev& mesh, const float* w, const float* pf, const float* p, const CParamsT<float>& prm,
+                      float* r, int ncell, cudaStream_t st) {
+  ArgPtrs<3, 1, float> a{{p, w, pf}, {r}};
+  CParamsT<float> q = prm;
+  q.g1 = -prm.g1;
+  return launch_cellop<P, CResRPhys<float>, kFusedCB, kResChebMinB>(mesh, a, q, ncell, st);
+}
+cudaError_t b_inv_fr(const MeshDev& mesh, const float* p, float c, const float* WA, float scale, float* w, int ncell,
+                     cudaStream_t st) {
+  ArgPtrs<1, 1, float> a{{p}, {w}};
+  BInvParams<float> q;
+  q.c = c;
+  q.inv = WA;
+  q.scale = scale;
+  return launch_cellop<P, BInvRPhys<float>, kFusedCB, kBInvMinB>(mesh, a, q, ncell, st);
+}
+cudaError_t res_cheb_fr(const MeshDev& mesh, const float* w, const float* pf, const float* din,
+                        const CParamsT<float>& prm, const float* WM, float alpha, float s, float* r, float* dout,
+                        float* x, int first, int ncell, cudaStream_t st) {
+  if (din == dout) return cudaErrorInvalidValue;
+  ArgPtrs<3, 1, float> a{{din, w, pf}, {r}};
+  ResChebParams<float> q;
+  static_cast<CParamsT<float>&>(q) = prm;
+  q.g1 = -prm.g1;
+  q.inv = WM;
+  q.alpha = alpha;
+  q.s = s;
+  q.r = r;
+  q.din = din;
+  q.dout = dout;
+  q.x = x;
+  q.first = first;
+  return launch_cellop<P, ResChebRPhys<float>, kFusedCB, kResChebMinB>(mesh, a, q, ncell, st);
+}
+
 constexpr int kTransferThreads = 256;
 
 template <class R>
@@ -872,7 +915,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         cob_weights<float>, cob_weights<double>,
                         cob_solve<float>,  cob_solve<double>,
                         cob_cheb<float>,   b_inv<float>,
-                        res_cheb<float>};
+                        res_cheb<float>,   mg_res_fr,
+                        b_inv_fr,          res_cheb_fr};
 
 }  // namespace
 

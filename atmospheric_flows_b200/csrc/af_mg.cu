@@ -165,6 +165,7 @@ struct af_schur_solver {
   std::vector<Level> lv;
   int nact = 0;                 // levels in use (the coarsest has lmax <= coarse_lmax)
   bool fp32 = false;
+  bool rq = false;              // FP32 levels with the reduced quadrature (P+1 Gauss points)
   bool setup_done = false, eig_done = false;
   double cB = 0, cdt = 0;       // B and C coefficients of the last setup
   double* part = nullptr;       // reductions
@@ -202,7 +203,7 @@ struct Prec<double> {
     return k->op_B(m, p, c, u, nc, st);
   }
   static cudaError_t res(const DegreeOps* k, const MeshDev& m, const double* w, const double* pf, const double* p,
-                         double cdt, double* r, int nc, cudaStream_t st) {
+                         double cdt, double* r, int nc, cudaStream_t st, bool /*rq: FP32 levels only*/) {
     CParams q{cdt, kG1, kGG};
     return k->mg_res_d(m, w, pf, p, q, r, nc, st);
   }
@@ -225,9 +226,9 @@ template <>
 struct Prec<float> {
   static constexpr bool kFused = true;
   static cudaError_t res(const DegreeOps* k, const MeshDev& m, const float* w, const float* pf, const float* p,
-                         double cdt, float* r, int nc, cudaStream_t st) {
+                         double cdt, float* r, int nc, cudaStream_t st, bool rq) {
     CParamsT<float> q{(float)cdt, (float)kG1, (float)kGG};
-    return k->mg_res_f(m, w, pf, p, q, r, nc, st);
+    return rq ? k->mg_res_fr(m, w, pf, p, q, r, nc, st) : k->mg_res_f(m, w, pf, p, q, r, nc, st);
   }
   static cudaError_t solve(const DegreeOps* k, const float* W, int ncomp, const float* b, double s, float* x, int nc,
                            cudaStream_t st) {
@@ -238,14 +239,14 @@ struct Prec<float> {
     return k->cob_cheb_f(W, r, (float)a, (float)s, d, x, first, nc, st);
   }
   static cudaError_t b_inv(const DegreeOps* k, const MeshDev& m, const float* p, double c, const float* LA, float* w,
-                           int nc, cudaStream_t st) {
-    return k->b_inv_f(m, p, (float)c, LA, 1.0f, w, nc, st);
+                           int nc, cudaStream_t st, bool rq) {
+    return (rq ? k->b_inv_fr : k->b_inv_f)(m, p, (float)c, LA, 1.0f, w, nc, st);
   }
   static cudaError_t res_cheb(const DegreeOps* k, const MeshDev& m, const float* w, const float* pf, const float* din,
                               double cdt, const float* LM, double a, double s, float* r, float* dout, float* x, int nc,
-                              cudaStream_t st) {
+                              cudaStream_t st, bool rq) {
     CParamsT<float> q{(float)cdt, (float)kG1, (float)kGG};
-    return k->res_cheb_f(m, w, pf, din, q, LM, (float)a, (float)s, r, dout, x, 0, nc, st);
+    return (rq ? k->res_cheb_fr : k->res_cheb_f)(m, w, pf, din, q, LM, (float)a, (float)s, r, dout, x, 0, nc, st);
   }
   static cudaError_t prolong(const DegreeOps* k, const float* xc, float* xf, int nxc, int nzc, cudaStream_t st) {
     return k->prolong_f(xc, xf, nxc, nzc, st);
@@ -261,14 +262,14 @@ int residual_update(af_schur_solver* s, Level& L, const R* v, R* r) {
   af_operator* o = s->op;
   const DegreeOps* k = o->ops;
   if constexpr (Prec<R>::kFused) {  // w = A^{-1} B v in one launch
-    MG_CU(Prec<R>::b_inv(k, L.mesh, v, s->cB, (const R*)L.LA, (R*)L.w, L.ncell, o->stream));
+    MG_CU(Prec<R>::b_inv(k, L.mesh, v, s->cB, (const R*)L.LA, (R*)L.w, L.ncell, o->stream, s->rq));
     o->launches += 1;
   } else {
     MG_CU(Prec<R>::B(k, L.mesh, v, s->cB, (R*)L.u, L.ncell, o->stream));
     MG_CU(Prec<R>::solve(k, (const R*)L.LA, 2, (const R*)L.u, 1.0, (R*)L.w, L.ncell, o->stream));
     o->launches += 2;
   }
-  MG_CU(Prec<R>::res(k, L.mesh, (const R*)L.w, (const R*)L.pfR, v, s->cdt, r, L.ncell, o->stream));
+  MG_CU(Prec<R>::res(k, L.mesh, (const R*)L.w, (const R*)L.pfR, v, s->cdt, r, L.ncell, o->stream, s->rq));
   o->launches += 1;
   return AF_OK;
 }
@@ -297,9 +298,9 @@ int chebyshev(af_schur_solver* s, Level& L, int degree, double lo, double hi, bo
     const double a = rho * rho_old, sc = ginv * 2.0 * rho / delta;
     if constexpr (Prec<R>::kFused) {
       // w = A^{-1} B d;  r += C0 w - D d;  dn = a d + sc M^{-1} r;  x += dn  (two launches)
-      MG_CU(Prec<R>::b_inv(k, L.mesh, d, s->cB, (const R*)L.LA, (R*)L.w, L.ncell, o->stream));
+      MG_CU(Prec<R>::b_inv(k, L.mesh, d, s->cB, (const R*)L.LA, (R*)L.w, L.ncell, o->stream, s->rq));
       MG_CU(Prec<R>::res_cheb(k, L.mesh, (const R*)L.w, (const R*)L.pfR, d, s->cdt, (const R*)L.LM, a, sc, r, dn, x,
-                              L.ncell, o->stream));
+                              L.ncell, o->stream, s->rq));
       o->launches += 2;
       std::swap(d, dn);
     } else {
@@ -461,6 +462,7 @@ int af_schur_default_options(af_schur_options* opt) {
   opt->min_coarse_cells = 16;
   opt->eig_iterations = 20;
   opt->restart = 30;
+  opt->reduced_quadrature = 1;
   return AF_OK;
 }
 
@@ -473,7 +475,8 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
   if (o.preconditioner < AF_SCHUR_JACOBI || o.preconditioner > AF_SCHUR_CHEB_FP32)
     return merr(AF_BAD_ARG, "af_schur_solver_create: unknown preconditioner");
   if (o.smoother_degree < 1 || o.coarse_degree < 1 || o.smoothing_range <= 1.0 || o.eig_iterations < 1 ||
-      o.restart < 1 || o.restart > 64 || !(o.coarse_lmax >= 0.0) || o.poly_degree < 1)
+      o.restart < 1 || o.restart > 64 || !(o.coarse_lmax >= 0.0) || o.poly_degree < 1 || o.reduced_quadrature < 0 ||
+      o.reduced_quadrature > 1)
     return merr(AF_BAD_ARG, "af_schur_solver_create: invalid options");
   if (o.preconditioner == AF_SCHUR_CHEB_FP64 || o.preconditioner == AF_SCHUR_CHEB_FP32) {
     // single level: the "coarse solve" on the operator's own mesh is the polynomial
@@ -485,6 +488,7 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
   s->op = op;
   s->opt = o;
   s->fp32 = o.preconditioner == AF_SCHUR_MG_FP32 || o.preconditioner == AF_SCHUR_CHEB_FP32;
+  s->rq = s->fp32 && o.reduced_quadrature != 0;
   const size_t rs = s->fp32 ? sizeof(float) : sizeof(double);
   const long ns0 = op->n_scalar();
   auto cleanup = [&](int code) {

@@ -342,6 +342,23 @@ struct ResChebPhys : CPhys<true, 1, R, false, true> {
   static constexpr int EPI = 2;
 };
 
+// Reduced-quadrature variants of the FP32 preconditioner's level operators: P+1 Gauss points
+// per direction instead of 2P+1.  On bilinear cells this integrates B (p div v: degree 2P+1
+// per direction with the adjugate of the Jacobian) and M, D exactly; C0 (p_fixed w . grad q,
+// degree 3P+1) and the rho-weighted A become approximations, which a preconditioner may use.
+template <class R>
+struct BInvRPhys : BInvPhys<R> {
+  static constexpr bool REDUCED_Q = true;
+};
+template <class R>
+struct ResChebRPhys : ResChebPhys<R> {
+  static constexpr bool REDUCED_Q = true;
+};
+template <class R>
+struct CResRPhys : CPhys<true, 1, R, false, true> {
+  static constexpr bool REDUCED_Q = true;
+};
+
 // ---------------------------------------------------------------- mass-type operators
 struct MassParams {
   double scale;

@@ -1,4 +1,5 @@
-// af_tables.cuh -- 1D basis tables for FE_DGQ(P) on Gauss-Lobatto points with QGauss(2P+1).
+// af_tables.cuh -- 1D basis tables for FE_DGQ(P) on Gauss-Lobatto points with QGauss(2P+1)
+// (and QGauss(P+1) for the reduced-quadrature preconditioner operators).
 //
 // The reference evaluates its fields with deal.II FEEvaluation<dim, p, 2p+1> (template
 // arguments at Atmospheric_Flow.cc:151-153, quadrature at :345).  Here the 1D values S and
@@ -16,16 +17,22 @@
 
 namespace af {
 
-template <int P, class R = double>
+// NQ_ Gauss points per direction: 2P+1 for the operators (the reference's quadrature), P+1
+// for the reduced-quadrature preconditioner operators.  Quadrature points pair as
+// (q, NQ-1-q) for q < QH, with a middle point q = QH when NQ is odd.
+template <int P, class R = double, int NQ_ = 2 * P + 1>
 struct TabT {
   static constexpr int P1 = P + 1;
-  static constexpr int NQ = 2 * P + 1;
+  static constexpr int NQ = NQ_;
   static constexpr int H = P1 / 2;        // node pairs (i, P-i), i < H
   static constexpr bool MIDN = (P % 2) == 0;  // a middle node exists
+  static constexpr int QH = NQ / 2;       // quadrature point pairs
+  static constexpr bool QMID = (NQ % 2) == 1;  // a middle quadrature point exists
+  static constexpr int QE = QH + (QMID ? 1 : 0);  // rows of the even/odd tables
   R S[NQ][P1], D[NQ][P1];
-  R Se[P + 1][H > 0 ? H : 1], So[P + 1][H > 0 ? H : 1];
-  R De[P + 1][H > 0 ? H : 1], Do[P + 1][H > 0 ? H : 1];
-  R Sm[P + 1], Dm[P + 1];
+  R Se[QE][H > 0 ? H : 1], So[QE][H > 0 ? H : 1];
+  R De[QE][H > 0 ? H : 1], Do[QE][H > 0 ? H : 1];
+  R Sm[QE], Dm[QE];
   R w[NQ], x[NQ];
 };
 template <int P>
@@ -137,9 +144,9 @@ inline LD dlag(const std::vector<LD>& nd, int i, LD s) {
   return acc;
 }
 
-template <int P, class R = double>
-inline TabT<P, R> make_tab() {
-  using T = TabT<P, R>;
+template <int P, class R = double, int NQ = 2 * P + 1>
+inline TabT<P, R, NQ> make_tab() {
+  using T = TabT<P, R, NQ>;
   T t{};
   std::vector<LD> nd = gll(P), x, w;
   gauss(T::NQ, x, w);
@@ -151,7 +158,7 @@ inline TabT<P, R> make_tab() {
       t.S[q][i] = (R)S[q][i];
       t.D[q][i] = (R)D[q][i];
     }
-  for (int q = 0; q <= P; ++q) {
+  for (int q = 0; q < T::QE; ++q) {
     for (int i = 0; i < T::H; ++i) {
       t.Se[q][i] = (R)((S[q][i] + S[q][P - i]) / 2);
       t.So[q][i] = (R)((S[q][i] - S[q][P - i]) / 2);

@@ -21,7 +21,7 @@ class Options(ctypes.Structure):
                 ("smoothing_range", ctypes.c_double), ("coarse_degree", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("min_coarse_cells", ctypes.c_int),
                 ("eig_iterations", ctypes.c_int), ("restart", ctypes.c_int), ("coarse_lmax", ctypes.c_double),
-                ("poly_degree", ctypes.c_int)]
+                ("poly_degree", ctypes.c_int), ("reduced_quadrature", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):

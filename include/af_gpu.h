@@ -169,6 +169,9 @@ typedef struct {
   int restart;              /* FGMRES directions per cycle, 1..64 (30)                         */
   double coarse_lmax;       /* the first level with lmax <= this is the coarsest (25)          */
   int poly_degree;          /* degree of the AF_SCHUR_CHEB_* polynomial preconditioner (16)    */
+  int reduced_quadrature;   /* FP32 levels: B, C0 with P+1 Gauss points per direction instead  */
+                            /* of 2P+1 (exact for B and D on bilinear cells, approximate for   */
+                            /* C0 and A; the outer FGMRES keeps the exact operator) (1)        */
 } af_schur_options;
 typedef struct {
   int iterations;           /* FGMRES iterations of the last solve                             */

@@ -5,7 +5,7 @@
    vanishes and the operator is linear): FP64 levels agree to 1e-12 relative, FP32 levels to
    1e-4.
 2. FGMRES with each preconditioner (Jacobi, FP64 and FP32 multigrid, FP64 and FP32 Chebyshev
-   polynomial) solves S x = S x_true
+   polynomial, the latter with reduced and full quadrature) solves S x = S x_true
    on a hill mesh to a true residual of 1e-10; the solution matches x_true and its residual,
    recomputed by the oracle's Schur apply on the CPU, is below 1e-9.
 """
@@ -153,8 +153,10 @@ def test_schur_solve_all_preconditioners():
     o.set_pres_fixed(st.p)
     o.set_NS_stage(2)
     its = {}
-    for pc in ("jacobi", "mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32"):
-        s = SchurSolver(op, pc)
+    cases = {"jacobi": {}, "mg_fp64": {}, "mg_fp32": {}, "cheb_fp64": {}, "cheb_fp32": {},
+             "cheb_fp32_full_quadrature": {"reduced_quadrature": 0}}
+    for pc, kw in cases.items():
+        s = SchurSolver(op, pc.replace("_full_quadrature", ""), **kw)
         s.setup()
         x = torch.zeros_like(b)
         out = s.solve(x, b, rel_tol=1e-10, max_iterations=5000)
@@ -165,5 +167,42 @@ def test_schur_solve_all_preconditioners():
         assert rel(xh, xt) < 1e-8, pc
         assert rel(o.vmult(xh), bh) < 1e-9, pc
     # the multigrid and polynomial preconditioners take far fewer iterations than Jacobi
-    for pc in ("mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32"):
+    for pc in ("mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32", "cheb_fp32_full_quadrature"):
         assert its[pc] * 2 < its["jacobi"], its
+
+
+def test_reduced_quadrature_preconditioner_is_exact_on_affine_cells():
+    """With P+1 Gauss points the FP32 level operators integrate B and D exactly on bilinear
+    cells, and C0 and A too when rho_for_fixed and pres_fixed are constant, so on a box mesh
+    with constant coefficients the reduced and the full-quadrature preconditioners agree to FP32
+    rounding; with the hill state's varying coefficients they differ (the reduced one is an
+    approximation)."""
+    from atmospheric_flows_b200.operator import EULEROperator
+    from atmospheric_flows_b200.schur import SchurSolver
+    P, dt = 4, 2.0
+    sc = M.Scaling()
+    out = {}
+    for name, m in (("box", M.box_mesh(16, 8, -20000.0, 20000.0, 0.0, 16000.0)), ("hill", M.hill_mesh(16, 8))):
+        n = m.n_cells * (P + 1) ** 2
+        op = EULEROperator(m, P, sc.Ma, sc.Fr, dt)
+        op.set_stream(torch.cuda.current_stream())
+        op.set_HYPERBOLIC_stage(1)
+        if name == "box":
+            op.set_rho_for_fixed(torch.full((n,), 1.3, dtype=torch.float64, device="cuda"))
+            op.set_pres_fixed(torch.full((n,), 0.9, dtype=torch.float64, device="cuda"))
+        else:
+            st = M.hill_state(m, P, modes=4)
+            op.set_rho_for_fixed(torch.from_numpy(st.rho).cuda())
+            op.set_pres_fixed(torch.from_numpy(st.p).cuda())
+        op.set_NS_stage(2)
+        b = torch.from_numpy(np.random.default_rng(5).standard_normal(n)).cuda()
+        z = {}
+        for rq in (0, 1):
+            s = SchurSolver(op, "cheb_fp32", reduced_quadrature=rq)
+            s.setup()
+            z[rq] = torch.zeros(n, dtype=torch.float64, device="cuda")
+            s.precondition(z[rq], b)
+        torch.cuda.synchronize()
+        out[name] = rel(z[1].cpu().numpy(), z[0].cpu().numpy())
+    assert out["box"] < 1e-4, out
+    assert out["hill"] > 10 * out["box"], out
