@@ -2,6 +2,7 @@
 // to the per-degree kernels, and the Schur complement orchestration.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -167,6 +168,13 @@ int af_destroy(af_operator* o) {
   cudaFree(o->d_Wm);
   cudaFree(o->d_La);
   if (o->own_stream) cudaStreamDestroy(o->own_stream);
+  if (o->copy_in) cudaStreamDestroy(o->copy_in);
+  if (o->copy_out) cudaStreamDestroy(o->copy_out);
+  if (o->ev_start) cudaEventDestroy(o->ev_start);
+  for (int k = 0; k < af_operator::kHostChunks; ++k) {
+    if (o->ev_in[k]) cudaEventDestroy(o->ev_in[k]);
+    if (o->ev_done[k]) cudaEventDestroy(o->ev_done[k]);
+  }
   delete o;
   return AF_OK;
 }
@@ -229,14 +237,19 @@ int af_set_u_fixed(af_operator* o, const double* v) {
   return copy_fixed(o, o ? o->d_u_fixed : nullptr, v, o ? 2 * o->n_scalar() : 0);
 }
 
-static int run_rhs(af_operator* o, int mask, const RhsSources& s, double* d_rho, double* d_u, double* d_p) {
+// cells [cbeg, cend) (cend < 0: the whole mesh); cbeg must be a multiple of the degree's
+// cells per CTA
+static int run_rhs(af_operator* o, int mask, const RhsSources& s, double* d_rho, double* d_u, double* d_p,
+                   int cbeg = 0, int cend = -1) {
   const double* ptrs[] = {s.rho[0], s.rho[1], s.rho[2], s.u[0], s.u[1], s.u[2], s.p[0], s.p[1], s.p[2], s.rho_c, s.u_fix,
                           d_rho, d_u, d_p};
   for (const double* p : ptrs)
     if (p && !aligned16(p)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
   const RhsParams prm = rhs_params(o, o->hs);
-  cudaError_t e = o->ops->rhs(o->mesh, o->hs, mask, s, prm, d_rho, d_u, d_p, o->ncell, o->stream);
+  MeshDev m = o->mesh;
+  m.cell0 = cbeg;
+  cudaError_t e = o->ops->rhs(m, o->hs, mask, s, prm, d_rho, d_u, d_p, cend < 0 ? o->ncell : cend, o->stream);
   if (e == cudaErrorInvalidValue) return fail(AF_BAD_ARG, "rhs: missing source or output for stage %d", o->hs);
   AF_CU(e);
   o->launches += 1;
@@ -279,7 +292,9 @@ int af_vmult_rhs_pressure(af_operator* o, double* dst, const double* const* src,
   return run_rhs(o, 4, s, nullptr, nullptr, dst);
 }
 
-int af_vmult_rhs_fused(af_operator* o, double* d_rho, double* d_u, double* d_p, const double* const* src, int n) {
+// the fused rhs over cells [cbeg, cend) (see run_rhs)
+static int rhs_fused_range(af_operator* o, double* d_rho, double* d_u, double* d_p, const double* const* src, int n,
+                           int cbeg, int cend) {
   if (!o || !src) return fail(AF_BAD_ARG, "null argument");
   const int mask = (d_rho ? 1 : 0) | (d_u ? 2 : 0) | (d_p ? 4 : 0);
   if (mask == 0) return fail(AF_BAD_ARG, "af_vmult_rhs_fused: no output requested");
@@ -288,15 +303,19 @@ int af_vmult_rhs_fused(af_operator* o, double* d_rho, double* d_u, double* d_p, 
     RhsSources s;
     int r = pressure_sources(o, src, n, s);
     if (r != AF_OK) return r;
-    r = run_rhs(o, 1, s, d_rho, nullptr, nullptr);
+    r = run_rhs(o, 1, s, d_rho, nullptr, nullptr, cbeg, cend);
     if (r != AF_OK) return r;
-    return run_rhs(o, mask & 6, s, nullptr, d_u, d_p);
+    return run_rhs(o, mask & 6, s, nullptr, d_u, d_p, cbeg, cend);
   }
   RhsSources s;
   int r = pressure_sources(o, src, n, s);
   if (r != AF_OK) return r;
   if (mask == 2 && o->hs == 3) s.rho_c = nullptr;
-  return run_rhs(o, mask, s, d_rho, d_u, d_p);
+  return run_rhs(o, mask, s, d_rho, d_u, d_p, cbeg, cend);
+}
+
+int af_vmult_rhs_fused(af_operator* o, double* d_rho, double* d_u, double* d_p, const double* const* src, int n) {
+  return rhs_fused_range(o, d_rho, d_u, d_p, src, n, 0, -1);
 }
 
 int af_vmult_rhs_fused_backward(af_operator* o, const double* const* src, int n, const double* ybar_rho,
@@ -349,22 +368,70 @@ int af_vmult_rhs_fused_host(af_operator* o, double* h_rho, double* h_u, double* 
     AF_CU(cudaMalloc(&o->d_stage, total * sizeof(double)));
     o->stage_len = total;
   }
-  std::vector<const double*> d_src(n);
+  // Rows of cells go through in chunks so that the copies overlap the kernel: the sources of
+  // chunk k+1 travel (copy_in) while chunk k is computed (the operator's stream) and chunk
+  // k-1's results return (copy_out).  A chunk's kernel also reads the row of cells above it
+  // (face neighbours), so it starts once the next chunk's sources are in.  Chunk boundaries
+  // are multiples of the kernel's cells per CTA; otherwise the call runs as one chunk.
+  const int nx = o->mesh.nx, nz = o->mesh.nz, cpb = o->ops->cells_per_block;
+  int rpc = (nz + af_operator::kHostChunks - 1) / af_operator::kHostChunks;  // rows per chunk
+  if (((long)rpc * nx) % cpb != 0) rpc = nz;
+  const int K = (nz + rpc - 1) / rpc;
+  if (!o->copy_in) AF_CU(cudaStreamCreateWithFlags(&o->copy_in, cudaStreamNonBlocking));
+  if (!o->copy_out) AF_CU(cudaStreamCreateWithFlags(&o->copy_out, cudaStreamNonBlocking));
+  if (!o->ev_start) {
+    AF_CU(cudaEventCreateWithFlags(&o->ev_start, cudaEventDisableTiming));
+    for (int k = 0; k < af_operator::kHostChunks; ++k) {
+      AF_CU(cudaEventCreateWithFlags(&o->ev_in[k], cudaEventDisableTiming));
+      AF_CU(cudaEventCreateWithFlags(&o->ev_done[k], cudaEventDisableTiming));
+    }
+  }
+  std::vector<double*> d_src(n);
   double* cur = o->d_stage;
   for (int k = 0; k < n; ++k) {
     if (!h_src[k]) return fail(AF_BAD_ARG, "af_vmult_rhs_fused_host: null source %d", k);
-    AF_CU(cudaMemcpyAsync(cur, h_src[k], len[k] * sizeof(double), cudaMemcpyHostToDevice, o->stream));
     d_src[k] = cur;
     cur += up2(len[k]);
   }
   double* d_rho = h_rho ? cur : nullptr;
   double* d_u = h_u ? cur + up2(ns) : nullptr;
   double* d_p = h_p ? cur + up2(ns) + 2 * ns : nullptr;
-  int r = af_vmult_rhs_fused(o, d_rho, d_u, d_p, d_src.data(), n);
-  if (r != AF_OK) return r;
-  if (h_rho) AF_CU(cudaMemcpyAsync(h_rho, d_rho, ns * sizeof(double), cudaMemcpyDeviceToHost, o->stream));
-  if (h_u) AF_CU(cudaMemcpyAsync(h_u, d_u, 2 * ns * sizeof(double), cudaMemcpyDeviceToHost, o->stream));
-  if (h_p) AF_CU(cudaMemcpyAsync(h_p, d_p, ns * sizeof(double), cudaMemcpyDeviceToHost, o->stream));
+  const long nd = o->nd;
+  // the staging buffer is reused: copies start after earlier work on the operator's stream
+  AF_CU(cudaEventRecord(o->ev_start, o->stream));
+  AF_CU(cudaStreamWaitEvent(o->copy_in, o->ev_start, 0));
+  AF_CU(cudaStreamWaitEvent(o->copy_out, o->ev_start, 0));
+  for (int c = 0; c < K; ++c) {
+    const long c0 = (long)c * rpc * nx, c1 = std::min<long>((long)(c + 1) * rpc, nz) * nx;
+    for (int k = 0; k < n; ++k) {
+      const long comps = len[k] / ns, off = c0 * comps * nd, cnt = (c1 - c0) * comps * nd;
+      AF_CU(cudaMemcpyAsync(d_src[k] + off, h_src[k] + off, cnt * sizeof(double), cudaMemcpyHostToDevice,
+                            o->copy_in));
+    }
+    AF_CU(cudaEventRecord(o->ev_in[c], o->copy_in));
+  }
+  std::vector<const double*> d_srcc(d_src.begin(), d_src.end());
+  for (int c = 0; c < K; ++c) {
+    const long c0 = (long)c * rpc * nx, c1 = std::min<long>((long)(c + 1) * rpc, nz) * nx;
+    AF_CU(cudaStreamWaitEvent(o->stream, o->ev_in[std::min(c + 1, K - 1)], 0));
+    const int r = rhs_fused_range(o, d_rho, d_u, d_p, d_srcc.data(), n, (int)c0, (int)c1);
+    if (r != AF_OK) {
+      cudaStreamSynchronize(o->copy_in);
+      return r;
+    }
+    AF_CU(cudaEventRecord(o->ev_done[c], o->stream));
+    AF_CU(cudaStreamWaitEvent(o->copy_out, o->ev_done[c], 0));
+    const long cnt = (c1 - c0) * nd;
+    if (h_rho)
+      AF_CU(cudaMemcpyAsync(h_rho + c0 * nd, d_rho + c0 * nd, cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                            o->copy_out));
+    if (h_u)
+      AF_CU(cudaMemcpyAsync(h_u + 2 * c0 * nd, d_u + 2 * c0 * nd, 2 * cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                            o->copy_out));
+    if (h_p)
+      AF_CU(cudaMemcpyAsync(h_p + c0 * nd, d_p + c0 * nd, cnt * sizeof(double), cudaMemcpyDeviceToHost, o->copy_out));
+  }
+  AF_CU(cudaStreamSynchronize(o->copy_out));
   AF_CU(cudaStreamSynchronize(o->stream));
   return AF_OK;
 }

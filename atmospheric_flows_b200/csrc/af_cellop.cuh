@@ -35,6 +35,8 @@ struct MeshDev {
   const double2* vtx;  // (nz+1)*(nx+1) vertices, row-major in (j, i)
   int nx, nz, periodic_x, gravity;
   double radial_a;
+  int cell0;  // cell kernels: the first cell of the launch (a multiple of its cells per CTA);
+              // the launch covers [cell0, ncell).  0 for whole-mesh launches
 };
 
 struct PointGeo {
@@ -380,7 +382,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   R* s_minv = smem + L::OE;
   bool epi_bulk = false;
   if constexpr (L::EPI != 0) {
-    const int c0e = blockIdx.x * CB, ncbe = min(CB, ncell - c0e);
+    const int c0e = mesh.cell0 + blockIdx.x * CB, ncbe = min(CB, ncell - c0e);
     const size_t bytes = sizeof(R) * (size_t)ncbe * ND;
     const R* srcm = prm.inv + (size_t)c0e * ND;
     epi_bulk = bytes % 16 == 0 && (reinterpret_cast<size_t>(srcm) & 15) == 0;
@@ -403,7 +405,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   const int tid = threadIdx.x;
   const int m = tid / CB;   // member: row / column / face point
   const int cl = tid % CB;  // cell within the block
-  const int c0 = blockIdx.x * CB;
+  const int c0 = mesh.cell0 + blockIdx.x * CB;
   const int ncb = min(CB, ncell - c0);  // valid cells in this block
   const int c = c0 + (cl < ncb ? cl : ncb - 1);
 
@@ -933,7 +935,9 @@ cudaError_t launch_cellop(const MeshDev& mesh,
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  const int nblk = (ncell + L::CB - 1) / L::CB;
+  if (mesh.cell0 % L::CB != 0 || mesh.cell0 < 0) return cudaErrorInvalidValue;
+  if (ncell <= mesh.cell0) return cudaSuccess;
+  const int nblk = (ncell - mesh.cell0 + L::CB - 1) / L::CB;
   k_cellop<P, Phys, CB_, MINB><<<nblk, L::NT, L::BYTES, stream>>>(mesh, ptr, prm, ncell);
   return cudaGetLastError();
 }

@@ -42,9 +42,13 @@ struct af_operator {
   double* d_Wm = nullptr;
   double* d_La = nullptr;
   bool Wm_valid = false, La_valid = false;
-  // host-buffer entry points: device staging
+  // host-buffer entry points: device staging, and the copy streams and events of the
+  // row-chunk pipeline (sources in / results out overlapping the kernel)
+  static constexpr int kHostChunks = 16;
   double* d_stage = nullptr;
   size_t stage_len = 0;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_in[kHostChunks] = {}, ev_done[kHostChunks] = {};
 
   long n_scalar() const { return (long)ncell * nd; }
 };
