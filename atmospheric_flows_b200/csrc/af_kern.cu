@@ -16,6 +16,7 @@ namespace af {
 static __constant__ Tab<AF_P> c_tab;
 static __constant__ TabT<AF_P, float> c_tabf;
 static __constant__ TabT<AF_P, float, AF_P + 1> c_tabfr;  // reduced quadrature (preconditioner)
+static __constant__ TabT<AF_P, double, AF_P + 1> c_tabr;  // reduced quadrature (exact B)
 static __constant__ TransT<AF_P, double> c_tr;
 static __constant__ TransT<AF_P, float> c_trf;
 static __constant__ CobT<AF_P, double> c_cob;
@@ -34,6 +35,10 @@ __device__ __forceinline__ const TabT<AF_P, float, AF_P + 1>& tabr<AF_P, float, 
   return c_tabfr;
 }
 template <>
+__device__ __forceinline__ const TabT<AF_P, double, AF_P + 1>& tabr<AF_P, double, AF_P + 1>() {
+  return c_tabr;
+}
+template <>
 __device__ __forceinline__ const CobT<AF_P, double>& cobr<AF_P, double>() {
   return c_cob;
 }
@@ -45,11 +50,15 @@ __device__ __forceinline__ const CobT<AF_P, float>& cobr<AF_P, float>() {
 namespace {
 
 constexpr int P = AF_P;
+// cells per CTA of the reduced-quadrature (P+1 points) B kernel: its CTAs have NQ = P+1
+// threads per cell, about half of the full-quadrature kernel's
+constexpr int kReducedCB = P == 4 ? 32 : cells_per_block<P>();
 
 cudaError_t upload_tables() {
   static const Tab<P> t = host::make_tab<P>();
   static const TabT<P, float> tf = host::make_tab<P, float>();
   static const TabT<P, float, P + 1> tfr = host::make_tab<P, float, P + 1>();
+  static const TabT<P, double, P + 1> tr1 = host::make_tab<P, double, P + 1>();
   static const TransT<P, double> tr = host::make_trans<P, double>();
   static const TransT<P, float> trf = host::make_trans<P, float>();
   static const CobT<P, double> cob = host::make_cob<P, double>();
@@ -59,6 +68,7 @@ cudaError_t upload_tables() {
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_cobf, &cobf, sizeof(cobf));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tabf, &tf, sizeof(tf));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tabfr, &tfr, sizeof(tfr));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tabr, &tr1, sizeof(tr1));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tr, &tr, sizeof(tr));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_trf, &trf, sizeof(trf));
   return e;
@@ -135,7 +145,7 @@ cudaError_t mass(const MeshDev& mesh, int ncomp, const double* src, const double
 
 cudaError_t op_B(const MeshDev& mesh, const double* p, double c, double* u, int ncell, cudaStream_t st) {
   ArgPtrs<1, 1> a{{p}, {u}};
-  return launch_cellop<P, BPhys>(mesh, a, BParams{c}, ncell, st);
+  return launch_cellop<P, BPhysExactReduced, kReducedCB>(mesh, a, BParams{c}, ncell, st);
 }
 
 cudaError_t op_C(const MeshDev& mesh, const double* w, const double* pf, const double* p, const CParams& prm,

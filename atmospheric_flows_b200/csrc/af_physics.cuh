@@ -249,6 +249,14 @@ struct BPhysT {
 };
 using BPhys = BPhysT<double>;
 
+// B of the operator with P+1 Gauss points per direction: the same bilinear form exactly (on a
+// bilinear cell p, the adjugate of the Jacobian and the test gradient give degree <= 2P per
+// direction, the face terms degree 2P), so it equals the 2P+1-point result up to rounding,
+// at a little over half of the work.
+struct BPhysExactReduced : BPhysT<double> {
+  static constexpr bool REDUCED_Q = true;
+};
+
 // B followed by the cell-wise A^{-1} in the kernel's epilogue: w = scale A^{-1} B p, with A^{-1}
 // by the change of basis to the Gauss points (inv = 1 / (rho JxW) there; cellop epilogue 1).
 template <class R>
