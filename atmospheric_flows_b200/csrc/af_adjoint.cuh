@@ -403,4 +403,86 @@ struct CTPhys {
   __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
 };
 
+// Derivatives of the implicit operators with respect to their fixed coefficients, transposed
+// (the tangents are the forward operators themselves, since A is linear in rho_for_fixed and C
+// is linear in pres_fixed):
+//   A(rho) x = int rho x . phi  ->  (d/drho [A(rho) x])^T y :  rhobar_j = int psi_j (x . y)
+// One group: x (2), y (2), no faces.  Output: rhobar (1).
+struct MassRhoTPhys {
+  static constexpr int NG = 1;
+  static constexpr bool FACES = false, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = 1;
+  using Params = MassParams;
+  using real = double;
+  static constexpr int out_ncomp(int) { return 1; }
+  static constexpr bool has_val(int) { return true; }
+  static constexpr bool has_grad(int) { return false; }
+  static constexpr int narr_of(int) { return 2; }
+  static constexpr int nf_of(int) { return 4; }
+  static constexpr int nfc_of(int) { return 4; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = 2;
+    static constexpr bool FACE = false;
+    static constexpr int ncomp(int) { return 2; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params&, const double* v, const PointGeo&, double* val,
+                                               double (*)[2]) {
+    val[0] += v[0] * v[2] + v[1] * v[3];
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params&, const double*, const double*, const double*, double*) {}
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
+};
+
+//   C(w; p_f) (vmult_enthalpy, euler_operator.h:1413-1507) is linear in p_f for a fixed w:
+//   (d/dp_f [C(w; p_f)])^T pbar = pfbar:
+//   cell:  pfbar = -cdt gg w . grad(pbar_h) (tested with psi)
+//   face:  F = cdt (gg/2 (p_f+ w+.n + p_f- w-.n) + g1/2 lambda(w) (p_f+ - p_f-)) enters the two
+//          sides with opposite signs, so  pfbar+ += cdt (gg/2 w+.n + g1/2 lambda) (pbar+ - pbar-)
+//   walls: no term (as C).
+// One group: w (2), pbar (gradient field).  Output: pfbar (1).
+struct CPfTPhys {
+  static constexpr int NG = 1;
+  static constexpr bool FACES = true, NEED_X = false, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = 1, NOUT = 1;
+  using Params = CParams;
+  using real = double;
+  static constexpr int out_ncomp(int) { return 1; }
+  static constexpr bool has_val(int) { return true; }
+  static constexpr bool has_grad(int) { return false; }
+  static constexpr int narr_of(int) { return 2; }
+  static constexpr int nf_of(int) { return 3; }
+  static constexpr int nfc_of(int) { return 3; }
+  static constexpr int nfg_of(int) { return 1; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = 2;
+    static constexpr bool FACE = true;
+    static constexpr int ncomp(int a) { return a == 0 ? 2 : 1; }
+    static constexpr bool face_only(int) { return false; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const double* deta,
+                                               const PointGeo& pg, double* val, double (*)[2]) {
+    const double J00 = pg.J[0], J01 = pg.J[1], J10 = pg.J[2], J11 = pg.J[3];
+    const double idet = 1.0 / (J00 * J11 - J01 * J10);
+    // v[3]: d/dxi of pbar (the gradient slot after the three cell fields), deta[0]: d/deta
+    const double gx = (J11 * v[3] - J10 * deta[0]) * idet, gz = (J00 * deta[0] - J01 * v[3]) * idet;
+    val[0] += -prm.cdt * prm.gg * (v[0] * gx + v[1] * gz);
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    const double wnp = vp[0] * n[0] + vp[1] * n[1], wnm = vm[0] * n[0] + vm[1] * n[1];
+    const double lam = fmax(fabs(wnp), fabs(wnm));
+    flux[0] = prm.cdt * (0.5 * prm.gg * wnp + 0.5 * prm.g1 * lam) * (vp[2] - vm[2]);
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params&, const double*, const double*, double*) {}
+};
+
 }  // namespace af

@@ -665,6 +665,24 @@ int af_vmult_enthalpy_transpose(af_operator* o, double* wbar, const double* w, c
   return AF_OK;
 }
 
+int af_vmult_velocity_mass_rho_transpose(af_operator* o, double* rhobar, const double* x, const double* y) {
+  if (!o || !rhobar || !x || !y) return fail(AF_BAD_ARG, "null argument");
+  if (!aligned16(rhobar) || !aligned16(x) || !aligned16(y)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
+  AF_CU(cudaSetDevice(o->device));
+  AF_CU(o->ops->op_A_rho_T(o->mesh, x, y, rhobar, o->ncell, o->stream));
+  o->launches += 1;
+  return AF_OK;
+}
+
+int af_vmult_enthalpy_pf_transpose(af_operator* o, double* pfbar, const double* w, const double* pbar) {
+  if (!o || !pfbar || !w || !pbar) return fail(AF_BAD_ARG, "null argument");
+  if (!aligned16(pfbar) || !aligned16(w) || !aligned16(pbar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
+  AF_CU(cudaSetDevice(o->device));
+  AF_CU(o->ops->op_C_pf_T(o->mesh, w, pbar, c_params(o), pfbar, o->ncell, o->stream));
+  o->launches += 1;
+  return AF_OK;
+}
+
 // w = A^{-1} B p into the workspace (2 ns), exact inverse
 static int schur_w(af_operator* o, const double* p, double* w, double* t) {
   AF_CU(o->ops->op_B(o->mesh, p, coeff_BC(o) * o->dt / (o->Ma * o->Ma), t, o->ncell, o->stream));

@@ -48,6 +48,12 @@ struct af_imex {
   KrylovState* kst;
   af_schur_solver* schur = nullptr;  // FGMRES + Jacobi/multigrid (schur_preconditioner >= 0)
   af_imex_stats stats{};
+  // stage-1 tangent / adjoint: the recorded fixed-point trajectory (pres_fixed and u_fixed
+  // entering each iteration, and the final iterate) and a workspace, allocated on first use
+  bool record = false;
+  int rec_iters = 0;
+  std::vector<double*> rec_p, rec_u;
+  double* adj_mem = nullptr;
 };
 
 static int ierr(int code, const std::string& msg) {
@@ -67,6 +73,21 @@ static int ierr(int code, const std::string& msg) {
   } while (0)
 
 using Apply = std::function<int(const double*, double*)>;
+
+// trajectory buffers of the stage-1 tangent / adjoint, one pair per fixed-point iterate
+static int ensure_rec(af_imex* h, int i) {
+  while ((int)h->rec_p.size() <= i) {
+    double *p = nullptr, *u = nullptr;
+    IM_CU(cudaMalloc(&p, h->ns * 8));
+    if (cudaMalloc(&u, 2 * h->ns * 8) != cudaSuccess) {
+      cudaFree(p);
+      return ierr(AF_CUDA, "stage-1 trajectory: device allocation failed");
+    }
+    h->rec_p.push_back(p);
+    h->rec_u.push_back(u);
+  }
+  return AF_OK;
+}
 
 // CG with Jacobi, x the initial guess, tolerance eps*|b| (deal.II SolverControl + SolverCG)
 static int cg_solve(af_imex* h, const Apply& A, const double* invd, double* x, const double* b, long n, double eps,
@@ -306,6 +327,11 @@ static int fixed_point(af_imex* h, int stage, double* p_out, double* u_out) {
   int iters = 0;
   double err = 0.0;
   for (int iter = 0; iter < h->opt.fixed_point_max_iterations; ++iter) {
+    if (h->record) {  // the iteration's inputs: pres_fixed (pfix_old) and u_fixed
+      IM_AF(ensure_rec(h, iter));
+      IM_CU(cudaMemcpyAsync(h->rec_p[iter], h->pfix_old, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+      IM_CU(cudaMemcpyAsync(h->rec_u[iter], h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+    }
     IM_AF(pressure_fixed_point(h, stage, iter));
     IM_AF(update_velocity(h, stage));
     ++iters;
@@ -320,6 +346,12 @@ static int fixed_point(af_imex* h, int stage, double* p_out, double* u_out) {
   }
   h->stats.fixed_point_iterations[stage - 1] = iters;
   h->stats.last_fixed_point_error = err;
+  if (h->record) {  // the final iterate
+    IM_AF(ensure_rec(h, iters));
+    IM_CU(cudaMemcpyAsync(h->rec_p[iters], h->pfix, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+    IM_CU(cudaMemcpyAsync(h->rec_u[iters], h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+    h->rec_iters = iters;
+  }
   IM_CU(cudaMemcpyAsync(p_out, h->pfix, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
   IM_CU(cudaMemcpyAsync(u_out, h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
   return AF_OK;
@@ -350,6 +382,246 @@ static int one_step(af_imex* h) {
   IM_AF(update_pressure(h));
   IM_CU(cudaMemcpyAsync(h->rho0, h->rhoc, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
   IM_CU(cudaMemcpyAsync(h->u0, h->uc, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  return AF_OK;
+}
+
+// ------------------------------------------------------------------ stage-1 tangent and adjoint
+// Stage 1 as a map (rho0, u0, p0) -> (rho2, u2, p2): the density update and the pressure fixed
+// point (update_density, pressure_fixed_point, update_velocity; Atmospheric_Flow.cc:1116-1156).
+// The tangent-linear and the adjoint differentiate the iterations as the forward ran them
+// (the recorded number of fixed-point iterations), each linear solve taken as exact: with
+// P_i, U_i the pres_fixed and u_fixed entering iteration i (P_0 = p0, U_0 = u0),
+//   rhs_p, rhs_u = R(rho0, u0, p0, rho2, U_i)           (fused stage-1 rhs triple)
+//   t       = A^{-1} rhs_u                                (A = A(rho2), rho2 = M^{-1} R_rho(rho0, u0))
+//   b       = rhs_p - C(t; P_i)
+//   P_{i+1} : S(P_i; P_{i+1}) = b,   S(p_f; p) = D p - C(A^{-1} B p; p_f)
+//   U_{i+1} = A^{-1} (rhs_u - B P_{i+1}).
+// A is linear in rho2 and C in p_f, so their coefficient tangents are the operators with the
+// perturbation as the coefficient: A(drho) x and C(w; dp_f).  Linearising the solve for P_{i+1}:
+//   J_S(P_{i+1}) dP = db - J_C(w) A^{-1} A(drho2) w + C(w; dP_i),   w = A^{-1} B P_{i+1}.
+
+constexpr int kAdjVectors = 28;  // velocity-sized work vectors of the tangent / adjoint
+
+static int ensure_adj(af_imex* h) {
+  if (h->adj_mem) return AF_OK;
+  IM_CU(cudaMalloc(&h->adj_mem, sizeof(double) * 2 * h->ns * kAdjVectors));
+  return AF_OK;
+}
+
+namespace {
+struct Stage1Ctx {
+  af_imex* h;
+  af_operator* o;
+  long ns;
+  cudaStream_t st;
+  CParams cp;
+  double* v[kAdjVectors];
+  int next = 0;
+  double* take() { return v[next++]; }
+};
+}  // namespace
+
+static int s1_ctx(af_imex* h, Stage1Ctx& c) {
+  if (!h->schur) return ierr(AF_UNSUPPORTED, "stage-1 tangent/adjoint: needs schur_preconditioner >= 0");
+  if (h->rec_iters < 1) return ierr(AF_BAD_ARG, "stage-1 tangent/adjoint: call af_imex_stage1_forward first");
+  IM_AF(ensure_adj(h));
+  c.h = h;
+  c.o = h->op;
+  c.ns = h->ns;
+  c.st = h->op->stream;
+  c.cp.cdt = h->op->a22t * h->op->dt;  // stage 1: the B/C coefficient a~22 (euler_operator.h:1428)
+  c.cp.g1 = 1.0 / (1.4 - 1.0);
+  c.cp.gg = 1.4 / (1.4 - 1.0);
+  for (int k = 0; k < kAdjVectors; ++k) c.v[k] = h->adj_mem + (size_t)k * 2 * h->ns;
+  IM_AF(af_set_HYPERBOLIC_stage(h->op, 1));
+  return AF_OK;
+}
+
+// x = A^{-1} b (NS 3) or M^{-1} b (NS 1), exact cell-wise inverses
+static int s1_inv(Stage1Ctx& c, int ns_stage, double* x, const double* b) {
+  IM_AF(af_set_NS_stage(c.o, ns_stage));
+  return af_vmult_inverse(c.o, x, b);
+}
+// dst = A(rho) x  (rho-weighted velocity mass with an arbitrary weight)
+static int s1_A(Stage1Ctx& c, const double* rho, const double* x, double* dst) {
+  IM_CU(c.o->ops->mass(c.o->mesh, 2, x, rho, 1.0, dst, c.o->ncell, c.st));
+  c.o->launches += 1;
+  return AF_OK;
+}
+// dst = C(w; pf)  (vmult_enthalpy with an arbitrary pres_fixed)
+static int s1_C(Stage1Ctx& c, const double* w, const double* pf, double* dst) {
+  IM_CU(c.o->ops->op_C(c.o->mesh, w, pf, nullptr, c.cp, dst, c.o->ncell, c.st));
+  c.o->launches += 1;
+  return AF_OK;
+}
+static int s1_axpby(Stage1Ctx& c, double a, const double* x, double b, double* y, long n) {
+  IM_CU(axpby(a, x, b, y, n, c.st));
+  c.o->launches += 1;
+  return AF_OK;
+}
+static int s1_copy(Stage1Ctx& c, double* dst, const double* src, long n) {
+  IM_CU(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToDevice, c.st));
+  return AF_OK;
+}
+static int s1_zero(Stage1Ctx& c, double* x, long n) {
+  IM_CU(cudaMemsetAsync(x, 0, n * 8, c.st));
+  return AF_OK;
+}
+// rhs_u at the linearisation point and t = A^{-1} rhs_u
+static int s1_rhs_u_t(Stage1Ctx& c, double* rhs_u, double* t) {
+  af_imex* h = c.h;
+  const double* su[] = {h->rho0, h->u0, h->p0, h->rho2};
+  IM_AF(af_vmult_rhs_velocity_fixed(c.o, rhs_u, su, 4));
+  return s1_inv(c, 3, t, rhs_u);
+}
+static int s1_tangent(af_imex* h, const double* drho0, const double* du0, const double* dp0, double* drho2_out,
+                      double* du2, double* dp2, double tol, int maxit) {
+  Stage1Ctx c;
+  IM_AF(s1_ctx(h, c));
+  const long ns = c.ns;
+  af_operator* o = c.o;
+  double *zs = c.take(), *zv = c.take(), *rhs_u = c.take(), *t = c.take(), *drr = c.take(), *drhs_u = c.take();
+  double *drhs_p = c.take(), *tmpA = c.take(), *dt = c.take(), *jc = c.take(), *cc = c.take(), *db = c.take();
+  double *Bp = c.take(), *w = c.take(), *aw = c.take(), *z = c.take(), *jz = c.take(), *cw = c.take();
+  double *dP = c.take(), *dU = c.take(), *dPf = c.take(), *dUf = c.take(), *drho2 = c.take(), *bdp = c.take();
+  IM_AF(s1_zero(c, zs, ns));
+  IM_AF(s1_zero(c, zv, 2 * ns));
+  IM_AF(s1_rhs_u_t(c, rhs_u, t));
+  // drho2 = M^{-1} dR_rho (the density rhs depends on rho0 and u0 only)
+  {
+    const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, h->rec_u[0]};
+    const double* dsrc[] = {drho0, du0, dp0, zs, zv};
+    IM_AF(af_vmult_rhs_fused_tangent(o, src, 5, dsrc, drr, drhs_u, drhs_p));
+    IM_AF(s1_inv(c, 1, drho2, drr));
+  }
+  IM_AF(s1_copy(c, dPf, dp0, ns));
+  IM_AF(s1_copy(c, dUf, du0, 2 * ns));
+  for (int i = 0; i < h->rec_iters; ++i) {
+    const double *Pi = h->rec_p[i], *Ui = h->rec_u[i], *Pn = h->rec_p[i + 1], *Un = h->rec_u[i + 1];
+    const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, Ui};
+    const double* dsrc[] = {drho0, du0, dp0, drho2, dUf};
+    IM_AF(af_vmult_rhs_fused_tangent(o, src, 5, dsrc, drr, drhs_u, drhs_p));
+    // dt = A^{-1} (drhs_u - A(drho2) t)
+    IM_AF(s1_A(c, drho2, t, tmpA));
+    IM_AF(s1_axpby(c, 1.0, drhs_u, -1.0, tmpA, 2 * ns));
+    IM_AF(s1_inv(c, 3, dt, tmpA));
+    // db = drhs_p - J_C(t; P_i) dt - C(t; dP_i)
+    IM_AF(af_set_pres_fixed(o, Pi));
+    IM_AF(af_vmult_enthalpy_tangent(o, jc, t, dt));
+    IM_AF(s1_C(c, t, dPf, cc));
+    IM_AF(s1_copy(c, db, drhs_p, ns));
+    IM_AF(s1_axpby(c, -1.0, jc, 1.0, db, ns));
+    IM_AF(s1_axpby(c, -1.0, cc, 1.0, db, ns));
+    // right-hand side of J_S(P_{i+1}) dP: db - J_C(w) A^{-1} A(drho2) w + C(w; dP_i)
+    IM_AF(af_vmult_pressure(o, Bp, Pn));
+    IM_AF(s1_inv(c, 3, w, Bp));
+    IM_AF(s1_A(c, drho2, w, aw));
+    IM_AF(s1_inv(c, 3, z, aw));
+    IM_AF(af_vmult_enthalpy_tangent(o, jz, w, z));
+    IM_AF(s1_C(c, w, dPf, cw));
+    IM_AF(s1_axpby(c, -1.0, jz, 1.0, db, ns));
+    IM_AF(s1_axpby(c, 1.0, cw, 1.0, db, ns));
+    IM_AF(s1_zero(c, dP, ns));
+    af_schur_stats sst{};
+    IM_AF(af_schur_solve_tangent(h->schur, Pn, dP, db, tol, maxit, &sst));
+    // dU = A^{-1} (drhs_u - B dP - A(drho2) U_{i+1})
+    IM_AF(af_vmult_pressure(o, bdp, dP));
+    IM_AF(s1_A(c, drho2, Un, tmpA));
+    IM_AF(s1_axpby(c, 1.0, drhs_u, -1.0, tmpA, 2 * ns));
+    IM_AF(s1_axpby(c, -1.0, bdp, 1.0, tmpA, 2 * ns));
+    IM_AF(s1_inv(c, 3, dU, tmpA));
+    IM_AF(s1_copy(c, dPf, dP, ns));
+    IM_AF(s1_copy(c, dUf, dU, 2 * ns));
+  }
+  IM_AF(s1_copy(c, drho2_out, drho2, ns));
+  IM_AF(s1_copy(c, du2, dUf, 2 * ns));
+  IM_AF(s1_copy(c, dp2, dPf, ns));
+  IM_CU(cudaStreamSynchronize(c.st));
+  return AF_OK;
+}
+
+// the transpose of s1_tangent, step by step in reverse
+static int s1_backward(af_imex* h, const double* rho2bar, const double* u2bar, const double* p2bar, double* rho0bar,
+                       double* u0bar, double* p0bar, double tol, int maxit) {
+  Stage1Ctx c;
+  IM_AF(s1_ctx(h, c));
+  const long ns = c.ns;
+  af_operator* o = c.o;
+  double *zs = c.take(), *rhs_u = c.take(), *t = c.take(), *R0 = c.take(), *U0 = c.take(), *P0 = c.take();
+  double *R2 = c.take(), *Pb = c.take(), *Ub = c.take(), *rub = c.take(), *rpb = c.take(), *Pfb = c.take();
+  double *s1 = c.take(), *tmp = c.take(), *x = c.take(), *Bp = c.take(), *w = c.take(), *jt = c.take();
+  double *z = c.take(), *ts = c.take(), *dtb = c.take(), *rrb = c.take();
+  double* xb[5] = {c.take(), c.take(), c.take(), c.take(), c.take()};
+  IM_AF(s1_zero(c, zs, ns));
+  IM_AF(s1_zero(c, R0, ns));
+  IM_AF(s1_zero(c, U0, 2 * ns));
+  IM_AF(s1_zero(c, P0, ns));
+  IM_AF(s1_copy(c, R2, rho2bar, ns));
+  IM_AF(s1_copy(c, Pb, p2bar, ns));
+  IM_AF(s1_copy(c, Ub, u2bar, 2 * ns));
+  IM_AF(s1_rhs_u_t(c, rhs_u, t));
+  for (int i = h->rec_iters - 1; i >= 0; --i) {
+    const double *Pi = h->rec_p[i], *Ui = h->rec_u[i], *Pn = h->rec_p[i + 1], *Un = h->rec_u[i + 1];
+    IM_AF(af_set_pres_fixed(o, Pi));
+    IM_AF(s1_zero(c, rpb, ns));
+    IM_AF(s1_zero(c, Pfb, ns));
+    // U_{i+1} = A^{-1} (rhs_u - B P_{i+1}):  s1 = A^{-1} Ub
+    IM_AF(s1_inv(c, 3, s1, Ub));
+    IM_AF(s1_copy(c, rub, s1, 2 * ns));
+    IM_AF(af_vmult_pressure_transpose(o, tmp, s1));
+    IM_AF(s1_axpby(c, -1.0, tmp, 1.0, Pb, ns));
+    IM_AF(af_vmult_velocity_mass_rho_transpose(o, ts, Un, s1));
+    IM_AF(s1_axpby(c, -1.0, ts, 1.0, R2, ns));
+    // P_{i+1}: x = J_S(P_{i+1})^{-T} Pb is the cotangent of db
+    IM_AF(s1_zero(c, x, ns));
+    af_schur_stats sst{};
+    IM_AF(af_schur_solve_transpose(h->schur, Pn, x, Pb, tol, maxit, &sst));
+    IM_AF(af_vmult_pressure(o, Bp, Pn));
+    IM_AF(s1_inv(c, 3, w, Bp));
+    IM_AF(af_vmult_enthalpy_pf_transpose(o, ts, w, x));  // + C(w; dP_i)
+    IM_AF(s1_axpby(c, 1.0, ts, 1.0, Pfb, ns));
+    IM_AF(af_vmult_enthalpy_transpose(o, jt, w, x));     // - J_C(w) A^{-1} A(drho2) w
+    IM_AF(s1_inv(c, 3, z, jt));
+    IM_AF(af_vmult_velocity_mass_rho_transpose(o, ts, w, z));
+    IM_AF(s1_axpby(c, -1.0, ts, 1.0, R2, ns));
+    // db = drhs_p - J_C(t) dt - C(t; dP_i)
+    IM_AF(s1_axpby(c, 1.0, x, 1.0, rpb, ns));
+    IM_AF(af_vmult_enthalpy_transpose(o, dtb, t, x));
+    IM_AF(af_vmult_enthalpy_pf_transpose(o, ts, t, x));
+    IM_AF(s1_axpby(c, -1.0, ts, 1.0, Pfb, ns));
+    // dt = A^{-1} (drhs_u - A(drho2) t), with the cotangent -J_C(t)^T x
+    IM_AF(s1_inv(c, 3, s1, dtb));
+    IM_AF(s1_axpby(c, -1.0, s1, 1.0, rub, 2 * ns));
+    IM_AF(af_vmult_velocity_mass_rho_transpose(o, ts, t, s1));
+    IM_AF(s1_axpby(c, 1.0, ts, 1.0, R2, ns));
+    // the rhs triple at (rho0, u0, p0, rho2, U_i)
+    {
+      const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, Ui};
+      IM_AF(af_vmult_rhs_fused_backward(o, src, 5, zs, rub, rpb, xb));
+      IM_AF(s1_axpby(c, 1.0, xb[0], 1.0, R0, ns));
+      IM_AF(s1_axpby(c, 1.0, xb[1], 1.0, U0, 2 * ns));
+      IM_AF(s1_axpby(c, 1.0, xb[2], 1.0, P0, ns));
+      IM_AF(s1_axpby(c, 1.0, xb[3], 1.0, R2, ns));
+    }
+    // the iteration's inputs P_i, U_i: their cotangents go to the previous iterate
+    IM_AF(s1_copy(c, Pb, Pfb, ns));
+    IM_AF(s1_copy(c, Ub, xb[4], 2 * ns));
+  }
+  IM_AF(s1_axpby(c, 1.0, Pb, 1.0, P0, ns));  // P_0 = p0, U_0 = u0
+  IM_AF(s1_axpby(c, 1.0, Ub, 1.0, U0, 2 * ns));
+  // rho2 = M^{-1} R_rho(rho0, u0)
+  IM_AF(s1_inv(c, 1, rrb, R2));
+  {
+    IM_AF(s1_zero(c, tmp, 2 * ns));
+    const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, h->rec_u[0]};
+    IM_AF(af_vmult_rhs_fused_backward(o, src, 5, rrb, tmp, zs, xb));
+    IM_AF(s1_axpby(c, 1.0, xb[0], 1.0, R0, ns));
+    IM_AF(s1_axpby(c, 1.0, xb[1], 1.0, U0, 2 * ns));
+  }
+  IM_AF(s1_copy(c, rho0bar, R0, ns));
+  IM_AF(s1_copy(c, u0bar, U0, 2 * ns));
+  IM_AF(s1_copy(c, p0bar, P0, ns));
+  IM_CU(cudaStreamSynchronize(c.st));
   return AF_OK;
 }
 
@@ -443,6 +715,9 @@ int af_imex_destroy(af_imex* h) {
   if (h->op) af_synchronize(h->op);
   af_schur_solver_destroy(h->schur);
   cudaFree(h->mem);
+  cudaFree(h->adj_mem);
+  for (double* p : h->rec_p) cudaFree(p);
+  for (double* u : h->rec_u) cudaFree(u);
   af_destroy(h->op);
   delete h;
   return AF_OK;
@@ -453,6 +728,7 @@ af_operator* af_imex_operator(af_imex* h) { return h ? h->op : nullptr; }
 int af_imex_set_state(af_imex* h, const double* rho, const double* u, const double* p) {
   if (!h || !rho || !u || !p) return ierr(AF_BAD_ARG, "null argument");
   cudaStream_t st = h->op->stream;
+  h->rec_iters = 0;  // the stage-1 linearisation point is gone
   IM_CU(cudaMemcpyAsync(h->rho0, rho, h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(h->u0, u, 2 * h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(h->p0, p, h->ns * 8, cudaMemcpyDeviceToDevice, st));
@@ -473,11 +749,60 @@ int af_imex_get_state(const af_imex* h, double* rho, double* u, double* p) {
 int af_imex_step(af_imex* h, int nsteps) {
   if (!h || nsteps < 0) return ierr(AF_BAD_ARG, "bad argument");
   IM_CU(cudaSetDevice(h->op->device));
+  h->rec_iters = 0;  // the stage-1 linearisation point is gone
   for (int s = 0; s < nsteps; ++s) {
     h->stats = af_imex_stats{};
     IM_AF(one_step(h));
   }
   return af_synchronize(h->op);
+}
+
+int af_imex_stage1_forward(af_imex* h, const double* rho0, const double* u0, const double* p0, double* rho2, double* u2,
+                           double* p2) {
+  if (!h || !rho0 || !u0 || !p0 || !rho2 || !u2 || !p2) return ierr(AF_BAD_ARG, "null argument");
+  if (!h->schur) return ierr(AF_UNSUPPORTED, "af_imex_stage1_forward: needs schur_preconditioner >= 0");
+  IM_CU(cudaSetDevice(h->op->device));
+  af_operator* o = h->op;
+  const long ns = h->ns;
+  h->rec_iters = 0;
+  IM_CU(cudaMemcpyAsync(h->rho0, rho0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(h->u0, u0, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(h->p0, p0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  h->stats = af_imex_stats{};
+  // stage 1 of one_step, with the fixed-point trajectory recorded
+  IM_AF(update_density(h, 1));
+  IM_AF(set_rho_for_fixed(h, h->rho2));
+  IM_CU(cudaMemcpyAsync(h->pfix_old, h->p0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(h->ufix, h->u0, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_AF(af_set_HYPERBOLIC_stage(o, 1));
+  h->record = true;
+  const int r = fixed_point(h, 1, h->p2, h->u2);
+  h->record = false;
+  if (r != AF_OK) {
+    h->rec_iters = 0;
+    return r;
+  }
+  IM_CU(cudaMemcpyAsync(rho2, h->rho2, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(u2, h->u2, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(p2, h->p2, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaStreamSynchronize(o->stream));
+  return AF_OK;
+}
+
+int af_imex_stage1_tangent(af_imex* h, const double* drho0, const double* du0, const double* dp0, double* drho2,
+                           double* du2, double* dp2, double rel_tol) {
+  if (!h || !drho0 || !du0 || !dp0 || !drho2 || !du2 || !dp2) return ierr(AF_BAD_ARG, "null argument");
+  if (!(rel_tol > 0.0)) return ierr(AF_BAD_ARG, "af_imex_stage1_tangent: invalid tolerance");
+  IM_CU(cudaSetDevice(h->op->device));
+  return s1_tangent(h, drho0, du0, dp0, drho2, du2, dp2, rel_tol, h->opt.max_iterations);
+}
+
+int af_imex_stage1_backward(af_imex* h, const double* rho2bar, const double* u2bar, const double* p2bar,
+                            double* rho0bar, double* u0bar, double* p0bar, double rel_tol) {
+  if (!h || !rho2bar || !u2bar || !p2bar || !rho0bar || !u0bar || !p0bar) return ierr(AF_BAD_ARG, "null argument");
+  if (!(rel_tol > 0.0)) return ierr(AF_BAD_ARG, "af_imex_stage1_backward: invalid tolerance");
+  IM_CU(cudaSetDevice(h->op->device));
+  return s1_backward(h, rho2bar, u2bar, p2bar, rho0bar, u0bar, p0bar, rel_tol, h->opt.max_iterations);
 }
 
 int af_imex_last_stats(const af_imex* h, af_imex_stats* out) {

@@ -110,6 +110,12 @@ struct DegreeOps {
   cudaError_t (*res_cheb_fr)(const MeshDev&, const float* w, const float* pf, const float* din,
                              const CParamsT<float>&, const float* WM, float alpha, float s, float* r, float* dout,
                              float* x, int first, int ncell, cudaStream_t);
+  // coefficient derivatives of the implicit operators, transposed:
+  //   rhobar = (d/drho [A(rho) x])^T y;   pfbar = (d/dp_f [C(w; p_f)])^T pbar
+  cudaError_t (*op_A_rho_T)(const MeshDev&, const double* x, const double* y, double* rhobar, int ncell,
+                            cudaStream_t);
+  cudaError_t (*op_C_pf_T)(const MeshDev&, const double* w, const double* pbar, const CParams&, double* pfbar,
+                           int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

@@ -890,6 +890,17 @@ cudaError_t res_cheb_fr(const MeshDev& mesh, const float* w, const float* pf, co
   return launch_cellop<P, ResChebRPhys<float>, kFusedCB, kResChebMinB>(mesh, a, q, ncell, st);
 }
 
+cudaError_t op_A_rho_T(const MeshDev& mesh, const double* x, const double* y, double* rhobar, int ncell,
+                       cudaStream_t st) {
+  ArgPtrs<2, 1> a{{x, y}, {rhobar}};
+  return launch_cellop<P, MassRhoTPhys>(mesh, a, MassParams{1.0}, ncell, st);
+}
+cudaError_t op_C_pf_T(const MeshDev& mesh, const double* w, const double* pbar, const CParams& prm, double* pfbar,
+                      int ncell, cudaStream_t st) {
+  ArgPtrs<2, 1> a{{w, pbar}, {pfbar}};
+  return launch_cellop<P, CPfTPhys>(mesh, a, prm, ncell, st);
+}
+
 constexpr int kTransferThreads = 256;
 
 template <class R>
@@ -926,7 +937,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         cob_solve<float>,  cob_solve<double>,
                         cob_cheb<float>,   b_inv<float>,
                         res_cheb<float>,   mg_res_fr,
-                        b_inv_fr,          res_cheb_fr};
+                        b_inv_fr,          res_cheb_fr,
+                        op_A_rho_T,        op_C_pf_T};
 
 }  // namespace
 

@@ -739,4 +739,17 @@ int af_schur_solve_transpose(af_schur_solver* s, const double* p, double* x, con
   return fgmres(s, A, x, b, rel_tol, max_iterations, stats);
 }
 
+// Tangent pressure solve: J_S(p) x = b, the linearised Schur system that the tangent-linear
+// of an IMEX stage solves, with the same FGMRES and preconditioner.
+int af_schur_solve_tangent(af_schur_solver* s, const double* p, double* x, const double* b, double rel_tol,
+                           int max_iterations, af_schur_stats* stats) {
+  if (!s || !p || !x || !b) return merr(AF_BAD_ARG, "null argument");
+  if (!s->setup_done) return merr(AF_BAD_ARG, "af_schur_solver_setup first");
+  if (!(rel_tol > 0.0) || max_iterations < 1) return merr(AF_BAD_ARG, "af_schur_solve_tangent: invalid tolerance or cap");
+  af_operator* o = s->op;
+  MG_CU(cudaSetDevice(o->device));
+  auto A = [o, p](double* out, const double* in) { return af_schur_tangent(o, out, p, in); };
+  return fgmres(s, A, x, b, rel_tol, max_iterations, stats);
+}
+
 }  // extern "C"

@@ -37,6 +37,9 @@ def _bind():
     L.af_imex_get_state.argtypes = [vp, vp, vp, vp]
     L.af_imex_step.argtypes = [vp, ctypes.c_int]
     L.af_imex_last_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    L.af_imex_stage1_forward.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.af_imex_stage1_tangent.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
+    L.af_imex_stage1_backward.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
     L._imex_bound = True
     return L
 
@@ -89,6 +92,33 @@ class IMEXStepper:
 
     def step(self, n=1):
         check(_bind().af_imex_step(self._h, n))
+
+    def _triple(self):
+        import torch
+        return (torch.empty(self.n_scalar, dtype=torch.float64, device="cuda"),
+                torch.empty(2 * self.n_scalar, dtype=torch.float64, device="cuda"),
+                torch.empty(self.n_scalar, dtype=torch.float64, device="cuda"))
+
+    def stage1_forward(self, rho0, u0, p0):
+        """Stage 1 (density update and pressure fixed point) from (rho0, u0, p0), recording the
+        linearisation point of stage1_tangent / stage1_backward; returns (rho2, u2, p2)."""
+        r, u, p = self._triple()
+        check(_bind().af_imex_stage1_forward(self._h, _ptr(rho0), _ptr(u0), _ptr(p0), _ptr(r), _ptr(u), _ptr(p)))
+        return r, u, p
+
+    def stage1_tangent(self, drho0, du0, dp0, rel_tol=1e-13):
+        """(drho2, du2, dp2) = J (drho0, du0, dp0) at the last stage1_forward"""
+        r, u, p = self._triple()
+        check(_bind().af_imex_stage1_tangent(self._h, _ptr(drho0), _ptr(du0), _ptr(dp0), _ptr(r), _ptr(u), _ptr(p),
+                                             rel_tol))
+        return r, u, p
+
+    def stage1_backward(self, rho2bar, u2bar, p2bar, rel_tol=1e-13):
+        """(rho0bar, u0bar, p0bar) = J^T (rho2bar, u2bar, p2bar) at the last stage1_forward"""
+        r, u, p = self._triple()
+        check(_bind().af_imex_stage1_backward(self._h, _ptr(rho2bar), _ptr(u2bar), _ptr(p2bar), _ptr(r), _ptr(u),
+                                              _ptr(p), rel_tol))
+        return r, u, p
 
     def stats(self):
         s = Stats()

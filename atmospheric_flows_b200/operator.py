@@ -61,7 +61,8 @@ def lib():
         for name in ("af_vmult_pressure_transpose",):
             getattr(L, name).argtypes = [vp, dp, dp]
         for name in ("af_vmult_enthalpy_tangent", "af_vmult_enthalpy_transpose", "af_schur_tangent",
-                     "af_schur_transpose"):
+                     "af_schur_transpose", "af_vmult_velocity_mass_rho_transpose",
+                     "af_vmult_enthalpy_pf_transpose"):
             getattr(L, name).argtypes = [vp, dp, dp, dp]
         L.af_compute_diagnostics.argtypes = [vp, dp, dp, dp, dp, ctypes.POINTER(Diagnostics)]
         L.af_l2_norm.argtypes = [vp, ip, dp, ctypes.POINTER(ctypes.c_double)]
@@ -241,6 +242,14 @@ class EULEROperator:
     def vmult_enthalpy_transpose(self, wbar, w, pbar):
         """wbar = J_C(w)^T pbar"""
         check(lib().af_vmult_enthalpy_transpose(self._h, _ptr(wbar), _ptr(w), _ptr(pbar)))
+
+    def velocity_mass_rho_transpose(self, rhobar, x, y):
+        """rhobar = (d/drho [A(rho) x])^T y  (A = the rho_for_fixed-weighted velocity mass)"""
+        check(lib().af_vmult_velocity_mass_rho_transpose(self._h, _ptr(rhobar), _ptr(x), _ptr(y)))
+
+    def enthalpy_pf_transpose(self, pfbar, w, pbar):
+        """pfbar = (d/dp_f [C(w; p_f)])^T pbar  (C = vmult_enthalpy, p_f = pres_fixed)"""
+        check(lib().af_vmult_enthalpy_pf_transpose(self._h, _ptr(pfbar), _ptr(w), _ptr(pbar)))
 
     def schur_tangent(self, dst, p, dp):
         """dst = J_S(p) dp"""

@@ -195,6 +195,10 @@ int af_schur_solve(af_schur_solver* s, double* x, const double* b, double rel_to
  * of the Schur apply at p (see af_schur_transpose), same FGMRES and preconditioner. */
 int af_schur_solve_transpose(af_schur_solver* s, const double* p, double* x, const double* b, double rel_tol,
                              int max_iterations, af_schur_stats* stats);
+/* Tangent pressure solve (no counterpart in the reference): J_S(p) x = b, same FGMRES and
+ * preconditioner; the tangent-linear counterpart of af_schur_solve_transpose. */
+int af_schur_solve_tangent(af_schur_solver* s, const double* p, double* x, const double* b, double rel_tol,
+                           int max_iterations, af_schur_stats* stats);
 
 /* ---------------------------------------------------------------- IMEX time stepping
  * One IMEX-DG step of the reference's EulerSolver::run (Atmospheric_Flow.cc:1110-1251):
@@ -236,6 +240,23 @@ int af_imex_set_state(af_imex* h, const double* rho, const double* u, const doub
 int af_imex_get_state(const af_imex* h, double* rho, double* u, double* p);
 int af_imex_step(af_imex* h, int nsteps);
 int af_imex_last_stats(const af_imex* h, af_imex_stats* stats);
+/* Tangent-linear and adjoint of IMEX stage 1 (no counterpart in the reference): the map
+ * (rho0, u0, p0) -> (rho_tmp_2, u_tmp_2, p_tmp_2) of the density update and the pressure fixed
+ * point (Atmospheric_Flow.cc:1116-1156).
+ *   af_imex_stage1_forward:  runs stage 1 from the given state (it also becomes the handle's
+ *                            state) and records the fixed-point trajectory;
+ *   af_imex_stage1_tangent:  (drho2, du2, dp2) = J (drho0, du0, dp0);
+ *   af_imex_stage1_backward: (rho0bar, u0bar, p0bar) = J^T (rho2bar, u2bar, p2bar);
+ * J differentiates the recorded iterations, each Schur solve taken as exact (solved to
+ * rel_tol with the handle's FGMRES and preconditioner: af_schur_solve_tangent / _transpose;
+ * the cell-wise A and M solves are exact).  Needs schur_preconditioner >= 0; af_imex_step
+ * drops the recorded linearisation point.  All vectors are device arrays. */
+int af_imex_stage1_forward(af_imex* h, const double* rho0, const double* u0, const double* p0, double* rho2, double* u2,
+                           double* p2);
+int af_imex_stage1_tangent(af_imex* h, const double* drho0, const double* du0, const double* dp0, double* drho2,
+                           double* du2, double* dp2, double rel_tol);
+int af_imex_stage1_backward(af_imex* h, const double* rho2bar, const double* u2bar, const double* p2bar,
+                            double* rho0bar, double* u0bar, double* p0bar, double rel_tol);
 
 /* The Schur complement apply D p - C A^{-1} B p of af_vmult (NS_stage 2) for callers that
  * must not allocate device memory (e.g. code inside a framework whose caching allocator owns
@@ -305,6 +326,15 @@ int af_vmult_enthalpy_tangent(af_operator* op, double* dst, const double* w, con
 int af_vmult_enthalpy_transpose(af_operator* op, double* wbar, const double* w, const double* pbar);
 int af_schur_tangent(af_operator* op, double* dst, const double* p, const double* dp);
 int af_schur_transpose(af_operator* op, double* dst, const double* p, const double* pbar);
+/* Coefficient derivatives of the implicit operators, transposed (no counterpart in the
+ * reference; building blocks of the IMEX-stage adjoint).  A (NS 3/5) is linear in
+ * rho_for_fixed and C (vmult_enthalpy) in pres_fixed, so their tangents are the operators
+ * applied with the perturbation as the coefficient; the transposes are
+ *   af_vmult_velocity_mass_rho_transpose:  rhobar = (d/drho [A(rho) x])^T y = int psi (x . y)
+ *   af_vmult_enthalpy_pf_transpose:        pfbar = (d/dp_f [C(w; p_f)])^T pbar
+ * (the HYPERBOLIC_stage coefficient of C as in af_vmult_enthalpy). */
+int af_vmult_velocity_mass_rho_transpose(af_operator* op, double* rhobar, const double* x, const double* y);
+int af_vmult_enthalpy_pf_transpose(af_operator* op, double* pfbar, const double* w, const double* pbar);
 
 /* Measures the FP64 FMA throughput of the current device (TFLOP/s) with a short
  * dependent-chain kernel; the denominator of the FP64 roofline the benchmark reports.

@@ -139,6 +139,35 @@ def test_implicit_dot_products(P, name):
         assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
 
 
+@pytest.mark.parametrize("P", [2, 4])
+@pytest.mark.parametrize("name", ["hill", "hill_periodic"])
+def test_coefficient_derivative_dot_products(P, name):
+    """A is linear in rho_for_fixed and C in pres_fixed, so their coefficient tangents are the
+    operators with the perturbation as coefficient; the transposed kernels pass the
+    dot-product test against them to 1e-12."""
+    m, op, src = _implicit_setup(name, P)
+    ns = m.n_cells * (P + 1) ** 2
+    rng = np.random.default_rng(23)
+    rnd = lambda n: _d(rng.standard_normal(n))
+    x, y, drho = rnd(2 * ns), rnd(2 * ns), rnd(ns)
+    w, pbar, dpf = _d(src[1]), rnd(ns), rnd(ns)
+    rhobar = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.velocity_mass_rho_transpose(rhobar, x, y)
+    pfbar = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.enthalpy_pf_transpose(pfbar, w, pbar)
+    Ax = torch.empty(2 * ns, dtype=torch.float64, device="cuda")
+    op.set_rho_for_fixed(drho)  # A(drho) x
+    op.set_NS_stage(3)
+    op.vmult(Ax, x)
+    Cw = torch.empty(ns, dtype=torch.float64, device="cuda")
+    op.set_pres_fixed(dpf)  # C(w; dpf)
+    op.vmult_enthalpy(Cw, w)
+    torch.cuda.synchronize()
+    for lhs, rhs, scale in ((_dot(y, Ax), _dot(rhobar, drho), float((y.abs() * Ax.abs()).sum())),
+                            (_dot(pbar, Cw), _dot(pfbar, dpf), float((pbar.abs() * Cw.abs()).sum()))):
+        assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
+
+
 @pytest.mark.parametrize("P", [2, 3])
 def test_implicit_tangents_match_differences(P):
     """J_C and J_S against 5-point differences of the forward C and Schur applies (rough
