@@ -486,3 +486,202 @@ struct CPfTPhys {
 };
 
 }  // namespace af
+
+namespace af {
+
+// ------------------------------------------------------------- automatic rhs derivatives
+// Tangent-linear and adjoint of the fused rhs triple RhsPhys<STAGE, 7> for every stage, from
+// its physics evaluated with dual numbers (af_physics.cuh), so that the derivatives follow the
+// forward code exactly (quirks included).  The rhs is a sum over the policy's groups of terms
+// that depend on that group's fields only, which both policies use.
+
+// Tangent: dy = sum_G J_G dv_G.  Group G's arrays: its cell arrays, their tangents, then the
+// face-only arrays (the stage-2 kinetic-jump quirk) and their tangents.
+template <int STAGE>
+struct RhsTanPhys {
+  using Base = RhsPhys<STAGE, 7>;
+  static constexpr int NG = Base::NG;
+  static constexpr bool FACES = true, NEED_X = true, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = Base::NOUT_ARR, NOUT = Base::NOUT;
+  using Params = RhsParams;
+  using real = double;
+  static constexpr int out_ncomp(int a) { return Base::out_ncomp(a); }
+  static constexpr bool has_val(int o) { return Base::has_val(o); }
+  static constexpr bool has_grad(int o) { return Base::has_grad(o); }
+  static constexpr int narr_of(int g) { return 2 * Base::narr_of(g); }
+  static constexpr int nf_of(int g) { return 2 * Base::nf_of(g); }
+  static constexpr int nfc_of(int g) { return 2 * Base::nfc_of(g); }
+  template <int G>
+  struct Grp {
+    using BG = typename Base::template Grp<G>;
+    static constexpr int NB = BG::NARR;
+    static constexpr bool Q = Base::quirk_group(G);  // its last base array is face-only
+    static constexpr int NBC = Q ? NB - 1 : NB;
+    static constexpr int NARR = 2 * NB;
+    static constexpr bool FACE = BG::FACE;
+    static constexpr int base_of(int a) { return a < NBC ? a : (a < 2 * NBC ? a - NBC : NBC); }
+    static constexpr int ncomp(int a) { return BG::ncomp(base_of(a)); }
+    static constexpr bool face_only(int a) { return Q && a >= 2 * NBC; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo& pg, double* val,
+                                               double (*gr)[2]) {
+    constexpr int NFC = Base::nfc_of(G), NF = Base::nf_of(G);
+    Dual vb[NF], fv[NOUT], fg[NOUT][2];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) vb[k] = k < NFC ? Dual{v[k], v[NFC + k]} : Dual{0.0, 0.0};
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) fv[o] = fg[o][0] = fg[o][1] = Dual{0.0, 0.0};
+    Base::template point_t<G, Dual>(prm, vb, pg, fv, fg);
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      val[o] += fv[o].d;
+      gr[o][0] += fg[o][0].d;
+      gr[o][1] += fg[o][1].d;
+    }
+  }
+  template <int G>
+  __device__ __forceinline__ static void load_face(const double* w, Dual* out) {
+    constexpr int NFC = Base::nfc_of(G), NF = Base::nf_of(G), NFO = NF - NFC;
+#pragma unroll
+    for (int k = 0; k < NF; ++k)
+      out[k] = k < NFC ? Dual{w[k], w[NFC + k]} : Dual{w[2 * NFC + (k - NFC)], w[2 * NFC + NFO + (k - NFC)]};
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm, const double* n,
+                                              double* flux) {
+    constexpr int NF = Base::nf_of(G);
+    Dual a[NF], b[NF], fl[NOUT];
+    load_face<G>(vp, a);
+    load_face<G>(vm, b);
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) fl[o] = Dual{0.0, 0.0};
+    Base::template face_t<G, Dual>(prm, a, b, n, fl);
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) flux[o] = fl[o].d;
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
+                                                  double* flux) {
+    constexpr int NF = Base::nf_of(G);
+    Dual a[NF], fl[NOUT];
+    load_face<G>(vp, a);
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) fl[o] = Dual{0.0, 0.0};
+    Base::template boundary_t<G, Dual>(prm, a, n, fl);
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) flux[o] = fl[o].d;
+  }
+};
+
+// Adjoint of group GB of RhsPhys<STAGE, 7>: xbar_GB = J_GB^T ybar, one launch per group.
+// Arrays: the group's cell arrays, the cotangents ybar_rho, ybar_u (2), ybar_p (gradient
+// fields), then the group's face-only array (quirk).  Outputs: xbar of the group's arrays.
+//   cell:     xbar_s = sum_o [ybar_o df_o/dv_s + grad(ybar_o) . dg_o/dv_s]   (tested with phi)
+//   faces:    xbar_s += sum_o dF_o/dv+_s (ybar_o+ - ybar_o-)   (the flux is antisymmetric under
+//             a side swap, so the neighbour's term supplies the minus side)
+//   boundary: xbar_s += sum_o dF_o/dv+_s ybar_o+
+// Each derivative is one dual evaluation seeded in field s.
+template <int STAGE, int GB>
+struct RhsAdjGPhys {
+  using Base = RhsPhys<STAGE, 7>;
+  using BG = typename Base::template Grp<GB>;
+  static constexpr int NFb = Base::nf_of(GB), NFCb = Base::nfc_of(GB), NFOb = NFb - NFCb;
+  static constexpr int NB = BG::NARR;
+  static constexpr bool Q = Base::quirk_group(GB);
+  static constexpr int NBC = Q ? NB - 1 : NB;
+  static constexpr int NG = 1;
+  static constexpr bool FACES = BG::FACE, NEED_X = true, ACCUMULATE = false;
+  static constexpr int NOUT_ARR = NB, NOUT = NFb;
+  static constexpr int NY = Base::NOUT;  // cotangent components: rho, u (2), p
+  using Params = RhsParams;
+  using real = double;
+  static constexpr int out_ncomp(int a) { return BG::ncomp(a); }
+  static constexpr bool has_val(int) { return true; }
+  static constexpr bool has_grad(int) { return false; }
+  static constexpr int narr_of(int) { return NB + 3; }
+  static constexpr int nf_of(int) { return NFb + NY; }
+  static constexpr int nfc_of(int) { return NFCb + NY; }
+  static constexpr int nfg_of(int) { return NY; }
+  template <int G>
+  struct Grp {
+    static constexpr int NARR = NB + 3;
+    static constexpr bool FACE = BG::FACE;
+    static constexpr int ncomp(int a) {
+      return a < NBC ? BG::ncomp(a) : (a < NBC + 3 ? (a == NBC + 1 ? 2 : 1) : BG::ncomp(NBC));
+    }
+    static constexpr bool face_only(int a) { return Q && a == NBC + 3; }
+  };
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const double* deta,
+                                               const PointGeo& pg, double* val, double (*)[2]) {
+    const double J00 = pg.J[0], J01 = pg.J[1], J10 = pg.J[2], J11 = pg.J[3];
+    const double idet = 1.0 / (J00 * J11 - J01 * J10);
+    double y[NY], gy[NY][2];
+#pragma unroll
+    for (int o = 0; o < NY; ++o) {
+      y[o] = v[NFCb + o];
+      const double dx = v[NFCb + NY + o], de = deta[o];  // d/dxi slots follow the cell fields
+      gy[o][0] = (J11 * dx - J10 * de) * idet;
+      gy[o][1] = (J00 * de - J01 * dx) * idet;
+    }
+#pragma unroll
+    for (int s = 0; s < NFCb; ++s) {
+      Dual vb[NFb], fv[NY], fg[NY][2];
+#pragma unroll
+      for (int k = 0; k < NFb; ++k) vb[k] = Dual{k < NFCb ? v[k] : 0.0, k == s ? 1.0 : 0.0};
+#pragma unroll
+      for (int o = 0; o < NY; ++o) fv[o] = fg[o][0] = fg[o][1] = Dual{0.0, 0.0};
+      Base::template point_t<GB, Dual>(prm, vb, pg, fv, fg);
+      double acc = 0.0;
+#pragma unroll
+      for (int o = 0; o < NY; ++o) acc += y[o] * fv[o].d + gy[o][0] * fg[o][0].d + gy[o][1] * fg[o][1].d;
+      val[s] += acc;
+    }
+  }
+  __device__ __forceinline__ static double field(const double* w, int k) {
+    return k < NFCb ? w[k] : w[NFCb + NY + (k - NFCb)];
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm, const double* n,
+                                              double* flux) {
+    double dy[NY];
+#pragma unroll
+    for (int o = 0; o < NY; ++o) dy[o] = vp[NFCb + o] - vm[NFCb + o];
+#pragma unroll
+    for (int s = 0; s < NFb; ++s) {
+      Dual a[NFb], b[NFb], fl[NY];
+#pragma unroll
+      for (int k = 0; k < NFb; ++k) {
+        a[k] = Dual{field(vp, k), k == s ? 1.0 : 0.0};
+        b[k] = Dual{field(vm, k), 0.0};
+      }
+#pragma unroll
+      for (int o = 0; o < NY; ++o) fl[o] = Dual{0.0, 0.0};
+      Base::template face_t<GB, Dual>(prm, a, b, n, fl);
+      double acc = 0.0;
+#pragma unroll
+      for (int o = 0; o < NY; ++o) acc += fl[o].d * dy[o];
+      flux[s] = acc;
+    }
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
+                                                  double* flux) {
+#pragma unroll
+    for (int s = 0; s < NFb; ++s) {
+      Dual a[NFb], fl[NY];
+#pragma unroll
+      for (int k = 0; k < NFb; ++k) a[k] = Dual{field(vp, k), k == s ? 1.0 : 0.0};
+#pragma unroll
+      for (int o = 0; o < NY; ++o) fl[o] = Dual{0.0, 0.0};
+      Base::template boundary_t<GB, Dual>(prm, a, n, fl);
+      double acc = 0.0;
+#pragma unroll
+      for (int o = 0; o < NY; ++o) acc += fl[o].d * vp[NFCb + o];
+      flux[s] = acc;
+    }
+  }
+};
+
+}  // namespace af

@@ -318,32 +318,43 @@ int af_vmult_rhs_fused(af_operator* o, double* d_rho, double* d_u, double* d_p, 
   return rhs_fused_range(o, d_rho, d_u, d_p, src, n, 0, -1);
 }
 
+// Stage 1: the hand-written adjoint / tangent kernels (RhsAdj1Phys, RhsTlm1Phys); stages 2 and
+// 3: the dual-number kernels (RhsAdjGPhys per group, RhsTanPhys), which differentiate the
+// forward physics itself.
 int af_vmult_rhs_fused_backward(af_operator* o, const double* const* src, int n, const double* ybar_rho,
                                 const double* ybar_u, const double* ybar_p, double* const* xbar) {
   if (!o || !src || !xbar || !ybar_rho || !ybar_u || !ybar_p) return fail(AF_BAD_ARG, "null argument");
-  if (o->hs != 1) return fail(AF_UNSUPPORTED, "af_vmult_rhs_fused_backward: HYPERBOLIC_stage 1 only");
-  if (n != 5) return fail(AF_BAD_ARG, "af_vmult_rhs_fused_backward: stage 1 expects 5 sources");
-  for (int k = 0; k < 5; ++k)
+  const int need = 3 * o->hs + 2;
+  if (n != need) return fail(AF_BAD_ARG, "af_vmult_rhs_fused_backward: stage %d expects %d sources", o->hs, need);
+  for (int k = 0; k < n; ++k)
     if (!src[k] || !xbar[k] || !aligned16(src[k]) || !aligned16(xbar[k]))
       return fail(AF_BAD_ARG, "af_vmult_rhs_fused_backward: null or unaligned vector");
   AF_CU(cudaSetDevice(o->device));
   const double* yb[3] = {ybar_rho, ybar_u, ybar_p};
-  AF_CU(o->ops->rhs_adjoint1(o->mesh, src, yb, xbar, rhs_params(o, 1), o->ncell, o->stream));
-  o->launches += 1;
+  if (o->hs == 1) {
+    AF_CU(o->ops->rhs_adjoint1(o->mesh, src, yb, xbar, rhs_params(o, 1), o->ncell, o->stream));
+    o->launches += 1;
+  } else {
+    AF_CU(o->ops->rhs_adjoint(o->mesh, o->hs, src, yb, xbar, o->d_ws, rhs_params(o, o->hs), o->ncell, o->stream));
+    o->launches += o->hs + 2;
+  }
   return AF_OK;
 }
 
 int af_vmult_rhs_fused_tangent(af_operator* o, const double* const* src, int n, const double* const* dsrc,
                                double* d_rho, double* d_u, double* d_p) {
   if (!o || !src || !dsrc || !d_rho || !d_u || !d_p) return fail(AF_BAD_ARG, "null argument");
-  if (o->hs != 1) return fail(AF_UNSUPPORTED, "af_vmult_rhs_fused_tangent: HYPERBOLIC_stage 1 only");
-  if (n != 5) return fail(AF_BAD_ARG, "af_vmult_rhs_fused_tangent: stage 1 expects 5 sources");
-  for (int k = 0; k < 5; ++k)
+  const int need = 3 * o->hs + 2;
+  if (n != need) return fail(AF_BAD_ARG, "af_vmult_rhs_fused_tangent: stage %d expects %d sources", o->hs, need);
+  for (int k = 0; k < n; ++k)
     if (!src[k] || !dsrc[k] || !aligned16(src[k]) || !aligned16(dsrc[k]))
       return fail(AF_BAD_ARG, "af_vmult_rhs_fused_tangent: null or unaligned vector");
   AF_CU(cudaSetDevice(o->device));
   double* dy[3] = {d_rho, d_u, d_p};
-  AF_CU(o->ops->rhs_tangent1(o->mesh, src, dsrc, dy, rhs_params(o, 1), o->ncell, o->stream));
+  if (o->hs == 1)
+    AF_CU(o->ops->rhs_tangent1(o->mesh, src, dsrc, dy, rhs_params(o, 1), o->ncell, o->stream));
+  else
+    AF_CU(o->ops->rhs_tangent(o->mesh, o->hs, src, dsrc, dy, rhs_params(o, o->hs), o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
 }

@@ -116,6 +116,13 @@ struct DegreeOps {
                             cudaStream_t);
   cudaError_t (*op_C_pf_T)(const MeshDev&, const double* w, const double* pbar, const CParams&, double* pfbar,
                            int ncell, cudaStream_t);
+  // tangent and adjoint of the fused rhs triple of any stage (dual-number evaluation of the
+  // same physics); vectors in the fused order rho_j, u_j, p_j (explicit stages), rho_c,
+  // u_fixed; dy / ybar = rho, u, p; scratch: one velocity-sized vector (stage 2)
+  cudaError_t (*rhs_tangent)(const MeshDev&, int stage, const double* const* in, const double* const* din,
+                             double* const* dy, const RhsParams&, int ncell, cudaStream_t);
+  cudaError_t (*rhs_adjoint)(const MeshDev&, int stage, const double* const* in, const double* const* ybar,
+                             double* const* xbar, double* scratch, const RhsParams&, int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

@@ -675,6 +675,106 @@ cudaError_t rhs_tangent1(const MeshDev& mesh, const double* const* in, const dou
   return launch_cellop<P, RhsTlm1Phys, kAdjCells, 2>(mesh, a, prm, ncell, st);
 }
 
+// ---- automatic tangents and adjoints of the fused rhs triple of any stage (dual numbers).
+// Vectors in the fused order: rho_j, u_j, p_j for each explicit stage j, then rho_c, u_fixed.
+template <int STAGE>
+cudaError_t rhs_tangent_s(const MeshDev& mesh, const double* const* in, const double* const* din, double* const* dy,
+                          const RhsParams& prm, int ncell, cudaStream_t st) {
+  using Ph = RhsTanPhys<STAGE>;
+  using B = RhsPhys<STAGE, 7>;
+  ArgPtrs<PhysInfo<Ph>::NARR_TOTAL, 3> a{};
+  int k = 0;
+  for (int j = 0; j < STAGE; ++j) {
+    for (int c = 0; c < 3; ++c) a.in[k++] = in[3 * j + c];
+    for (int c = 0; c < 3; ++c) a.in[k++] = din[3 * j + c];
+    if (B::quirk_group(j)) {  // u_old of the stage-2 kinetic jump
+      a.in[k++] = in[1];
+      a.in[k++] = din[1];
+    }
+  }
+  a.in[k++] = in[3 * STAGE];
+  a.in[k++] = in[3 * STAGE + 1];
+  a.in[k++] = din[3 * STAGE];
+  a.in[k++] = din[3 * STAGE + 1];
+  a.out[0] = dy[0];
+  a.out[1] = dy[1];
+  a.out[2] = dy[2];
+  for (int i = 0; i < k; ++i)
+    if (!a.in[i]) return cudaErrorInvalidValue;
+  return launch_cellop<P, Ph, kAdjCells, 2>(mesh, a, prm, ncell, st);
+}
+
+template <int STAGE, int G>
+cudaError_t rhs_adj_group(const MeshDev& mesh, const double* const* in, const double* const* ybar, double* const* xbar,
+                          double* scratch, const RhsParams& prm, int ncell, cudaStream_t st) {
+  using Ph = RhsAdjGPhys<STAGE, G>;
+  ArgPtrs<Ph::NB + 3, Ph::NB> a{};
+  const int base = 3 * G;  // the group's first vector in the fused order (implicit group: 3 STAGE)
+  for (int i = 0; i < Ph::NBC; ++i) {
+    a.in[i] = in[base + i];
+    a.out[i] = xbar[base + i];
+  }
+  a.in[Ph::NBC] = ybar[0];
+  a.in[Ph::NBC + 1] = ybar[1];
+  a.in[Ph::NBC + 2] = ybar[2];
+  if constexpr (Ph::Q) {  // u_old: its cotangent goes to scratch, added to u_0's by the caller
+    a.in[Ph::NBC + 3] = in[1];
+    a.out[Ph::NBC] = scratch;
+  }
+  return launch_cellop<P, Ph, kAdjCells, 2>(mesh, a, prm, ncell, st);
+}
+
+__global__ void k_add(const double* __restrict__ x, double* __restrict__ y, const long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
+}
+
+// host-side compile-time loop (sfor is device-only)
+template <class F, int... I>
+void host_for_impl(F& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+void host_for(F&& f) {
+  host_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+template <int STAGE>
+cudaError_t rhs_adjoint_s(const MeshDev& mesh, const double* const* in, const double* const* ybar, double* const* xbar,
+                          double* scratch, const RhsParams& prm, int ncell, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  host_for<STAGE + 1>([&](auto gc) {
+    constexpr int G = decltype(gc)::value;
+    if (e == cudaSuccess) e = rhs_adj_group<STAGE, G>(mesh, in, ybar, xbar, scratch, prm, ncell, st);
+  });
+  if (e != cudaSuccess) return e;
+  if constexpr (RhsPhys<STAGE, 7>::quirk_group(1)) {
+    const long n = 2L * ncell * kND;
+    k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(scratch, xbar[1], n);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+cudaError_t rhs_tangent(const MeshDev& mesh, int stage, const double* const* in, const double* const* din,
+                        double* const* dy, const RhsParams& prm, int ncell, cudaStream_t st) {
+  switch (stage) {
+    case 1: return rhs_tangent_s<1>(mesh, in, din, dy, prm, ncell, st);
+    case 2: return rhs_tangent_s<2>(mesh, in, din, dy, prm, ncell, st);
+    case 3: return rhs_tangent_s<3>(mesh, in, din, dy, prm, ncell, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+cudaError_t rhs_adjoint(const MeshDev& mesh, int stage, const double* const* in, const double* const* ybar,
+                        double* const* xbar, double* scratch, const RhsParams& prm, int ncell, cudaStream_t st) {
+  switch (stage) {
+    case 1: return rhs_adjoint_s<1>(mesh, in, ybar, xbar, scratch, prm, ncell, st);
+    case 2: return rhs_adjoint_s<2>(mesh, in, ybar, xbar, scratch, prm, ncell, st);
+    case 3: return rhs_adjoint_s<3>(mesh, in, ybar, xbar, scratch, prm, ncell, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t op_BT(const MeshDev& mesh, const double* ubar, double c, double* pbar, int ncell, cudaStream_t st) {
   ArgPtrs<1, 1> a{{ubar}, {pbar}};
   return launch_cellop<P, BTPhys>(mesh, a, BParams{c}, ncell, st);
@@ -938,7 +1038,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         cob_cheb<float>,   b_inv<float>,
                         res_cheb<float>,   mg_res_fr,
                         b_inv_fr,          res_cheb_fr,
-                        op_A_rho_T,        op_C_pf_T};
+                        op_A_rho_T,        op_C_pf_T,
+                        rhs_tangent,       rhs_adjoint};
 
 }  // namespace
 

@@ -48,6 +48,31 @@ __device__ __forceinline__ void gravity_dir(const RhsParams& prm, const PointGeo
   }
 }
 
+// Forward-mode dual number (value, one directional derivative) for the automatic tangents and
+// adjoints of the rhs policies: the rhs physics below is written once for a scalar type T and
+// evaluated with T = double (the operator) or T = Dual (its derivatives).  |x| and max(a, b)
+// follow the branch of the value (at max(a, b) the first argument when a >= b), which is the
+// frozen-branch derivative of the Rusanov wave speed.
+struct Dual {
+  double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, fma(a.v, b.d, a.d * b.v)}; }
+__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+__device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__device__ __forceinline__ Dual& operator+=(Dual& a, Dual b) { a.v += b.v; a.d += b.d; return a; }
+__device__ __forceinline__ Dual& operator-=(Dual& a, Dual b) { a.v -= b.v; a.d -= b.d; return a; }
+__device__ __forceinline__ double aabs(double x) { return fabs(x); }
+__device__ __forceinline__ double amax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ Dual aabs(Dual x) { return x.v > 0.0 ? x : (x.v < 0.0 ? -x : Dual{0.0, 0.0}); }
+__device__ __forceinline__ Dual amax(Dual a, Dual b) { return a.v >= b.v ? a : b; }
+
 template <int STAGE, int MASK>
 struct RhsPhys {
   static constexpr bool RHO = (MASK & 1) != 0, VEL = (MASK & 2) != 0, PRES = (MASK & 4) != 0;
@@ -88,13 +113,13 @@ struct RhsPhys {
     static constexpr bool face_only(int a) { return EXPL && a == 3; }
   };
 
-  template <int G>
-  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo& pg,
-                                               double* val, double (*gr)[2]) {
+  template <int G, class T>
+  __device__ __forceinline__ static void point_t(const Params& prm, const T* v, const PointGeo& pg, T* val,
+                                                 T (*gr)[2]) {
     double e0, e1, fac;
     gravity_dir(prm, pg, e0, e1, fac);
     if constexpr (G < STAGE) {
-      const double rho = v[0], ux = v[1], uz = v[2];
+      const T rho = v[0], ux = v[1], uz = v[2];
       const double ca = prm.ca[G] * prm.dt, cg = prm.cg[G] * prm.dt;
       if constexpr (RHO) {  // euler_operator.h:378-380 (and stage 2/3 analogues)
         if (G == 0) val[O_RHO] += rho;
@@ -102,83 +127,83 @@ struct RhsPhys {
         gr[O_RHO][1] += ca * rho * uz;
       }
       if constexpr (VEL || PRES) {
-        const double p = v[3];
+        const T p = v[3];
         const double ct = prm.ct[G] * prm.dt;
         if constexpr (VEL) {  // :1686-1691
           if (G == 0) { val[O_U] += rho * ux; val[O_U + 1] += rho * uz; }
-          const double gfac = cg * prm.invFr2 * rho * fac;
+          const T gfac = cg * prm.invFr2 * rho * fac;
           val[O_U] -= gfac * e0;
           val[O_U + 1] -= gfac * e1;
-          const double cr = ca * rho, pt = ct * prm.invMa2 * p;
+          const T cr = ca * rho, pt = ct * prm.invMa2 * p;
           gr[O_U][0] += cr * ux * ux + pt;
           gr[O_U][1] += cr * ux * uz;
           gr[O_U + 1][0] += cr * uz * ux;
           gr[O_U + 1][1] += cr * uz * uz + pt;
         }
         if constexpr (PRES) {  // :806-813: rho E = p/(g-1) + Ma^2 rho |u|^2 / 2
-          const double uu = ux * ux + uz * uz;
+          const T uu = ux * ux + uz * uz;
           if (G == 0) val[O_P] += p * prm.g1 + 0.5 * prm.Ma2 * rho * uu;
           val[O_P] -= cg * prm.Ma2Fr2 * rho * (ux * e0 + uz * e1) * fac;
-          const double s = 0.5 * ca * prm.Ma2 * uu * rho + ct * prm.gg * p;
+          const T s = 0.5 * ca * prm.Ma2 * uu * rho + ct * prm.gg * p;
           gr[O_P][0] += s * ux;
           gr[O_P][1] += s * uz;
         }
       }
     } else {
-      const double rc = v[0];
+      const T rc = v[0];
       const double cgI = prm.cgI * prm.dt;
       if constexpr (VEL && STAGE < 3) {
-        const double gfac = cgI * prm.invFr2 * rc * fac;
+        const T gfac = cgI * prm.invFr2 * rc * fac;
         val[O_U] -= gfac * e0;
         val[O_U + 1] -= gfac * e1;
       }
       if constexpr (PRES) {
-        const double fx = v[1], fz = v[2];
+        const T fx = v[1], fz = v[2];
         val[O_P] -= 0.5 * rc * prm.Ma2 * (fx * fx + fz * fz);
         if (STAGE < 3) val[O_P] -= cgI * prm.Ma2Fr2 * rc * (fx * e0 + fz * e1) * fac;
       }
     }
   }
 
-  template <int G>
-  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
-                                              const double* n, double* flux) {
+  template <int G, class T>
+  __device__ __forceinline__ static void face_t(const Params& prm, const T* vp, const T* vm, const double* n,
+                                                T* flux) {
     if constexpr (G < STAGE) {
-      const double rp = vp[0], upx = vp[1], upz = vp[2];
-      const double rm = vm[0], umx = vm[1], umz = vm[2];
-      const double unp = upx * n[0] + upz * n[1], unm = umx * n[0] + umz * n[1];
-      const double lam = fmax(fabs(unp), fabs(unm));
+      const T rp = vp[0], upx = vp[1], upz = vp[2];
+      const T rm = vm[0], umx = vm[1], umz = vm[2];
+      const T unp = upx * n[0] + upz * n[1], unm = umx * n[0] + umz * n[1];
+      const T lam = amax(aabs(unp), aabs(unm));
       const double ca = prm.ca[G] * prm.dt;
       if constexpr (RHO) {  // :519-526
-        const double F = ca * (0.5 * (rp * unp + rm * unm) + 0.5 * lam * (rp - rm));
+        const T F = ca * (0.5 * (rp * unp + rm * unm) + 0.5 * lam * (rp - rm));
         flux[O_RHO] = -F;
       }
       if constexpr (VEL || PRES) {
-        const double pp = vp[3], pm = vm[3];
+        const T pp = vp[3], pm = vm[3];
         const double ct = prm.ct[G] * prm.dt;
         if constexpr (VEL) {  // :1938-1950
-          const double pa = ct * prm.invMa2 * 0.5 * (pp + pm);
-          const double Fx = ca * 0.5 * (rp * upx * unp + rm * umx * unm) + pa * n[0] + ca * 0.5 * lam * (rp * upx - rm * umx);
-          const double Fz = ca * 0.5 * (rp * upz * unp + rm * umz * unm) + pa * n[1] + ca * 0.5 * lam * (rp * upz - rm * umz);
+          const T pa = ct * prm.invMa2 * 0.5 * (pp + pm);
+          const T Fx = ca * 0.5 * (rp * upx * unp + rm * umx * unm) + pa * n[0] + ca * 0.5 * lam * (rp * upx - rm * umx);
+          const T Fz = ca * 0.5 * (rp * upz * unp + rm * umz * unm) + pa * n[1] + ca * 0.5 * lam * (rp * upz - rm * umz);
           flux[O_U] = -Fx;
           flux[O_U + 1] = -Fz;
         }
         if constexpr (PRES) {  // :1057-1079 (stage 1), :1141-1194 (2), :1275-1355 (3)
-          const double uup = upx * upx + upz * upz, uum = umx * umx + umz * umz;
-          const double kin = 0.5 * (0.5 * uup * rp * unp + 0.5 * uum * rm * unm);
-          const double ent = 0.5 * prm.gg * (pp * unp + pm * unm);
-          double F;
+          const T uup = upx * upx + upz * upz, uum = umx * umx + umz * umz;
+          const T kin = 0.5 * (0.5 * uup * rp * unp + 0.5 * uum * rm * unm);
+          const T ent = 0.5 * prm.gg * (pp * unp + pm * unm);
+          T F;
           if constexpr (STAGE < 3) {
-            double jk;
+            T jk;
             if constexpr (quirk_group(G)) {  // :1182-1183 uses u_tmp_2 . u_old
               jk = rp * 0.5 * (upx * vp[4] + upz * vp[5]) - rm * 0.5 * (umx * vm[4] + umz * vm[5]);
             } else {
               jk = rp * 0.5 * uup - rm * 0.5 * uum;
             }
-            const double je = prm.g1 * (pp - pm);
+            const T je = prm.g1 * (pp - pm);
             F = ca * prm.Ma2 * (kin + 0.5 * lam * jk) + ct * (ent + 0.5 * lam * je);
           } else {
-            const double jE = prm.g1 * (pp - pm) + 0.5 * prm.Ma2 * (rp * uup - rm * uum);
+            const T jE = prm.g1 * (pp - pm) + 0.5 * prm.Ma2 * (rp * uup - rm * uum);
             F = ca * prm.Ma2 * kin + ca * ent + ca * 0.5 * lam * jE;
           }
           flux[O_P] = -F;
@@ -187,15 +212,29 @@ struct RhsPhys {
     }
   }
 
-  template <int G>
-  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
-                                                  double* flux) {
+  template <int G, class T>
+  __device__ __forceinline__ static void boundary_t(const Params& prm, const T* vp, const double* n, T* flux) {
     if constexpr (G < STAGE && VEL) {  // :2189-2305, p_D = p
-      const double pp = vp[3];
-      const double s = prm.ct[G] * prm.dt * prm.invMa2 * (0.5 * (pp + pp));
+      const T pp = vp[3];
+      const T s = prm.ct[G] * prm.dt * prm.invMa2 * (0.5 * (pp + pp));
       flux[O_U] = -s * n[0];
       flux[O_U + 1] = -s * n[1];
     }
+  }
+  template <int G>
+  __device__ __forceinline__ static void point(const Params& prm, const double* v, const PointGeo& pg,
+                                               double* val, double (*gr)[2]) {
+    point_t<G, double>(prm, v, pg, val, gr);
+  }
+  template <int G>
+  __device__ __forceinline__ static void face(const Params& prm, const double* vp, const double* vm,
+                                              const double* n, double* flux) {
+    face_t<G, double>(prm, vp, vm, n, flux);
+  }
+  template <int G>
+  __device__ __forceinline__ static void boundary(const Params& prm, const double* vp, const double* n,
+                                                  double* flux) {
+    boundary_t<G, double>(prm, vp, n, flux);
   }
 };
 

@@ -204,7 +204,7 @@ class EULEROperator:
 
     # --- forward / backward pair of the fused stage-1 rhs (autograd-style) ---
     def vmult_rhs_fused_backward(self, src, ybar_rho, ybar_u, ybar_p, xbar):
-        """xbar[k] = (d rhs / d src[k])^T ybar for the five stage-1 sources (overwritten)."""
+        """xbar[k] = (d rhs / d src[k])^T ybar for the sources of the current stage (overwritten)."""
         check(lib().af_vmult_rhs_fused_backward(self._h, _ptr_array(src), len(src), _ptr(ybar_rho), _ptr(ybar_u),
                                                 _ptr(ybar_p), _ptr_array(xbar)))
 

@@ -92,18 +92,19 @@ int af_vmult_rhs_fused(af_operator* op, double* dst_rho, double* dst_u, double* 
  * call a deal.II host-vector caller makes. */
 int af_vmult_rhs_fused_host(af_operator* op, double* dst_rho, double* dst_u, double* dst_p,
                             const double* const* src, int n_src);
-/* Backward (vector-Jacobian product) of af_vmult_rhs_fused at HYPERBOLIC_stage 1, the role
- * of a torch.autograd.Function's backward for the forward above (no counterpart in the
- * reference): src = {rho_old, u_old, pres_old, rho_tmp_2, u_fixed} as for the forward, ybar_*
- * = cotangents of its rho, u, p outputs, xbar[5] receives the cotangents of the five sources
- * (overwritten).  Hand-written adjoint kernel: transposed sum factorisation of the cell
- * terms, and the own-side flux Jacobian applied to the cotangent jump on faces, with the
- * Rusanov wave-speed branch frozen as taken by the forward pass.  AF_UNSUPPORTED at stages 2, 3. */
+/* Backward (vector-Jacobian product) of af_vmult_rhs_fused, the role of a
+ * torch.autograd.Function's backward for the forward above (no counterpart in the
+ * reference): src as for the forward (3 HYPERBOLIC_stage + 2 vectors), ybar_* = cotangents of
+ * its rho, u, p outputs, xbar[n] receives the cotangents of the sources (overwritten).
+ * Stage 1: a hand-written adjoint kernel (transposed sum factorisation of the cell terms, the
+ * own-side flux Jacobian applied to the cotangent jump on faces, the Rusanov wave-speed branch
+ * frozen as taken by the forward pass).  Stages 2 and 3: one dual-number kernel per group of
+ * sources, differentiating the forward physics with the same frozen branch. */
 int af_vmult_rhs_fused_backward(af_operator* op, const double* const* src, int n, const double* ybar_rho,
                                 const double* ybar_u, const double* ybar_p, double* const* xbar);
 /* Tangent-linear of the same forward (no counterpart in the reference): dy = J(src) dsrc, with
- * dsrc[5] directions of the five sources and the wave-speed branch frozen as in the backward,
- * so that <ybar, tangent(dsrc)> = <backward(ybar), dsrc> to rounding. */
+ * dsrc[n] directions of the sources and the wave-speed branch frozen as in the backward, so
+ * that <ybar, tangent(dsrc)> = <backward(ybar), dsrc> to rounding (any stage). */
 int af_vmult_rhs_fused_tangent(af_operator* op, const double* const* src, int n, const double* const* dsrc,
                                double* d_rho, double* d_u, double* d_p);
 

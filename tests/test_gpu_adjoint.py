@@ -228,3 +228,68 @@ def test_adjoint_pressure_solve(pc):
     op.schur_tangent(Jp, p, p)
     torch.cuda.synchronize()
     assert float(torch.linalg.norm(Jp - Sp) / torch.linalg.norm(Sp)) < 1e-12
+
+
+def _stage_sources(m, P, stage, rough):
+    """The fused rhs sources of a stage: rho, u, p of each explicit stage, then rho_c, u_fixed."""
+    mk = (lambda k: M.random_state(m, P, seed=40 + k)) if rough else (lambda k: M.hill_state(m, P, seed=40 + k,
+                                                                                               amplitude=0.05))
+    st = [mk(k) for k in range(stage + 1)]
+    src = []
+    for j in range(stage):
+        src += [st[j].rho, st[j].u, st[j].p]
+    return src + [st[stage].rho, st[stage].u]
+
+
+@pytest.mark.parametrize("P", [2, 3])
+@pytest.mark.parametrize("stage", [2, 3])
+@pytest.mark.parametrize("name,rough", [("hill", True), ("hill_periodic", False), ("annulus", True)])
+def test_dot_product_stages_2_3(P, stage, name, rough):
+    """Stages 2 and 3 (dual-number kernels): <ybar, J dx> = <J^T ybar, dx> to 1e-12."""
+    from atmospheric_flows_b200.operator import EULEROperator
+    m, Ma, Fr, _ = _case(name, P, rough)
+    src = _stage_sources(m, P, stage, rough or name == "annulus")
+    op = EULEROperator(m, P, Ma, Fr, 2.0)
+    op.set_HYPERBOLIC_stage(stage)
+    ns = m.n_cells * (P + 1) ** 2
+    rng = np.random.default_rng(9)
+    dx = [rng.standard_normal(a.size) for a in src]
+    yb = [rng.standard_normal(n) for n in (ns, 2 * ns, ns)]
+    s = [_d(a) for a in src]
+    dy = [torch.empty(n, dtype=torch.float64, device="cuda") for n in (ns, 2 * ns, ns)]
+    op.vmult_rhs_fused_tangent(s, [_d(a) for a in dx], *dy)
+    xb = [torch.full((a.size,), np.nan, dtype=torch.float64, device="cuda") for a in src]
+    op.vmult_rhs_fused_backward(s, *[_d(a) for a in yb], xb)
+    torch.cuda.synchronize()
+    lhs = sum(float(np.dot(a, b.cpu().numpy())) for a, b in zip(yb, dy))
+    terms = [float(np.dot(b.cpu().numpy(), a)) for a, b in zip(dx, xb)]
+    assert abs(lhs - sum(terms)) <= 1e-12 * sum(abs(t) for t in terms), (lhs, sum(terms))
+
+
+@pytest.mark.parametrize("stage", [1, 2, 3])
+def test_tangent_matches_forward_differences(stage):
+    """The tangent (hand-written at stage 1, dual numbers at 2 and 3) against central differences
+    of the forward rhs on a rough state (face traces differ, so no wave-speed branch flips
+    within the step): 1e-7 relative."""
+    from atmospheric_flows_b200.operator import EULEROperator
+    P = 3
+    m, Ma, Fr, _ = _case("hill", P, True)
+    src = _stage_sources(m, P, stage, True)
+    op = EULEROperator(m, P, Ma, Fr, 2.0)
+    op.set_HYPERBOLIC_stage(stage)
+    ns = m.n_cells * (P + 1) ** 2
+    rng = np.random.default_rng(13)
+    dx = [1e-2 * np.abs(a).max() * rng.standard_normal(a.size) for a in src]
+    dy = [torch.empty(n, dtype=torch.float64, device="cuda") for n in (ns, 2 * ns, ns)]
+    op.vmult_rhs_fused_tangent([_d(a) for a in src], [_d(a) for a in dx], *dy)
+
+    def fwd(sign, h):
+        out = [torch.empty(n, dtype=torch.float64, device="cuda") for n in (ns, 2 * ns, ns)]
+        op.vmult_rhs_fused(*out, [_d(a + sign * h * b) for a, b in zip(src, dx)])
+        return out
+    h = 1e-4
+    yp, ym = fwd(1, h), fwd(-1, h)
+    torch.cuda.synchronize()
+    for a, b, t in zip(yp, ym, dy):
+        err = float(torch.linalg.norm((a - b) / (2 * h) - t) / torch.linalg.norm(t))
+        assert err < 1e-7, (stage, err)
