@@ -17,6 +17,7 @@
 // systems and tolerances are the same, so the solutions agree to the solver tolerance.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -48,11 +49,13 @@ struct af_imex {
   KrylovState* kst;
   af_schur_solver* schur = nullptr;  // FGMRES + Jacobi/multigrid (schur_preconditioner >= 0)
   af_imex_stats stats{};
-  // stage-1 tangent / adjoint: the recorded fixed-point trajectory (pres_fixed and u_fixed
-  // entering each iteration, and the final iterate) and a workspace, allocated on first use
-  bool record = false;
-  int rec_iters = 0;
-  std::vector<double*> rec_p, rec_u;
+  // tangent / adjoint: the recorded fixed-point trajectories of stages 1 and 2 (pres_fixed and
+  // u_fixed entering each iteration, and the final iterate), the linearisation point kind
+  // (1: stage 1, 2: a whole step) and a workspace, allocated on first use
+  int record = 0;  // bit s-1: record the fixed point of stage s
+  int rec_iters[2] = {0, 0};
+  std::vector<double*> rec_p[2], rec_u[2];
+  int lin = 0;
   double* adj_mem = nullptr;
 };
 
@@ -74,17 +77,17 @@ static int ierr(int code, const std::string& msg) {
 
 using Apply = std::function<int(const double*, double*)>;
 
-// trajectory buffers of the stage-1 tangent / adjoint, one pair per fixed-point iterate
-static int ensure_rec(af_imex* h, int i) {
-  while ((int)h->rec_p.size() <= i) {
+// trajectory buffers of the tangent / adjoint, one pair per fixed-point iterate of stage k+1
+static int ensure_rec(af_imex* h, int k, int i) {
+  while ((int)h->rec_p[k].size() <= i) {
     double *p = nullptr, *u = nullptr;
     IM_CU(cudaMalloc(&p, h->ns * 8));
     if (cudaMalloc(&u, 2 * h->ns * 8) != cudaSuccess) {
       cudaFree(p);
-      return ierr(AF_CUDA, "stage-1 trajectory: device allocation failed");
+      return ierr(AF_CUDA, "fixed-point trajectory: device allocation failed");
     }
-    h->rec_p.push_back(p);
-    h->rec_u.push_back(u);
+    h->rec_p[k].push_back(p);
+    h->rec_u[k].push_back(u);
   }
   return AF_OK;
 }
@@ -327,10 +330,11 @@ static int fixed_point(af_imex* h, int stage, double* p_out, double* u_out) {
   int iters = 0;
   double err = 0.0;
   for (int iter = 0; iter < h->opt.fixed_point_max_iterations; ++iter) {
-    if (h->record) {  // the iteration's inputs: pres_fixed (pfix_old) and u_fixed
-      IM_AF(ensure_rec(h, iter));
-      IM_CU(cudaMemcpyAsync(h->rec_p[iter], h->pfix_old, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-      IM_CU(cudaMemcpyAsync(h->rec_u[iter], h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+    if (h->record & (1 << (stage - 1))) {  // the iteration's inputs: pres_fixed and u_fixed
+      const int k = stage - 1;
+      IM_AF(ensure_rec(h, k, iter));
+      IM_CU(cudaMemcpyAsync(h->rec_p[k][iter], h->pfix_old, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+      IM_CU(cudaMemcpyAsync(h->rec_u[k][iter], h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
     }
     IM_AF(pressure_fixed_point(h, stage, iter));
     IM_AF(update_velocity(h, stage));
@@ -346,11 +350,12 @@ static int fixed_point(af_imex* h, int stage, double* p_out, double* u_out) {
   }
   h->stats.fixed_point_iterations[stage - 1] = iters;
   h->stats.last_fixed_point_error = err;
-  if (h->record) {  // the final iterate
-    IM_AF(ensure_rec(h, iters));
-    IM_CU(cudaMemcpyAsync(h->rec_p[iters], h->pfix, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-    IM_CU(cudaMemcpyAsync(h->rec_u[iters], h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-    h->rec_iters = iters;
+  if (h->record & (1 << (stage - 1))) {  // the final iterate
+    const int k = stage - 1;
+    IM_AF(ensure_rec(h, k, iters));
+    IM_CU(cudaMemcpyAsync(h->rec_p[k][iters], h->pfix, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+    IM_CU(cudaMemcpyAsync(h->rec_u[k][iters], h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+    h->rec_iters[k] = iters;
   }
   IM_CU(cudaMemcpyAsync(p_out, h->pfix, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
   IM_CU(cudaMemcpyAsync(u_out, h->ufix, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
@@ -385,246 +390,426 @@ static int one_step(af_imex* h) {
   return AF_OK;
 }
 
-// ------------------------------------------------------------------ stage-1 tangent and adjoint
-// Stage 1 as a map (rho0, u0, p0) -> (rho2, u2, p2): the density update and the pressure fixed
-// point (update_density, pressure_fixed_point, update_velocity; Atmospheric_Flow.cc:1116-1156).
-// The tangent-linear and the adjoint differentiate the iterations as the forward ran them
-// (the recorded number of fixed-point iterations), each linear solve taken as exact: with
-// P_i, U_i the pres_fixed and u_fixed entering iteration i (P_0 = p0, U_0 = u0),
-//   rhs_p, rhs_u = R(rho0, u0, p0, rho2, U_i)           (fused stage-1 rhs triple)
-//   t       = A^{-1} rhs_u                                (A = A(rho2), rho2 = M^{-1} R_rho(rho0, u0))
-//   b       = rhs_p - C(t; P_i)
-//   P_{i+1} : S(P_i; P_{i+1}) = b,   S(p_f; p) = D p - C(A^{-1} B p; p_f)
-//   U_{i+1} = A^{-1} (rhs_u - B P_{i+1}).
-// A is linear in rho2 and C in p_f, so their coefficient tangents are the operators with the
-// perturbation as the coefficient: A(drho) x and C(w; dp_f).  Linearising the solve for P_{i+1}:
-//   J_S(P_{i+1}) dP = db - J_C(w) A^{-1} A(drho2) w + C(w; dP_i),   w = A^{-1} B P_{i+1}.
+// ------------------------------------------------------------------ tangent-linear and adjoint
+// One IMEX step as a map (rho0, u0, p0) -> (rho_c, u_c, p_new), and stage 1 alone as
+// (rho0, u0, p0) -> (rho2, u2, p2).  The tangent-linear and the adjoint differentiate the step
+// as the forward ran it: the recorded fixed-point iterations of stages 1 and 2, each linear
+// solve taken as exact (Schur solves to a given tolerance with the stepper's FGMRES and
+// preconditioner; the cell-wise A, M, D inverses are exact).
+//
+// Fixed-point stage s (1 or 2), explicit fields E (rho_j, u_j, p_j of the earlier stages):
+//   rho_{s+1} = M^{-1} R_rho(E);  with P_0 = p_s, U_0 = u_s the last explicit p, u and A = A(rho_{s+1}):
+//   rhs_p, rhs_u = R(E, rho_{s+1}, U_i)                    (fused rhs triple of stage s)
+//   t        = A^{-1} rhs_u;  b = rhs_p - C(t; P_i)
+//   P_{i+1}  : S(P_i; P_{i+1}) = b,   S(p_f; p) = D p - C(A^{-1} B p; p_f)
+//   U_{i+1}  = A^{-1} (rhs_u - B P_{i+1}).
+// A is linear in rho and C in p_f, so their coefficient tangents are the operators with the
+// perturbation as the coefficient; linearising the Schur solve:
+//   J_S(P_{i+1}) dP = db - J_C(w) A^{-1} A(drho) w + C(w; dP_i),   w = A^{-1} B P_{i+1}.
+// Stage 3 (explicit fields E of stages 1..3):  rho_c = M^{-1} R_rho(E),  u_c = A(rho_c)^{-1} R_u(E),
+//   p_new = D^{-1} R_p(E, rho_c, u_c).
 
-constexpr int kAdjVectors = 28;  // velocity-sized work vectors of the tangent / adjoint
+constexpr int kAdjVectors = 64;  // velocity-sized work vectors of the tangent / adjoint
+constexpr int kSaved = 3;        // the first three hold the linearisation's input state
 
 static int ensure_adj(af_imex* h) {
   if (h->adj_mem) return AF_OK;
   IM_CU(cudaMalloc(&h->adj_mem, sizeof(double) * 2 * h->ns * kAdjVectors));
   return AF_OK;
 }
+static double* saved(af_imex* h, int k) { return h->adj_mem + (size_t)k * 2 * h->ns; }
 
 namespace {
-struct Stage1Ctx {
+struct Ctx {
   af_imex* h;
   af_operator* o;
   long ns;
   cudaStream_t st;
-  CParams cp;
-  double* v[kAdjVectors];
-  int next = 0;
-  double* take() { return v[next++]; }
+  int next = kSaved;
+  double* take() { return h->adj_mem + (size_t)(next++) * 2 * ns; }
 };
 }  // namespace
 
-static int s1_ctx(af_imex* h, Stage1Ctx& c) {
-  if (!h->schur) return ierr(AF_UNSUPPORTED, "stage-1 tangent/adjoint: needs schur_preconditioner >= 0");
-  if (h->rec_iters < 1) return ierr(AF_BAD_ARG, "stage-1 tangent/adjoint: call af_imex_stage1_forward first");
+#define AD_TAKE(c) ((c).next < kAdjVectors ? (c).take() : nullptr)
+
+static int ctx_init(af_imex* h, Ctx& c, int need_lin) {
+  if (!h->schur) return ierr(AF_UNSUPPORTED, "tangent/adjoint: needs schur_preconditioner >= 0");
+  if (h->lin < need_lin) return ierr(AF_BAD_ARG, "tangent/adjoint: run the recorded forward first");
   IM_AF(ensure_adj(h));
   c.h = h;
   c.o = h->op;
   c.ns = h->ns;
   c.st = h->op->stream;
-  c.cp.cdt = h->op->a22t * h->op->dt;  // stage 1: the B/C coefficient a~22 (euler_operator.h:1428)
-  c.cp.g1 = 1.0 / (1.4 - 1.0);
-  c.cp.gg = 1.4 / (1.4 - 1.0);
-  for (int k = 0; k < kAdjVectors; ++k) c.v[k] = h->adj_mem + (size_t)k * 2 * h->ns;
-  IM_AF(af_set_HYPERBOLIC_stage(h->op, 1));
   return AF_OK;
 }
-
-// x = A^{-1} b (NS 3) or M^{-1} b (NS 1), exact cell-wise inverses
-static int s1_inv(Stage1Ctx& c, int ns_stage, double* x, const double* b) {
+static CParams stage_cparams(const af_operator* o, int stage) {
+  CParams cp;
+  cp.cdt = (stage == 1 ? o->a22t : o->a33t) * o->dt;  // the B/C coefficient (euler_operator.h:1428)
+  cp.g1 = 1.0 / (1.4 - 1.0);
+  cp.gg = 1.4 / (1.4 - 1.0);
+  return cp;
+}
+// the operator in the state of a stage: HYPERBOLIC_stage, rho_for_fixed, preconditioner
+static int stage_setup(Ctx& c, int stage, const double* rho_fixed) {
+  IM_AF(af_set_HYPERBOLIC_stage(c.o, stage));
+  IM_AF(af_set_rho_for_fixed(c.o, rho_fixed));
+  if (stage < 3) IM_AF(af_schur_solver_setup(c.h->schur, 0));
+  return AF_OK;
+}
+// x = A^{-1} b (NS 3), M^{-1} b (NS 1) or D^{-1} b (NS 6), exact cell-wise inverses
+static int ad_inv(Ctx& c, int ns_stage, double* x, const double* b) {
   IM_AF(af_set_NS_stage(c.o, ns_stage));
   return af_vmult_inverse(c.o, x, b);
 }
 // dst = A(rho) x  (rho-weighted velocity mass with an arbitrary weight)
-static int s1_A(Stage1Ctx& c, const double* rho, const double* x, double* dst) {
+static int ad_A(Ctx& c, const double* rho, const double* x, double* dst) {
   IM_CU(c.o->ops->mass(c.o->mesh, 2, x, rho, 1.0, dst, c.o->ncell, c.st));
   c.o->launches += 1;
   return AF_OK;
 }
 // dst = C(w; pf)  (vmult_enthalpy with an arbitrary pres_fixed)
-static int s1_C(Stage1Ctx& c, const double* w, const double* pf, double* dst) {
-  IM_CU(c.o->ops->op_C(c.o->mesh, w, pf, nullptr, c.cp, dst, c.o->ncell, c.st));
+static int ad_C(Ctx& c, int stage, const double* w, const double* pf, double* dst) {
+  IM_CU(c.o->ops->op_C(c.o->mesh, w, pf, nullptr, stage_cparams(c.o, stage), dst, c.o->ncell, c.st));
   c.o->launches += 1;
   return AF_OK;
 }
-static int s1_axpby(Stage1Ctx& c, double a, const double* x, double b, double* y, long n) {
+static int ad_axpby(Ctx& c, double a, const double* x, double b, double* y, long n) {
   IM_CU(axpby(a, x, b, y, n, c.st));
   c.o->launches += 1;
   return AF_OK;
 }
-static int s1_copy(Stage1Ctx& c, double* dst, const double* src, long n) {
+static int ad_copy(Ctx& c, double* dst, const double* src, long n) {
   IM_CU(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToDevice, c.st));
   return AF_OK;
 }
-static int s1_zero(Stage1Ctx& c, double* x, long n) {
+static int ad_zero(Ctx& c, double* x, long n) {
   IM_CU(cudaMemsetAsync(x, 0, n * 8, c.st));
   return AF_OK;
 }
-// rhs_u at the linearisation point and t = A^{-1} rhs_u
-static int s1_rhs_u_t(Stage1Ctx& c, double* rhs_u, double* t) {
-  af_imex* h = c.h;
-  const double* su[] = {h->rho0, h->u0, h->p0, h->rho2};
-  IM_AF(af_vmult_rhs_velocity_fixed(c.o, rhs_u, su, 4));
-  return s1_inv(c, 3, t, rhs_u);
+static long comp_len(long ns, int k) { return (k % 3 == 1) ? 2 * ns : ns; }  // rho, u, p pattern
+
+static void lin_fields(af_imex* h, const double** E) {
+  E[0] = saved(h, 0); E[1] = saved(h, 1); E[2] = saved(h, 2);
+  E[3] = h->rho2; E[4] = h->u2; E[5] = h->p2;
+  E[6] = h->rho3; E[7] = h->u3; E[8] = h->p3;
 }
-static int s1_tangent(af_imex* h, const double* drho0, const double* du0, const double* dp0, double* drho2_out,
-                      double* du2, double* dp2, double tol, int maxit) {
-  Stage1Ctx c;
-  IM_AF(s1_ctx(h, c));
-  const long ns = c.ns;
+static double* rho_next(af_imex* h, int s) { return s == 1 ? h->rho2 : h->rho3; }
+
+// tangent of fixed-point stage s: dE (3 s explicit-field tangents) -> (drho_{s+1}, dU_I, dP_I)
+static int fp_tangent(Ctx& c, int s, const double* const* dE, double* drho_out, double* du_out, double* dp_out,
+                      double tol, int maxit) {
+  af_imex* h = c.h;
   af_operator* o = c.o;
+  const long ns = c.ns;
+  const int k = s - 1, n = 3 * s + 2;
+  const double* E[9];
+  lin_fields(h, E);
+  double* rn = rho_next(h, s);
+  IM_AF(stage_setup(c, s, rn));
+  const int mark = c.next;
   double *zs = c.take(), *zv = c.take(), *rhs_u = c.take(), *t = c.take(), *drr = c.take(), *drhs_u = c.take();
   double *drhs_p = c.take(), *tmpA = c.take(), *dt = c.take(), *jc = c.take(), *cc = c.take(), *db = c.take();
   double *Bp = c.take(), *w = c.take(), *aw = c.take(), *z = c.take(), *jz = c.take(), *cw = c.take();
-  double *dP = c.take(), *dU = c.take(), *dPf = c.take(), *dUf = c.take(), *drho2 = c.take(), *bdp = c.take();
-  IM_AF(s1_zero(c, zs, ns));
-  IM_AF(s1_zero(c, zv, 2 * ns));
-  IM_AF(s1_rhs_u_t(c, rhs_u, t));
-  // drho2 = M^{-1} dR_rho (the density rhs depends on rho0 and u0 only)
-  {
-    const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, h->rec_u[0]};
-    const double* dsrc[] = {drho0, du0, dp0, zs, zv};
-    IM_AF(af_vmult_rhs_fused_tangent(o, src, 5, dsrc, drr, drhs_u, drhs_p));
-    IM_AF(s1_inv(c, 1, drho2, drr));
-  }
-  IM_AF(s1_copy(c, dPf, dp0, ns));
-  IM_AF(s1_copy(c, dUf, du0, 2 * ns));
-  for (int i = 0; i < h->rec_iters; ++i) {
-    const double *Pi = h->rec_p[i], *Ui = h->rec_u[i], *Pn = h->rec_p[i + 1], *Un = h->rec_u[i + 1];
-    const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, Ui};
-    const double* dsrc[] = {drho0, du0, dp0, drho2, dUf};
-    IM_AF(af_vmult_rhs_fused_tangent(o, src, 5, dsrc, drr, drhs_u, drhs_p));
-    // dt = A^{-1} (drhs_u - A(drho2) t)
-    IM_AF(s1_A(c, drho2, t, tmpA));
-    IM_AF(s1_axpby(c, 1.0, drhs_u, -1.0, tmpA, 2 * ns));
-    IM_AF(s1_inv(c, 3, dt, tmpA));
+  double *dP = c.take(), *dU = c.take(), *dPf = c.take(), *dUf = c.take(), *drho = c.take(), *bdp = c.take();
+  IM_AF(ad_zero(c, zs, ns));
+  IM_AF(ad_zero(c, zv, 2 * ns));
+  const double* su[8];
+  for (int j = 0; j < 3 * s; ++j) su[j] = E[j];
+  su[3 * s] = rn;
+  IM_AF(af_vmult_rhs_velocity_fixed(o, rhs_u, su, 3 * s + 1));
+  IM_AF(ad_inv(c, 3, t, rhs_u));
+  const double* src[11];
+  const double* dsrc[11];
+  for (int j = 0; j < 3 * s; ++j) { src[j] = E[j]; dsrc[j] = dE[j]; }
+  src[3 * s] = rn;
+  src[3 * s + 1] = h->rec_u[k][0];
+  dsrc[3 * s] = zs;
+  dsrc[3 * s + 1] = zv;
+  IM_AF(af_vmult_rhs_fused_tangent(o, src, n, dsrc, drr, drhs_u, drhs_p));  // the density rhs
+  IM_AF(ad_inv(c, 1, drho, drr));
+  IM_AF(ad_copy(c, dPf, dE[3 * s - 1], ns));      // P_0 = p_s
+  IM_AF(ad_copy(c, dUf, dE[3 * s - 2], 2 * ns));  // U_0 = u_s
+  dsrc[3 * s] = drho;
+  dsrc[3 * s + 1] = dUf;
+  for (int i = 0; i < h->rec_iters[k]; ++i) {
+    const double *Pi = h->rec_p[k][i], *Ui = h->rec_u[k][i], *Pn = h->rec_p[k][i + 1], *Un = h->rec_u[k][i + 1];
+    src[3 * s + 1] = Ui;
+    IM_AF(af_vmult_rhs_fused_tangent(o, src, n, dsrc, drr, drhs_u, drhs_p));
+    // dt = A^{-1} (drhs_u - A(drho) t)
+    IM_AF(ad_A(c, drho, t, tmpA));
+    IM_AF(ad_axpby(c, 1.0, drhs_u, -1.0, tmpA, 2 * ns));
+    IM_AF(ad_inv(c, 3, dt, tmpA));
     // db = drhs_p - J_C(t; P_i) dt - C(t; dP_i)
     IM_AF(af_set_pres_fixed(o, Pi));
     IM_AF(af_vmult_enthalpy_tangent(o, jc, t, dt));
-    IM_AF(s1_C(c, t, dPf, cc));
-    IM_AF(s1_copy(c, db, drhs_p, ns));
-    IM_AF(s1_axpby(c, -1.0, jc, 1.0, db, ns));
-    IM_AF(s1_axpby(c, -1.0, cc, 1.0, db, ns));
-    // right-hand side of J_S(P_{i+1}) dP: db - J_C(w) A^{-1} A(drho2) w + C(w; dP_i)
+    IM_AF(ad_C(c, s, t, dPf, cc));
+    IM_AF(ad_copy(c, db, drhs_p, ns));
+    IM_AF(ad_axpby(c, -1.0, jc, 1.0, db, ns));
+    IM_AF(ad_axpby(c, -1.0, cc, 1.0, db, ns));
+    // right-hand side of J_S(P_{i+1}) dP: db - J_C(w) A^{-1} A(drho) w + C(w; dP_i)
     IM_AF(af_vmult_pressure(o, Bp, Pn));
-    IM_AF(s1_inv(c, 3, w, Bp));
-    IM_AF(s1_A(c, drho2, w, aw));
-    IM_AF(s1_inv(c, 3, z, aw));
+    IM_AF(ad_inv(c, 3, w, Bp));
+    IM_AF(ad_A(c, drho, w, aw));
+    IM_AF(ad_inv(c, 3, z, aw));
     IM_AF(af_vmult_enthalpy_tangent(o, jz, w, z));
-    IM_AF(s1_C(c, w, dPf, cw));
-    IM_AF(s1_axpby(c, -1.0, jz, 1.0, db, ns));
-    IM_AF(s1_axpby(c, 1.0, cw, 1.0, db, ns));
-    IM_AF(s1_zero(c, dP, ns));
+    IM_AF(ad_C(c, s, w, dPf, cw));
+    IM_AF(ad_axpby(c, -1.0, jz, 1.0, db, ns));
+    IM_AF(ad_axpby(c, 1.0, cw, 1.0, db, ns));
+    IM_AF(ad_zero(c, dP, ns));
     af_schur_stats sst{};
     IM_AF(af_schur_solve_tangent(h->schur, Pn, dP, db, tol, maxit, &sst));
-    // dU = A^{-1} (drhs_u - B dP - A(drho2) U_{i+1})
+    // dU = A^{-1} (drhs_u - B dP - A(drho) U_{i+1})
     IM_AF(af_vmult_pressure(o, bdp, dP));
-    IM_AF(s1_A(c, drho2, Un, tmpA));
-    IM_AF(s1_axpby(c, 1.0, drhs_u, -1.0, tmpA, 2 * ns));
-    IM_AF(s1_axpby(c, -1.0, bdp, 1.0, tmpA, 2 * ns));
-    IM_AF(s1_inv(c, 3, dU, tmpA));
-    IM_AF(s1_copy(c, dPf, dP, ns));
-    IM_AF(s1_copy(c, dUf, dU, 2 * ns));
+    IM_AF(ad_A(c, drho, Un, tmpA));
+    IM_AF(ad_axpby(c, 1.0, drhs_u, -1.0, tmpA, 2 * ns));
+    IM_AF(ad_axpby(c, -1.0, bdp, 1.0, tmpA, 2 * ns));
+    IM_AF(ad_inv(c, 3, dU, tmpA));
+    IM_AF(ad_copy(c, dPf, dP, ns));
+    IM_AF(ad_copy(c, dUf, dU, 2 * ns));
   }
-  IM_AF(s1_copy(c, drho2_out, drho2, ns));
-  IM_AF(s1_copy(c, du2, dUf, 2 * ns));
-  IM_AF(s1_copy(c, dp2, dPf, ns));
-  IM_CU(cudaStreamSynchronize(c.st));
+  IM_AF(ad_copy(c, drho_out, drho, ns));
+  IM_AF(ad_copy(c, du_out, dUf, 2 * ns));
+  IM_AF(ad_copy(c, dp_out, dPf, ns));
+  c.next = mark;
   return AF_OK;
 }
 
-// the transpose of s1_tangent, step by step in reverse
-static int s1_backward(af_imex* h, const double* rho2bar, const double* u2bar, const double* p2bar, double* rho0bar,
-                       double* u0bar, double* p0bar, double tol, int maxit) {
-  Stage1Ctx c;
-  IM_AF(s1_ctx(h, c));
-  const long ns = c.ns;
+// adjoint of fixed-point stage s: (rho_{s+1}, U_I, P_I) cotangents -> Ebar (3 s, accumulated)
+static int fp_backward(Ctx& c, int s, const double* rho_bar, const double* u_bar, const double* p_bar,
+                       double* const* Ebar, double tol, int maxit) {
+  af_imex* h = c.h;
   af_operator* o = c.o;
-  double *zs = c.take(), *rhs_u = c.take(), *t = c.take(), *R0 = c.take(), *U0 = c.take(), *P0 = c.take();
-  double *R2 = c.take(), *Pb = c.take(), *Ub = c.take(), *rub = c.take(), *rpb = c.take(), *Pfb = c.take();
-  double *s1 = c.take(), *tmp = c.take(), *x = c.take(), *Bp = c.take(), *w = c.take(), *jt = c.take();
-  double *z = c.take(), *ts = c.take(), *dtb = c.take(), *rrb = c.take();
-  double* xb[5] = {c.take(), c.take(), c.take(), c.take(), c.take()};
-  IM_AF(s1_zero(c, zs, ns));
-  IM_AF(s1_zero(c, R0, ns));
-  IM_AF(s1_zero(c, U0, 2 * ns));
-  IM_AF(s1_zero(c, P0, ns));
-  IM_AF(s1_copy(c, R2, rho2bar, ns));
-  IM_AF(s1_copy(c, Pb, p2bar, ns));
-  IM_AF(s1_copy(c, Ub, u2bar, 2 * ns));
-  IM_AF(s1_rhs_u_t(c, rhs_u, t));
-  for (int i = h->rec_iters - 1; i >= 0; --i) {
-    const double *Pi = h->rec_p[i], *Ui = h->rec_u[i], *Pn = h->rec_p[i + 1], *Un = h->rec_u[i + 1];
+  const long ns = c.ns;
+  const int k = s - 1, n = 3 * s + 2;
+  const double* E[9];
+  lin_fields(h, E);
+  double* rn = rho_next(h, s);
+  IM_AF(stage_setup(c, s, rn));
+  const int mark = c.next;
+  double *zs = c.take(), *zv = c.take(), *rhs_u = c.take(), *t = c.take(), *R2 = c.take(), *Pb = c.take();
+  double *Ub = c.take(), *rub = c.take(), *rpb = c.take(), *Pfb = c.take(), *s1 = c.take(), *tmp = c.take();
+  double *x = c.take(), *Bp = c.take(), *w = c.take(), *jt = c.take(), *z = c.take(), *ts = c.take();
+  double *dtb = c.take(), *rrb = c.take();
+  double* xb[11];
+  for (int j = 0; j < n; ++j) xb[j] = c.take();
+  IM_AF(ad_zero(c, zs, ns));
+  IM_AF(ad_zero(c, zv, 2 * ns));
+  IM_AF(ad_copy(c, R2, rho_bar, ns));
+  IM_AF(ad_copy(c, Pb, p_bar, ns));
+  IM_AF(ad_copy(c, Ub, u_bar, 2 * ns));
+  const double* su[8];
+  for (int j = 0; j < 3 * s; ++j) su[j] = E[j];
+  su[3 * s] = rn;
+  IM_AF(af_vmult_rhs_velocity_fixed(o, rhs_u, su, 3 * s + 1));
+  IM_AF(ad_inv(c, 3, t, rhs_u));
+  const double* src[11];
+  for (int j = 0; j < 3 * s; ++j) src[j] = E[j];
+  src[3 * s] = rn;
+  for (int i = h->rec_iters[k] - 1; i >= 0; --i) {
+    const double *Pi = h->rec_p[k][i], *Ui = h->rec_u[k][i], *Pn = h->rec_p[k][i + 1], *Un = h->rec_u[k][i + 1];
     IM_AF(af_set_pres_fixed(o, Pi));
-    IM_AF(s1_zero(c, rpb, ns));
-    IM_AF(s1_zero(c, Pfb, ns));
+    IM_AF(ad_zero(c, rpb, ns));
+    IM_AF(ad_zero(c, Pfb, ns));
     // U_{i+1} = A^{-1} (rhs_u - B P_{i+1}):  s1 = A^{-1} Ub
-    IM_AF(s1_inv(c, 3, s1, Ub));
-    IM_AF(s1_copy(c, rub, s1, 2 * ns));
+    IM_AF(ad_inv(c, 3, s1, Ub));
+    IM_AF(ad_copy(c, rub, s1, 2 * ns));
     IM_AF(af_vmult_pressure_transpose(o, tmp, s1));
-    IM_AF(s1_axpby(c, -1.0, tmp, 1.0, Pb, ns));
+    IM_AF(ad_axpby(c, -1.0, tmp, 1.0, Pb, ns));
     IM_AF(af_vmult_velocity_mass_rho_transpose(o, ts, Un, s1));
-    IM_AF(s1_axpby(c, -1.0, ts, 1.0, R2, ns));
+    IM_AF(ad_axpby(c, -1.0, ts, 1.0, R2, ns));
     // P_{i+1}: x = J_S(P_{i+1})^{-T} Pb is the cotangent of db
-    IM_AF(s1_zero(c, x, ns));
+    IM_AF(ad_zero(c, x, ns));
     af_schur_stats sst{};
     IM_AF(af_schur_solve_transpose(h->schur, Pn, x, Pb, tol, maxit, &sst));
     IM_AF(af_vmult_pressure(o, Bp, Pn));
-    IM_AF(s1_inv(c, 3, w, Bp));
+    IM_AF(ad_inv(c, 3, w, Bp));
     IM_AF(af_vmult_enthalpy_pf_transpose(o, ts, w, x));  // + C(w; dP_i)
-    IM_AF(s1_axpby(c, 1.0, ts, 1.0, Pfb, ns));
-    IM_AF(af_vmult_enthalpy_transpose(o, jt, w, x));     // - J_C(w) A^{-1} A(drho2) w
-    IM_AF(s1_inv(c, 3, z, jt));
+    IM_AF(ad_axpby(c, 1.0, ts, 1.0, Pfb, ns));
+    IM_AF(af_vmult_enthalpy_transpose(o, jt, w, x));     // - J_C(w) A^{-1} A(drho) w
+    IM_AF(ad_inv(c, 3, z, jt));
     IM_AF(af_vmult_velocity_mass_rho_transpose(o, ts, w, z));
-    IM_AF(s1_axpby(c, -1.0, ts, 1.0, R2, ns));
+    IM_AF(ad_axpby(c, -1.0, ts, 1.0, R2, ns));
     // db = drhs_p - J_C(t) dt - C(t; dP_i)
-    IM_AF(s1_axpby(c, 1.0, x, 1.0, rpb, ns));
+    IM_AF(ad_axpby(c, 1.0, x, 1.0, rpb, ns));
     IM_AF(af_vmult_enthalpy_transpose(o, dtb, t, x));
     IM_AF(af_vmult_enthalpy_pf_transpose(o, ts, t, x));
-    IM_AF(s1_axpby(c, -1.0, ts, 1.0, Pfb, ns));
-    // dt = A^{-1} (drhs_u - A(drho2) t), with the cotangent -J_C(t)^T x
-    IM_AF(s1_inv(c, 3, s1, dtb));
-    IM_AF(s1_axpby(c, -1.0, s1, 1.0, rub, 2 * ns));
+    IM_AF(ad_axpby(c, -1.0, ts, 1.0, Pfb, ns));
+    // dt = A^{-1} (drhs_u - A(drho) t), with the cotangent -J_C(t)^T x
+    IM_AF(ad_inv(c, 3, s1, dtb));
+    IM_AF(ad_axpby(c, -1.0, s1, 1.0, rub, 2 * ns));
     IM_AF(af_vmult_velocity_mass_rho_transpose(o, ts, t, s1));
-    IM_AF(s1_axpby(c, 1.0, ts, 1.0, R2, ns));
-    // the rhs triple at (rho0, u0, p0, rho2, U_i)
-    {
-      const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, Ui};
-      IM_AF(af_vmult_rhs_fused_backward(o, src, 5, zs, rub, rpb, xb));
-      IM_AF(s1_axpby(c, 1.0, xb[0], 1.0, R0, ns));
-      IM_AF(s1_axpby(c, 1.0, xb[1], 1.0, U0, 2 * ns));
-      IM_AF(s1_axpby(c, 1.0, xb[2], 1.0, P0, ns));
-      IM_AF(s1_axpby(c, 1.0, xb[3], 1.0, R2, ns));
-    }
+    IM_AF(ad_axpby(c, 1.0, ts, 1.0, R2, ns));
+    // the rhs triple at (E, rho_{s+1}, U_i)
+    src[3 * s + 1] = Ui;
+    IM_AF(af_vmult_rhs_fused_backward(o, src, n, zs, rub, rpb, xb));
+    for (int j = 0; j < 3 * s; ++j) IM_AF(ad_axpby(c, 1.0, xb[j], 1.0, Ebar[j], comp_len(ns, j)));
+    IM_AF(ad_axpby(c, 1.0, xb[3 * s], 1.0, R2, ns));
     // the iteration's inputs P_i, U_i: their cotangents go to the previous iterate
-    IM_AF(s1_copy(c, Pb, Pfb, ns));
-    IM_AF(s1_copy(c, Ub, xb[4], 2 * ns));
+    IM_AF(ad_copy(c, Pb, Pfb, ns));
+    IM_AF(ad_copy(c, Ub, xb[3 * s + 1], 2 * ns));
   }
-  IM_AF(s1_axpby(c, 1.0, Pb, 1.0, P0, ns));  // P_0 = p0, U_0 = u0
-  IM_AF(s1_axpby(c, 1.0, Ub, 1.0, U0, 2 * ns));
-  // rho2 = M^{-1} R_rho(rho0, u0)
-  IM_AF(s1_inv(c, 1, rrb, R2));
-  {
-    IM_AF(s1_zero(c, tmp, 2 * ns));
-    const double* src[] = {h->rho0, h->u0, h->p0, h->rho2, h->rec_u[0]};
-    IM_AF(af_vmult_rhs_fused_backward(o, src, 5, rrb, tmp, zs, xb));
-    IM_AF(s1_axpby(c, 1.0, xb[0], 1.0, R0, ns));
-    IM_AF(s1_axpby(c, 1.0, xb[1], 1.0, U0, 2 * ns));
-  }
-  IM_AF(s1_copy(c, rho0bar, R0, ns));
-  IM_AF(s1_copy(c, u0bar, U0, 2 * ns));
-  IM_AF(s1_copy(c, p0bar, P0, ns));
+  IM_AF(ad_axpby(c, 1.0, Pb, 1.0, Ebar[3 * s - 1], ns));      // P_0 = p_s
+  IM_AF(ad_axpby(c, 1.0, Ub, 1.0, Ebar[3 * s - 2], 2 * ns));  // U_0 = u_s
+  // rho_{s+1} = M^{-1} R_rho(E)
+  IM_AF(ad_inv(c, 1, rrb, R2));
+  src[3 * s + 1] = h->rec_u[k][0];
+  IM_AF(af_vmult_rhs_fused_backward(o, src, n, rrb, zv, zs, xb));
+  for (int j = 0; j < 3 * s; ++j) IM_AF(ad_axpby(c, 1.0, xb[j], 1.0, Ebar[j], comp_len(ns, j)));
+  c.next = mark;
+  return AF_OK;
+}
+
+// stage 3: dE (9 explicit-field tangents) -> (drho_c, du_c, dp_new)
+static int s3_tangent(Ctx& c, const double* const* dE, double* drc, double* duc, double* dpn) {
+  af_imex* h = c.h;
+  af_operator* o = c.o;
+  const long ns = c.ns;
+  const double* E[9];
+  lin_fields(h, E);
+  IM_AF(stage_setup(c, 3, h->rhoc));
+  const int mark = c.next;
+  double *zs = c.take(), *zv = c.take(), *drr = c.take(), *dru = c.take(), *drp = c.take(), *tmpA = c.take();
+  IM_AF(ad_zero(c, zs, ns));
+  IM_AF(ad_zero(c, zv, 2 * ns));
+  const double* src[11];
+  const double* dsrc[11];
+  for (int j = 0; j < 9; ++j) { src[j] = E[j]; dsrc[j] = dE[j]; }
+  src[9] = h->rhoc;
+  src[10] = h->uc;
+  dsrc[9] = zs;
+  dsrc[10] = zv;
+  IM_AF(af_vmult_rhs_fused_tangent(o, src, 11, dsrc, drr, dru, drp));  // density and velocity rhs
+  IM_AF(ad_inv(c, 1, drc, drr));
+  IM_AF(ad_A(c, drc, h->uc, tmpA));  // du_c = A^{-1} (dR_u - A(drho_c) u_c)
+  IM_AF(ad_axpby(c, 1.0, dru, -1.0, tmpA, 2 * ns));
+  IM_AF(ad_inv(c, 3, duc, tmpA));
+  dsrc[9] = drc;
+  dsrc[10] = duc;
+  IM_AF(af_vmult_rhs_fused_tangent(o, src, 11, dsrc, drr, dru, drp));  // the pressure rhs
+  IM_AF(ad_inv(c, 6, dpn, drp));
+  c.next = mark;
+  return AF_OK;
+}
+
+// adjoint of stage 3: (rho_c, u_c, p_new) cotangents -> Ebar (9, accumulated)
+static int s3_backward(Ctx& c, const double* rc_bar, const double* uc_bar, const double* pn_bar, double* const* Ebar) {
+  af_imex* h = c.h;
+  af_operator* o = c.o;
+  const long ns = c.ns;
+  const double* E[9];
+  lin_fields(h, E);
+  IM_AF(stage_setup(c, 3, h->rhoc));
+  const int mark = c.next;
+  double *zs = c.take(), *zv = c.take(), *rpb = c.take(), *Rc = c.take(), *Uc = c.take(), *s1 = c.take();
+  double *rub = c.take(), *ts = c.take(), *rrb = c.take();
+  double* xb[11];
+  for (int j = 0; j < 11; ++j) xb[j] = c.take();
+  IM_AF(ad_zero(c, zs, ns));
+  IM_AF(ad_zero(c, zv, 2 * ns));
+  const double* src[11];
+  for (int j = 0; j < 9; ++j) src[j] = E[j];
+  src[9] = h->rhoc;
+  src[10] = h->uc;
+  IM_AF(ad_inv(c, 6, rpb, pn_bar));  // p_new = D^{-1} R_p (D symmetric)
+  IM_AF(af_vmult_rhs_fused_backward(o, src, 11, zs, zv, rpb, xb));
+  for (int j = 0; j < 9; ++j) IM_AF(ad_axpby(c, 1.0, xb[j], 1.0, Ebar[j], comp_len(ns, j)));
+  IM_AF(ad_copy(c, Rc, rc_bar, ns));
+  IM_AF(ad_axpby(c, 1.0, xb[9], 1.0, Rc, ns));
+  IM_AF(ad_copy(c, Uc, uc_bar, 2 * ns));
+  IM_AF(ad_axpby(c, 1.0, xb[10], 1.0, Uc, 2 * ns));
+  IM_AF(ad_inv(c, 3, s1, Uc));  // u_c = A(rho_c)^{-1} R_u
+  IM_AF(ad_copy(c, rub, s1, 2 * ns));
+  IM_AF(af_vmult_velocity_mass_rho_transpose(o, ts, h->uc, s1));
+  IM_AF(ad_axpby(c, -1.0, ts, 1.0, Rc, ns));
+  IM_AF(ad_inv(c, 1, rrb, Rc));  // rho_c = M^{-1} R_rho
+  IM_AF(af_vmult_rhs_fused_backward(o, src, 11, rrb, rub, zs, xb));
+  for (int j = 0; j < 9; ++j) IM_AF(ad_axpby(c, 1.0, xb[j], 1.0, Ebar[j], comp_len(ns, j)));
+  c.next = mark;
+  return AF_OK;
+}
+
+static int step_tangent(af_imex* h, const double* const* dx, double* const* dy, double tol, int maxit) {
+  Ctx c;
+  IM_AF(ctx_init(h, c, 2));
+  const double* dE[9] = {dx[0], dx[1], dx[2]};
+  double* t[6];
+  for (int j = 0; j < 6; ++j) t[j] = c.take();
+  IM_AF(fp_tangent(c, 1, dE, t[0], t[1], t[2], tol, maxit));
+  dE[3] = t[0]; dE[4] = t[1]; dE[5] = t[2];
+  IM_AF(fp_tangent(c, 2, dE, t[3], t[4], t[5], tol, maxit));
+  dE[6] = t[3]; dE[7] = t[4]; dE[8] = t[5];
+  IM_AF(s3_tangent(c, dE, dy[0], dy[1], dy[2]));
   IM_CU(cudaStreamSynchronize(c.st));
   return AF_OK;
 }
 
+static int step_backward(af_imex* h, const double* const* ybar, double* const* xbar, double tol, int maxit) {
+  Ctx c;
+  IM_AF(ctx_init(h, c, 2));
+  double* Eb[9];
+  for (int j = 0; j < 9; ++j) {
+    Eb[j] = c.take();
+    IM_AF(ad_zero(c, Eb[j], comp_len(c.ns, j)));
+  }
+  IM_AF(s3_backward(c, ybar[0], ybar[1], ybar[2], Eb));
+  IM_AF(fp_backward(c, 2, Eb[6], Eb[7], Eb[8], Eb, tol, maxit));
+  IM_AF(fp_backward(c, 1, Eb[3], Eb[4], Eb[5], Eb, tol, maxit));
+  for (int j = 0; j < 3; ++j) IM_AF(ad_copy(c, xbar[j], Eb[j], comp_len(c.ns, j)));
+  IM_CU(cudaStreamSynchronize(c.st));
+  return AF_OK;
+}
+
+static int s1_tangent(af_imex* h, const double* const* dx, double* const* dy, double tol, int maxit) {
+  Ctx c;
+  IM_AF(ctx_init(h, c, 1));
+  IM_AF(fp_tangent(c, 1, dx, dy[0], dy[1], dy[2], tol, maxit));
+  IM_CU(cudaStreamSynchronize(c.st));
+  return AF_OK;
+}
+
+static int s1_backward(af_imex* h, const double* const* ybar, double* const* xbar, double tol, int maxit) {
+  Ctx c;
+  IM_AF(ctx_init(h, c, 1));
+  for (int j = 0; j < 3; ++j) IM_AF(ad_zero(c, xbar[j], comp_len(c.ns, j)));
+  IM_AF(fp_backward(c, 1, ybar[0], ybar[1], ybar[2], xbar, tol, maxit));
+  IM_CU(cudaStreamSynchronize(c.st));
+  return AF_OK;
+}
+
+// the recorded forward: stage 1 (stages = 1) or a whole step (stages = 3) from (rho0, u0, p0)
+static int recorded_forward(af_imex* h, const double* rho0, const double* u0, const double* p0, int stages) {
+  af_operator* o = h->op;
+  const long ns = h->ns;
+  h->lin = 0;
+  IM_AF(ensure_adj(h));
+  // the linearisation's input state (rho0, u0, p0 may alias the saved copies)
+  if (rho0 != saved(h, 0)) IM_CU(cudaMemcpyAsync(saved(h, 0), rho0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  if (u0 != saved(h, 1)) IM_CU(cudaMemcpyAsync(saved(h, 1), u0, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  if (p0 != saved(h, 2)) IM_CU(cudaMemcpyAsync(saved(h, 2), p0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(h->rho0, saved(h, 0), ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(h->u0, saved(h, 1), 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  IM_CU(cudaMemcpyAsync(h->p0, saved(h, 2), ns * 8, cudaMemcpyDeviceToDevice, o->stream));
+  h->stats = af_imex_stats{};
+  int r = AF_OK;
+  if (stages == 1) {  // stage 1 of one_step
+    h->record = 1;
+    r = update_density(h, 1);
+    if (r == AF_OK) r = set_rho_for_fixed(h, h->rho2);
+    if (r == AF_OK && cudaMemcpyAsync(h->pfix_old, h->p0, ns * 8, cudaMemcpyDeviceToDevice, o->stream) != cudaSuccess)
+      r = ierr(AF_CUDA, "copy failed");
+    if (r == AF_OK && cudaMemcpyAsync(h->ufix, h->u0, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream) != cudaSuccess)
+      r = ierr(AF_CUDA, "copy failed");
+    if (r == AF_OK) r = af_set_HYPERBOLIC_stage(o, 1);
+    if (r == AF_OK) r = fixed_point(h, 1, h->p2, h->u2);
+  } else {
+    h->record = 3;
+    r = one_step(h);
+  }
+  h->record = 0;
+  IM_AF(r);
+  h->lin = stages == 1 ? 1 : 2;
+  return AF_OK;
+}
 extern "C" {
 
 int af_imex_default_options(af_imex_options* opt) {
@@ -716,8 +901,10 @@ int af_imex_destroy(af_imex* h) {
   af_schur_solver_destroy(h->schur);
   cudaFree(h->mem);
   cudaFree(h->adj_mem);
-  for (double* p : h->rec_p) cudaFree(p);
-  for (double* u : h->rec_u) cudaFree(u);
+  for (int k = 0; k < 2; ++k) {
+    for (double* p : h->rec_p[k]) cudaFree(p);
+    for (double* u : h->rec_u[k]) cudaFree(u);
+  }
   af_destroy(h->op);
   delete h;
   return AF_OK;
@@ -728,7 +915,7 @@ af_operator* af_imex_operator(af_imex* h) { return h ? h->op : nullptr; }
 int af_imex_set_state(af_imex* h, const double* rho, const double* u, const double* p) {
   if (!h || !rho || !u || !p) return ierr(AF_BAD_ARG, "null argument");
   cudaStream_t st = h->op->stream;
-  h->rec_iters = 0;  // the stage-1 linearisation point is gone
+  h->lin = 0;  // the recorded linearisation point is gone
   IM_CU(cudaMemcpyAsync(h->rho0, rho, h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(h->u0, u, 2 * h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(h->p0, p, h->ns * 8, cudaMemcpyDeviceToDevice, st));
@@ -749,7 +936,7 @@ int af_imex_get_state(const af_imex* h, double* rho, double* u, double* p) {
 int af_imex_step(af_imex* h, int nsteps) {
   if (!h || nsteps < 0) return ierr(AF_BAD_ARG, "bad argument");
   IM_CU(cudaSetDevice(h->op->device));
-  h->rec_iters = 0;  // the stage-1 linearisation point is gone
+  h->lin = 0;  // the recorded linearisation point is gone
   for (int s = 0; s < nsteps; ++s) {
     h->stats = af_imex_stats{};
     IM_AF(one_step(h));
@@ -762,30 +949,12 @@ int af_imex_stage1_forward(af_imex* h, const double* rho0, const double* u0, con
   if (!h || !rho0 || !u0 || !p0 || !rho2 || !u2 || !p2) return ierr(AF_BAD_ARG, "null argument");
   if (!h->schur) return ierr(AF_UNSUPPORTED, "af_imex_stage1_forward: needs schur_preconditioner >= 0");
   IM_CU(cudaSetDevice(h->op->device));
-  af_operator* o = h->op;
-  const long ns = h->ns;
-  h->rec_iters = 0;
-  IM_CU(cudaMemcpyAsync(h->rho0, rho0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  IM_CU(cudaMemcpyAsync(h->u0, u0, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  IM_CU(cudaMemcpyAsync(h->p0, p0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  h->stats = af_imex_stats{};
-  // stage 1 of one_step, with the fixed-point trajectory recorded
-  IM_AF(update_density(h, 1));
-  IM_AF(set_rho_for_fixed(h, h->rho2));
-  IM_CU(cudaMemcpyAsync(h->pfix_old, h->p0, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  IM_CU(cudaMemcpyAsync(h->ufix, h->u0, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  IM_AF(af_set_HYPERBOLIC_stage(o, 1));
-  h->record = true;
-  const int r = fixed_point(h, 1, h->p2, h->u2);
-  h->record = false;
-  if (r != AF_OK) {
-    h->rec_iters = 0;
-    return r;
-  }
-  IM_CU(cudaMemcpyAsync(rho2, h->rho2, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  IM_CU(cudaMemcpyAsync(u2, h->u2, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  IM_CU(cudaMemcpyAsync(p2, h->p2, ns * 8, cudaMemcpyDeviceToDevice, o->stream));
-  IM_CU(cudaStreamSynchronize(o->stream));
+  IM_AF(recorded_forward(h, rho0, u0, p0, 1));
+  cudaStream_t st = h->op->stream;
+  IM_CU(cudaMemcpyAsync(rho2, h->rho2, h->ns * 8, cudaMemcpyDeviceToDevice, st));
+  IM_CU(cudaMemcpyAsync(u2, h->u2, 2 * h->ns * 8, cudaMemcpyDeviceToDevice, st));
+  IM_CU(cudaMemcpyAsync(p2, h->p2, h->ns * 8, cudaMemcpyDeviceToDevice, st));
+  IM_CU(cudaStreamSynchronize(st));
   return AF_OK;
 }
 
@@ -794,7 +963,9 @@ int af_imex_stage1_tangent(af_imex* h, const double* drho0, const double* du0, c
   if (!h || !drho0 || !du0 || !dp0 || !drho2 || !du2 || !dp2) return ierr(AF_BAD_ARG, "null argument");
   if (!(rel_tol > 0.0)) return ierr(AF_BAD_ARG, "af_imex_stage1_tangent: invalid tolerance");
   IM_CU(cudaSetDevice(h->op->device));
-  return s1_tangent(h, drho0, du0, dp0, drho2, du2, dp2, rel_tol, h->opt.max_iterations);
+  const double* dx[3] = {drho0, du0, dp0};
+  double* dy[3] = {drho2, du2, dp2};
+  return s1_tangent(h, dx, dy, rel_tol, h->opt.max_iterations);
 }
 
 int af_imex_stage1_backward(af_imex* h, const double* rho2bar, const double* u2bar, const double* p2bar,
@@ -802,7 +973,105 @@ int af_imex_stage1_backward(af_imex* h, const double* rho2bar, const double* u2b
   if (!h || !rho2bar || !u2bar || !p2bar || !rho0bar || !u0bar || !p0bar) return ierr(AF_BAD_ARG, "null argument");
   if (!(rel_tol > 0.0)) return ierr(AF_BAD_ARG, "af_imex_stage1_backward: invalid tolerance");
   IM_CU(cudaSetDevice(h->op->device));
-  return s1_backward(h, rho2bar, u2bar, p2bar, rho0bar, u0bar, p0bar, rel_tol, h->opt.max_iterations);
+  const double* yb[3] = {rho2bar, u2bar, p2bar};
+  double* xb[3] = {rho0bar, u0bar, p0bar};
+  return s1_backward(h, yb, xb, rel_tol, h->opt.max_iterations);
+}
+
+int af_imex_step_forward(af_imex* h, const double* rho0, const double* u0, const double* p0, double* rho1, double* u1,
+                         double* p1) {
+  if (!h || !rho0 || !u0 || !p0 || !rho1 || !u1 || !p1) return ierr(AF_BAD_ARG, "null argument");
+  if (!h->schur) return ierr(AF_UNSUPPORTED, "af_imex_step_forward: needs schur_preconditioner >= 0");
+  IM_CU(cudaSetDevice(h->op->device));
+  IM_AF(recorded_forward(h, rho0, u0, p0, 3));
+  IM_AF(af_imex_get_state(h, rho1, u1, p1));
+  return AF_OK;
+}
+
+int af_imex_step_tangent(af_imex* h, const double* drho0, const double* du0, const double* dp0, double* drho1,
+                         double* du1, double* dp1, double rel_tol) {
+  if (!h || !drho0 || !du0 || !dp0 || !drho1 || !du1 || !dp1) return ierr(AF_BAD_ARG, "null argument");
+  if (!(rel_tol > 0.0)) return ierr(AF_BAD_ARG, "af_imex_step_tangent: invalid tolerance");
+  IM_CU(cudaSetDevice(h->op->device));
+  const double* dx[3] = {drho0, du0, dp0};
+  double* dy[3] = {drho1, du1, dp1};
+  return step_tangent(h, dx, dy, rel_tol, h->opt.max_iterations);
+}
+
+int af_imex_step_backward(af_imex* h, const double* rho1bar, const double* u1bar, const double* p1bar,
+                          double* rho0bar, double* u0bar, double* p0bar, double rel_tol) {
+  if (!h || !rho1bar || !u1bar || !p1bar || !rho0bar || !u0bar || !p0bar) return ierr(AF_BAD_ARG, "null argument");
+  if (!(rel_tol > 0.0)) return ierr(AF_BAD_ARG, "af_imex_step_backward: invalid tolerance");
+  IM_CU(cudaSetDevice(h->op->device));
+  const double* yb[3] = {rho1bar, u1bar, p1bar};
+  double* xb[3] = {rho0bar, u0bar, p0bar};
+  return step_backward(h, yb, xb, rel_tol, h->opt.max_iterations);
+}
+
+int af_imex_gradient(af_imex* h, const double* rho0, const double* u0, const double* p0, int nsteps,
+                     int checkpoint_every, const double* rhobar, const double* ubar, const double* pbar,
+                     double* rho0bar, double* u0bar, double* p0bar, double rel_tol) {
+  if (!h || !rho0 || !u0 || !p0 || !rhobar || !ubar || !pbar || !rho0bar || !u0bar || !p0bar)
+    return ierr(AF_BAD_ARG, "null argument");
+  if (nsteps < 1 || checkpoint_every < 1 || !(rel_tol > 0.0)) return ierr(AF_BAD_ARG, "af_imex_gradient: bad argument");
+  if (!h->schur) return ierr(AF_UNSUPPORTED, "af_imex_gradient: needs schur_preconditioner >= 0");
+  IM_CU(cudaSetDevice(h->op->device));
+  af_operator* o = h->op;
+  cudaStream_t st = o->stream;
+  const long ns = h->ns, S = 4 * ns;  // one state: rho, u (2), p
+  const int K = checkpoint_every, nck = (nsteps + K - 1) / K;
+  double* mem = nullptr;
+  // checkpoints, the states of one segment, and the running cotangent (+ a copy)
+  IM_CU(cudaMalloc(&mem, sizeof(double) * S * ((size_t)nck + K + 2)));
+  double* ck = mem;
+  double* seg = ck + (size_t)S * nck;
+  double* bar = seg + (size_t)S * K;
+  double* bar2 = bar + S;
+  auto R = [ns](double* b) { return b; };
+  auto U = [ns](double* b) { return b + ns; };
+  auto Pp = [ns](double* b) { return b + 3 * ns; };
+  int r = AF_OK;
+  auto copy = [&](double* d, const double* s_, long n) {
+    if (r == AF_OK && cudaMemcpyAsync(d, s_, n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      r = ierr(AF_CUDA, "af_imex_gradient: copy failed");
+  };
+  auto save_state = [&](double* b) {
+    if (r == AF_OK) r = af_imex_get_state(h, R(b), U(b), Pp(b));
+  };
+  // forward sweep, one checkpoint every K steps
+  r = af_imex_set_state(h, rho0, u0, p0);
+  for (int n = 0; n < nsteps && r == AF_OK; ++n) {
+    if (n % K == 0) save_state(ck + (size_t)S * (n / K));
+    if (r == AF_OK) r = one_step(h);
+  }
+  copy(R(bar), rhobar, ns);
+  copy(U(bar), ubar, 2 * ns);
+  copy(Pp(bar), pbar, ns);
+  // reverse sweep: recompute each segment's states from its checkpoint, then adjoint steps
+  for (int c = nck - 1; c >= 0 && r == AF_OK; --c) {
+    const int beg = c * K, end = std::min(nsteps, beg + K);
+    double* x = ck + (size_t)S * c;
+    r = af_imex_set_state(h, R(x), U(x), Pp(x));
+    for (int n = beg; n < end && r == AF_OK; ++n) {
+      save_state(seg + (size_t)S * (n - beg));
+      if (r == AF_OK && n + 1 < end) r = one_step(h);
+    }
+    for (int n = end - 1; n >= beg && r == AF_OK; --n) {
+      double* xs = seg + (size_t)S * (n - beg);
+      r = recorded_forward(h, R(xs), U(xs), Pp(xs), 3);
+      if (r != AF_OK) break;
+      const double* yb[3] = {R(bar), U(bar), Pp(bar)};
+      double* xb[3] = {R(bar2), U(bar2), Pp(bar2)};
+      r = step_backward(h, yb, xb, rel_tol, h->opt.max_iterations);
+      std::swap(bar, bar2);
+    }
+  }
+  copy(rho0bar, R(bar), ns);
+  copy(u0bar, U(bar), 2 * ns);
+  copy(p0bar, Pp(bar), ns);
+  cudaStreamSynchronize(st);
+  cudaFree(mem);
+  return r;
 }
 
 int af_imex_last_stats(const af_imex* h, af_imex_stats* out) {

@@ -40,6 +40,11 @@ def _bind():
     L.af_imex_stage1_forward.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.af_imex_stage1_tangent.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
     L.af_imex_stage1_backward.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
+    L.af_imex_step_forward.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.af_imex_step_tangent.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
+    L.af_imex_step_backward.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
+    L.af_imex_gradient.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp,
+                                   ctypes.c_double]
     L._imex_bound = True
     return L
 
@@ -111,6 +116,32 @@ class IMEXStepper:
         r, u, p = self._triple()
         check(_bind().af_imex_stage1_tangent(self._h, _ptr(drho0), _ptr(du0), _ptr(dp0), _ptr(r), _ptr(u), _ptr(p),
                                              rel_tol))
+        return r, u, p
+
+    def step_forward(self, rho0, u0, p0):
+        """One IMEX step from (rho0, u0, p0), recording the linearisation point of step_tangent /
+        step_backward; returns the new state (also the stepper's state)."""
+        r, u, p = self._triple()
+        check(_bind().af_imex_step_forward(self._h, _ptr(rho0), _ptr(u0), _ptr(p0), _ptr(r), _ptr(u), _ptr(p)))
+        return r, u, p
+
+    def step_tangent(self, drho0, du0, dp0, rel_tol=1e-13):
+        r, u, p = self._triple()
+        check(_bind().af_imex_step_tangent(self._h, _ptr(drho0), _ptr(du0), _ptr(dp0), _ptr(r), _ptr(u), _ptr(p),
+                                           rel_tol))
+        return r, u, p
+
+    def step_backward(self, rho1bar, u1bar, p1bar, rel_tol=1e-13):
+        r, u, p = self._triple()
+        check(_bind().af_imex_step_backward(self._h, _ptr(rho1bar), _ptr(u1bar), _ptr(p1bar), _ptr(r), _ptr(u),
+                                            _ptr(p), rel_tol))
+        return r, u, p
+
+    def gradient(self, rho0, u0, p0, nsteps, checkpoint_every, rhobar, ubar, pbar, rel_tol=1e-12):
+        """(d state_N / d state_0)^T (rhobar, ubar, pbar) with checkpointed recomputation."""
+        r, u, p = self._triple()
+        check(_bind().af_imex_gradient(self._h, _ptr(rho0), _ptr(u0), _ptr(p0), nsteps, checkpoint_every,
+                                       _ptr(rhobar), _ptr(ubar), _ptr(pbar), _ptr(r), _ptr(u), _ptr(p), rel_tol))
         return r, u, p
 
     def stage1_backward(self, rho2bar, u2bar, p2bar, rel_tol=1e-13):

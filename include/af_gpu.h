@@ -258,6 +258,25 @@ int af_imex_stage1_tangent(af_imex* h, const double* drho0, const double* du0, c
                            double* du2, double* dp2, double rel_tol);
 int af_imex_stage1_backward(af_imex* h, const double* rho2bar, const double* u2bar, const double* p2bar,
                             double* rho0bar, double* u0bar, double* p0bar, double rel_tol);
+/* The same for one whole IMEX step (stages 1-3, no counterpart in the reference):
+ * (rho0, u0, p0) -> (rho1, u1, p1) = the state after af_imex_step(h, 1) from (rho0, u0, p0);
+ * the forward records both fixed points and leaves (rho1, u1, p1) as the handle's state. */
+int af_imex_step_forward(af_imex* h, const double* rho0, const double* u0, const double* p0, double* rho1, double* u1,
+                         double* p1);
+int af_imex_step_tangent(af_imex* h, const double* drho0, const double* du0, const double* dp0, double* drho1,
+                         double* du1, double* dp1, double rel_tol);
+int af_imex_step_backward(af_imex* h, const double* rho1bar, const double* u1bar, const double* p1bar,
+                          double* rho0bar, double* u0bar, double* p0bar, double rel_tol);
+/* Gradient through nsteps IMEX steps with checkpointed recomputation (no counterpart in the
+ * reference): (rho0bar, u0bar, p0bar) = (d state_N / d state_0)^T (rhobar, ubar, pbar), the
+ * cotangent of a functional of the final state pulled back to the initial state.  The forward
+ * sweep keeps one state every checkpoint_every steps; the reverse sweep recomputes each segment
+ * from its checkpoint and runs af_imex_step_backward step by step (device memory:
+ * ceil(nsteps / checkpoint_every) + checkpoint_every + 2 states).  The handle's state is
+ * overwritten. */
+int af_imex_gradient(af_imex* h, const double* rho0, const double* u0, const double* p0, int nsteps,
+                     int checkpoint_every, const double* rhobar, const double* ubar, const double* pbar,
+                     double* rho0bar, double* u0bar, double* p0bar, double rel_tol);
 
 /* The Schur complement apply D p - C A^{-1} B p of af_vmult (NS_stage 2) for callers that
  * must not allocate device memory (e.g. code inside a framework whose caching allocator owns
