@@ -271,7 +271,9 @@ struct Layout {
   // region E (epilogue policies): the CTA's Gauss-point inverse weights, 16-byte aligned
   static constexpr int EPI = EpiOf<Phys>::value;
   static constexpr int OE = (RA + RB + R_FLUX + R_GEO + R_S + ALIGN - 1) / ALIGN * ALIGN;
-  static constexpr int TOTAL = EPI ? OE + CB * ND : RA + RB + R_FLUX + R_GEO + R_S;
+  // EPI 2 also prefetches the residual, the previous direction and the iterate of its cells
+  static constexpr int NE = EPI == 2 ? 4 : 1;
+  static constexpr int TOTAL = EPI ? OE + NE * CB * ND : RA + RB + R_FLUX + R_GEO + R_S;
   // the epilogue's scratch (input rows and half-transformed values) lives in region A
   static_assert(EPI == 0 || RA >= (NOUT + 1) * CB * ND, "region A too small for the epilogue");
   static constexpr size_t BYTES = sizeof(R) * TOTAL;
@@ -384,21 +386,34 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   if constexpr (L::EPI != 0) {
     const int c0e = mesh.cell0 + blockIdx.x * CB, ncbe = min(CB, ncell - c0e);
     const size_t bytes = sizeof(R) * (size_t)ncbe * ND;
-    const R* srcm = prm.inv + (size_t)c0e * ND;
-    epi_bulk = bytes % 16 == 0 && (reinterpret_cast<size_t>(srcm) & 15) == 0;
+    // the chunks: weights (and for EPI 2: r, din, x), each [cell][node] over the CTA's cells
+    const R* srcs[4] = {prm.inv + (size_t)c0e * ND, nullptr, nullptr, nullptr};
+    if constexpr (L::EPI == 2) {
+      srcs[1] = prm.r + (size_t)c0e * ND;
+      srcs[2] = prm.din + (size_t)c0e * ND;
+      srcs[3] = prm.x + (size_t)c0e * ND;
+    }
+    epi_bulk = bytes % 16 == 0;
+#pragma unroll
+    for (int k = 0; k < L::NE; ++k) epi_bulk = epi_bulk && (reinterpret_cast<size_t>(srcs[k]) & 15) == 0;
     if (epi_bulk) {
       if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_e) : "memory");
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar_e), "r"((unsigned)bytes)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar_e),
+                     "r"((unsigned)(bytes * L::NE))
                      : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                         (unsigned)__cvta_generic_to_shared(s_minv)),
-                     "l"(srcm), "r"((unsigned)bytes), "r"(bar_e)
-                     : "memory");
+#pragma unroll
+        for (int k = 0; k < L::NE; ++k)
+          asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                           (unsigned)__cvta_generic_to_shared(s_minv + k * CB * ND)),
+                       "l"(srcs[k]), "r"((unsigned)bytes), "r"(bar_e)
+                       : "memory");
       }
     } else {
-      for (int e = threadIdx.x; e < ncbe * ND; e += L::NT) cp_async_el(&s_minv[e], srcm + e);
+#pragma unroll
+      for (int k = 0; k < L::NE; ++k)
+        for (int e = threadIdx.x; e < ncbe * ND; e += L::NT) cp_async_el(&s_minv[k * CB * ND + e], srcs[k] + e);
     }
   }
 
@@ -847,9 +862,10 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     const CobT<P, R>& cb = cobr<P, R>();
     if constexpr (L::EPI == 2) {
       R* r = prm.r + (size_t)c0 * ND;
+      const R* s_r = s_minv + CB * ND;  // prefetched residual
       for (int e = tid; e < ncb * ND; e += NT) {
         const int cc = e / ND, k = e % ND;
-        const R rn = r[e] + s_out[cc * L::NDP + k];
+        const R rn = s_r[e] + s_out[cc * L::NDP + k];
         r[e] = rn;
         s_y[cc * ND + k] = rn;
       }
@@ -912,11 +928,12 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         if constexpr (L::EPI == 1) {
           // one output array, NOUT components, [cell][comp][node]
           ptr.out[0][((size_t)(c0 + cc) * NOUT + o) * ND + iz * P1 + ix] = prm.scale * y;
-        } else {
-          const size_t g = (size_t)(c0 + cc) * ND + iz * P1 + ix;
-          const R nd = (prm.alpha != R(0) ? prm.alpha * prm.din[g] : R(0)) + prm.s * y;
+        } else {  // din and x come from the prefetched chunks
+          const int l = cc * ND + iz * P1 + ix;
+          const size_t g = (size_t)c0 * ND + l;
+          const R nd = (prm.alpha != R(0) ? prm.alpha * s_minv[2 * CB * ND + l] : R(0)) + prm.s * y;
           prm.dout[g] = nd;
-          prm.x[g] = prm.first ? nd : prm.x[g] + nd;
+          prm.x[g] = prm.first ? nd : s_minv[3 * CB * ND + l] + nd;
         }
       }
     }
