@@ -138,6 +138,30 @@ class IMEXStepper {
     return s;
   }
 
+  // The forward / backward pair of one step, the role a torch.autograd.Function plays in a
+  // Python code (no counterpart in the reference): forward records the linearisation point,
+  // tangent and backward apply J and J^T there (Schur solves to rel_tol).
+  void step_forward(const double* rho0, const double* u0, const double* p0, double* rho1, double* u1, double* p1) {
+    check(af_imex_step_forward(h_, rho0, u0, p0, rho1, u1, p1), "af_imex_step_forward");
+  }
+  void step_tangent(const double* drho0, const double* du0, const double* dp0, double* drho1, double* du1,
+                    double* dp1, double rel_tol = 1e-12) {
+    check(af_imex_step_tangent(h_, drho0, du0, dp0, drho1, du1, dp1, rel_tol), "af_imex_step_tangent");
+  }
+  void step_backward(const double* rho1bar, const double* u1bar, const double* p1bar, double* rho0bar,
+                     double* u0bar, double* p0bar, double rel_tol = 1e-12) {
+    check(af_imex_step_backward(h_, rho1bar, u1bar, p1bar, rho0bar, u0bar, p0bar, rel_tol), "af_imex_step_backward");
+  }
+  // cotangent of a functional of the state after nsteps, pulled back to (rho0, u0, p0) with
+  // one checkpoint every checkpoint_every steps
+  void gradient(const double* rho0, const double* u0, const double* p0, int nsteps, int checkpoint_every,
+                const double* rhobar, const double* ubar, const double* pbar, double* rho0bar, double* u0bar,
+                double* p0bar, double rel_tol = 1e-12) {
+    check(af_imex_gradient(h_, rho0, u0, p0, nsteps, checkpoint_every, rhobar, ubar, pbar, rho0bar, u0bar, p0bar,
+                           rel_tol),
+          "af_imex_gradient");
+  }
+
  private:
   af_imex* h_ = nullptr;
 };

@@ -1,6 +1,7 @@
 // C++ caller of libaf_gpu.so through include/af_euler_operator.hpp, in the shape of the
 // reference's stage drivers: density rhs -> mass solve, pressure/velocity rhs, Schur solve,
-// a time step; checked against the C ABI called directly and for error reporting.
+// a time step and its forward / tangent / backward pair; checked against the C ABI called
+// directly, by a dot-product test and for error reporting.
 // Built and run by tests/test_gpu_cpp_shim.py.  Prints "OK" on success.
 #include <cuda_runtime.h>
 
@@ -129,6 +130,29 @@ int main() {
   const auto s = stepper.stats();
   REQUIRE(s.fixed_point_iterations[0] >= 1 && s.gmres_iterations > 0);
   for (double v : download(f_p, n)) REQUIRE(std::isfinite(v) && v > 0.0);
+
+  // the step's forward / tangent / backward pair: <J dx, ybar> = <dx, J^T ybar>
+  {
+    std::vector<double> hx(n), hu(2 * n);
+    for (long k = 0; k < n; ++k) hx[k] = std::sin(0.7 * k);
+    for (long k = 0; k < 2 * n; ++k) hu[k] = std::cos(0.3 * k);
+    double *dr = upload(hx), *du = upload(hu), *dp = upload(hx), *yr = upload(hx), *yu = upload(hu), *yp = upload(hx);
+    double *tr = upload(hx), *tu = upload(hu), *tp = upload(hx), *xr = upload(hx), *xu = upload(hu), *xp = upload(hx);
+    stepper.step_forward(d_rho, d_u, d_p, f_rho, f_u, f_p);
+    stepper.step_tangent(dr, du, dp, tr, tu, tp, 1e-12);
+    stepper.step_backward(yr, yu, yp, xr, xu, xp, 1e-12);
+    auto dot = [&](const double* a, const double* b, size_t m, double& scale) {
+      auto x = download(a, m), y = download(b, m);
+      double s = 0;
+      for (size_t k = 0; k < m; ++k) { s += x[k] * y[k]; scale += std::fabs(x[k] * y[k]); }
+      return s;
+    };
+    double s1 = 0, s2 = 0;
+    const double lhs = dot(tr, yr, n, s1) + dot(tu, yu, 2 * n, s1) + dot(tp, yp, n, s1);
+    const double rhs = dot(xr, dr, n, s2) + dot(xu, du, 2 * n, s2) + dot(xp, dp, n, s2);
+    REQUIRE(std::fabs(lhs - rhs) <= 1e-10 * s1);
+    for (double* q : {dr, du, dp, yr, yu, yp, tr, tu, tp, xr, xu, xp}) cudaFree(q);
+  }
   for (double* q : {d_rho, d_u, d_p, r_rho, r_u, r_p, f_rho, f_u, f_p}) cudaFree(q);
   std::printf("OK\n");
   return 0;
