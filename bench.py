@@ -431,12 +431,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    t_total = e0.elapsed_time(e1) * 1e-3
+    t_total = reduce_max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
     launches = op.launch_count() - launches0
-    if world > 1:
-        t = torch.tensor([t_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
     t_step = t_total / args.steps
     dofs = 4 * ns
     value = dofs * world / t_step / 1e9
@@ -455,11 +451,7 @@ def run_ours(args, rank, world, local_rank):
         op.vmult_rhs_fused_host(*out_pin, src_pin)
     e3.record(stream)
     e3.synchronize()
-    t_e2e = e2.elapsed_time(e3) * 1e-3 / K2
-    if world > 1:
-        t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = reduce_max_over_ranks(e2.elapsed_time(e3) * 1e-3 / K2, world, dev)
     h2d = sum(a.nbytes for a in src_pin)
     d2h = sum(a.nbytes for a in out_pin)
     # parity spot check of the e2e outputs against the device outputs
@@ -484,8 +476,11 @@ def run_ours(args, rank, world, local_rank):
     line = None
     if rank == 0:
         # ---- degree sweep (same mesh), device-resident
+        # the sweep, the solver measurements and the CPU baseline belong to the 1-GPU line; at
+        # N > 1 the line carries the replicated apply and its end-to-end time only
+        extras = world == 1
         sweep = {}
-        if not args.no_sweep:
+        if not args.no_sweep and extras:
             for Pd in (2, 3, 4, 5, 6):
                 md, sh = workload(Pd, modes=4)
                 nsd = md.n_cells * (Pd + 1) ** 2
@@ -520,9 +515,9 @@ def run_ours(args, rank, world, local_rank):
         autodiff = {"forward_ms": t_step * 1e3, "tangent_ms": t_tan * 1e3, "backward_ms": t_bwd * 1e3,
                     "backward_over_forward": t_bwd / t_step,
                     "note": "af_vmult_rhs_fused_tangent / _backward on the bench workload (one launch each)"}
-        solvers = {} if args.no_solvers else run_solvers(dev)
+        solvers = {} if (args.no_solvers or not extras) else run_solvers(dev)
         threads = os.cpu_count() or 1
-        cpu_v, cpu_m = cpu_baseline_oracle(64, 3, threads)
+        cpu_v, cpu_m = cpu_baseline_oracle(64, 3, threads) if extras else (None, None)
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64",
@@ -532,11 +527,23 @@ def run_ours(args, rank, world, local_rank):
                         "call": "af_vmult_rhs_fused_host (pinned host buffers)"},
                 "roofline": roofline, "gpu_launches": launches,
                 "clocks": clk.summary(),
-                "cpu_baseline": {"value": cpu_v, "unit": "GDoF/s", "cores": threads, "kind": "port",
-                                 "sample": f"{NX}x64 strip of the workload mesh, best of 3 (1/4 of the work)"},
+                "cpu_baseline": ({"value": cpu_v, "unit": "GDoF/s", "cores": threads, "kind": "port",
+                                  "sample": f"{NX}x64 strip of the workload mesh, best of 3 (1/4 of the work)"}
+                                 if extras else None),
                 "degree_sweep": sweep, "autodiff": autodiff, **solvers}
         print(json.dumps(line), flush=True)
     return line
+
+
+def reduce_max_over_ranks(value, world, device):
+    """The maximum of a per-rank time over all ranks (all ranks call it, in the same order)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_profile_case(kind):
