@@ -647,12 +647,20 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
 
   // ================= merged z pass: member = quadrature column qx =================
   // All groups' fields are evaluated at each point, their integrands summed, and the sum
-  // is mapped to reference coordinates and contracted along z once.
-  R acc_a[NOUT][P1], acc_b[NOUT][P1];
+  // is mapped to reference coordinates and contracted along z once.  The contraction of a
+  // point pair (q, NQ-1-q) goes into even/odd accumulators of the node pairs (i, P-i):
+  //   S terms:  E_i += Se[q][i] (f1 + f2),  O_i += So[q][i] (f1 - f2),  mid += Sm[q] (f1 + f2)
+  //   D terms:  E_i += De[q][i] (g1 - g2),  O_i += Do[q][i] (g1 + g2),  mid += Dm[q] (g1 - g2)
+  // (S[NQ-1-q][i] = S[q][P-i], D[NQ-1-q][i] = -D[q][P-i]); node i gets E_i + O_i, node P-i
+  // gets E_i - O_i.  A middle point is a pair with f2 = g2 = 0.
+  constexpr int HE = H > 0 ? H : 1;
+  R aE[NOUT][HE], aO[NOUT][HE], aM[NOUT], bE[NOUT][HE], bO[NOUT][HE], bM[NOUT];
 #pragma unroll
-  for (int o = 0; o < NOUT; ++o)
+  for (int o = 0; o < NOUT; ++o) {
 #pragma unroll
-    for (int i = 0; i < P1; ++i) acc_a[o][i] = acc_b[o][i] = 0.0;
+    for (int i = 0; i < HE; ++i) aE[o][i] = aO[o][i] = bE[o][i] = bO[o][i] = R(0);
+    aM[o] = bM[o] = R(0);
+  }
   {
     const int qx = m;
     const R* g = s_geo + cl * 24;
@@ -661,7 +669,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     const R J01 = fmaR(g[2], xi, g[4]);  // x_eta (x component)
     const R J11 = fmaR(g[3], xi, g[5]);  // x_eta (z component)
     constexpr int NFG_ALL = PhysInfo<Phys>::NFG_TOTAL;
-    auto point = [&](const R* v, const R* deta, const int qz) {
+    // the mapped integrands of one point: fv (tested with phi), fx, fe (with d/dxi, d/deta phi)
+    auto integrand = [&](const R* v, const R* deta, const int qz, R* fvo, R* fxo, R* feo) {
       const R eta = tb.x[qz];
       const R J00 = fmaR(g[2], eta, g[0]);
       const R J10 = fmaR(g[3], eta, g[1]);
@@ -689,18 +698,9 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       const R a00 = J11 * w, a01 = J01 * w, a10 = J10 * w, a11 = J00 * w;  // adj(J) w
 #pragma unroll
       for (int o = 0; o < NOUT; ++o) {
-        const bool hv = Phys::has_val(o), hg = Phys::has_grad(o);
-        const R fv = val[o] * dw;
-        const R fx = a00 * gr[o][0] - a01 * gr[o][1];
-        const R fe = a11 * gr[o][1] - a10 * gr[o][0];
-#pragma unroll
-        for (int iz = 0; iz < P1; ++iz) {
-          if (hv) acc_a[o][iz] = fmaR(tb.S[qz][iz], fv, acc_a[o][iz]);
-          if (hg) {
-            acc_a[o][iz] = fmaR(tb.D[qz][iz], fe, acc_a[o][iz]);
-            acc_b[o][iz] = fmaR(tb.S[qz][iz], fx, acc_b[o][iz]);
-          }
-        }
+        fvo[o] = val[o] * dw;
+        fxo[o] = a00 * gr[o][0] - a01 * gr[o][1];
+        feo[o] = a11 * gr[o][1] - a10 * gr[o][0];
       }
     };
 #pragma unroll kZUnroll
@@ -743,8 +743,57 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
           }
         });
       }
-      point(v1, d1, k);
-      if (pair) point(v2, d2, NQ - 1 - k);
+      R fv1[NOUT], fx1[NOUT], fe1[NOUT], fv2[NOUT], fx2[NOUT], fe2[NOUT];
+      integrand(v1, d1, k, fv1, fx1, fe1);
+      if (pair) {
+        integrand(v2, d2, NQ - 1 - k, fv2, fx2, fe2);
+      } else {
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) fv2[o] = fx2[o] = fe2[o] = R(0);
+      }
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) {
+        const bool hv = Phys::has_val(o), hg = Phys::has_grad(o);
+        const R se = hv ? fv1[o] + fv2[o] : R(0), so = hv ? fv1[o] - fv2[o] : R(0);
+        const R ge = hg ? fe1[o] - fe2[o] : R(0), go = hg ? fe1[o] + fe2[o] : R(0);
+        const R xe = fx1[o] + fx2[o], xo = fx1[o] - fx2[o];
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+          if (hv) {
+            aE[o][i] = fmaR(tb.Se[k][i], se, aE[o][i]);
+            aO[o][i] = fmaR(tb.So[k][i], so, aO[o][i]);
+          }
+          if (hg) {
+            aE[o][i] = fmaR(tb.De[k][i], ge, aE[o][i]);
+            aO[o][i] = fmaR(tb.Do[k][i], go, aO[o][i]);
+            bE[o][i] = fmaR(tb.Se[k][i], xe, bE[o][i]);
+            bO[o][i] = fmaR(tb.So[k][i], xo, bO[o][i]);
+          }
+        }
+        if (MIDN) {
+          if (hv) aM[o] = fmaR(tb.Sm[k], se, aM[o]);
+          if (hg) {
+            aM[o] = fmaR(tb.Dm[k], ge, aM[o]);
+            bM[o] = fmaR(tb.Sm[k], xe, bM[o]);
+          }
+        }
+      }
+    }
+  }
+  // node values of the accumulators
+  R acc_a[NOUT][P1], acc_b[NOUT][P1];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o) {
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      acc_a[o][i] = aE[o][i] + aO[o][i];
+      acc_a[o][P - i] = aE[o][i] - aO[o][i];
+      acc_b[o][i] = bE[o][i] + bO[o][i];
+      acc_b[o][P - i] = bE[o][i] - bO[o][i];
+    }
+    if (MIDN) {
+      acc_a[o][P / 2] = aM[o];
+      acc_b[o][P / 2] = bM[o];
     }
   }
   __syncthreads();  // region A: x-contracted rows consumed -> accumulators
