@@ -132,3 +132,18 @@ def test_gradient_with_checkpointing():
     jp, _ = J(tuple(a + h * b for a, b in zip(x, dx)))
     jm, _ = J(tuple(a - h * b for a, b in zip(x, dx)))
     assert abs((jp - jm) / (2 * h) - dJ) <= 1e-5 * abs(dJ), ((jp - jm) / (2 * h), dJ)
+
+
+def test_tangent_needs_a_recorded_forward():
+    """The tangent / backward of a step refuse to run before the recorded forward, and after
+    af_imex_step moved the state (the linearisation point is gone)."""
+    from atmospheric_flows_b200.operator import AFError
+    m, g, x = _stepper(2, 1e-10)
+    dx = _dirs(x, 6, 1.0)
+    with pytest.raises(AFError):
+        g.step_tangent(*dx)
+    g.step_forward(*x)
+    g.step_tangent(*dx)  # fine now
+    g.step(1)
+    with pytest.raises(AFError):
+        g.step_backward(*dx)
