@@ -426,11 +426,17 @@ struct Ctx {
   long ns;
   cudaStream_t st;
   int next = kSaved;
-  double* take() { return h->adj_mem + (size_t)(next++) * 2 * ns; }
+  // a velocity-sized work vector; past the pool's end it hands out the last one and the
+  // caller's ws_ok() check fails before any of them is used
+  double* take() {
+    const int k = next < kAdjVectors ? next : kAdjVectors - 1;
+    ++next;
+    return h->adj_mem + (size_t)k * 2 * ns;
+  }
+  bool ws_ok() const { return next <= kAdjVectors; }
 };
 }  // namespace
 
-#define AD_TAKE(c) ((c).next < kAdjVectors ? (c).take() : nullptr)
 
 static int ctx_init(af_imex* h, Ctx& c, int need_lin) {
   if (!h->schur) return ierr(AF_UNSUPPORTED, "tangent/adjoint: needs schur_preconditioner >= 0");
@@ -511,6 +517,7 @@ static int fp_tangent(Ctx& c, int s, const double* const* dE, double* drho_out, 
   double *drhs_p = c.take(), *tmpA = c.take(), *dt = c.take(), *jc = c.take(), *cc = c.take(), *db = c.take();
   double *Bp = c.take(), *w = c.take(), *aw = c.take(), *z = c.take(), *jz = c.take(), *cw = c.take();
   double *dP = c.take(), *dU = c.take(), *dPf = c.take(), *dUf = c.take(), *drho = c.take(), *bdp = c.take();
+  if (!c.ws_ok()) return ierr(AF_BAD_ARG, "tangent: work vectors exhausted");
   IM_AF(ad_zero(c, zs, ns));
   IM_AF(ad_zero(c, zv, 2 * ns));
   const double* su[8];
@@ -592,6 +599,7 @@ static int fp_backward(Ctx& c, int s, const double* rho_bar, const double* u_bar
   double *dtb = c.take(), *rrb = c.take();
   double* xb[11];
   for (int j = 0; j < n; ++j) xb[j] = c.take();
+  if (!c.ws_ok()) return ierr(AF_BAD_ARG, "adjoint: work vectors exhausted");
   IM_AF(ad_zero(c, zs, ns));
   IM_AF(ad_zero(c, zv, 2 * ns));
   IM_AF(ad_copy(c, R2, rho_bar, ns));
@@ -669,6 +677,7 @@ static int s3_tangent(Ctx& c, const double* const* dE, double* drc, double* duc,
   IM_AF(stage_setup(c, 3, h->rhoc));
   const int mark = c.next;
   double *zs = c.take(), *zv = c.take(), *drr = c.take(), *dru = c.take(), *drp = c.take(), *tmpA = c.take();
+  if (!c.ws_ok()) return ierr(AF_BAD_ARG, "tangent: work vectors exhausted");
   IM_AF(ad_zero(c, zs, ns));
   IM_AF(ad_zero(c, zv, 2 * ns));
   const double* src[11];
@@ -704,6 +713,7 @@ static int s3_backward(Ctx& c, const double* rc_bar, const double* uc_bar, const
   double *rub = c.take(), *ts = c.take(), *rrb = c.take();
   double* xb[11];
   for (int j = 0; j < 11; ++j) xb[j] = c.take();
+  if (!c.ws_ok()) return ierr(AF_BAD_ARG, "adjoint: work vectors exhausted");
   IM_AF(ad_zero(c, zs, ns));
   IM_AF(ad_zero(c, zv, 2 * ns));
   const double* src[11];
@@ -1027,7 +1037,7 @@ int af_imex_gradient(af_imex* h, const double* rho0, const double* u0, const dou
   double* seg = ck + (size_t)S * nck;
   double* bar = seg + (size_t)S * K;
   double* bar2 = bar + S;
-  auto R = [ns](double* b) { return b; };
+  auto R = [](double* b) { return b; };
   auto U = [ns](double* b) { return b + ns; };
   auto Pp = [ns](double* b) { return b + 3 * ns; };
   int r = AF_OK;
