@@ -76,7 +76,7 @@ def _smooth_direction(m, P):
     return (d(other.rho - base.rho), d(other.u - base.u), d(other.p - base.p))
 
 
-@pytest.mark.parametrize("P", [2, 3])
+@pytest.mark.parametrize("P", [2, 3, 4])
 def test_step_dot_product(P):
     """A whole IMEX step (both fixed points, stage 3): dot product to 1e-12 of its scale
     (5.6e-16 measured at p = 2)."""
