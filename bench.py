@@ -343,7 +343,7 @@ def run_solvers(dev):
         "grad_norms": [float(torch.linalg.norm(v)) for v in gb],
     }
     del ga, gb
-    # ---- production size (BASELINE cfg 5's mesh): periodic hill 2048x512, p = 4, 104.9 M DoFs,
+    # ---- production size: periodic hill 2048x512, p = 4, 104.9 M DoFs,
     #      dt 0.125 s, eps 1e-8, one warm-up and two timed steps per precision
     pm = M.hill_mesh(2048, 512, periodic_x=True)
     pst = M.hill_state(pm, P, seed=SEED, modes=4)
