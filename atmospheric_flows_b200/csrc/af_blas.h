@@ -7,6 +7,11 @@ namespace af {
 
 constexpr int kMaxPartials = 1184;  // 8 x 148 SMs
 
+// Leading dimension of a stored Krylov basis of length-n FP64 vectors: n rounded up to even,
+// so that every basis vector starts on a 16-byte boundary (the operator entry points and the
+// cell kernel's bulk copies need that) when n is odd, e.g. 1 x 3 cells at degree 4.
+constexpr long krylov_stride(long n) { return (n + 1) & ~1L; }
+
 // Device-resident Krylov scalars.  status: 0 ok, 1 iteration cap, 2 breakdown, 3 NaN/Inf.
 struct KrylovState {
   double rr, rz, rr0, tol2, pAp, alpha, beta;

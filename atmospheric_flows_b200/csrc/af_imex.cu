@@ -125,6 +125,7 @@ static int gmres_solve(af_imex* h, const Apply& A, const double* invd, double* x
                        int* its_out) {
   cudaStream_t st = h->op->stream;
   const int m = h->opt.gmres_restart;
+  const long ld = krylov_stride(n);  // basis vectors start on 16-byte boundaries
   int total = 0;
   std::vector<double> H((m + 1) * m), cs(m), sn(m), g(m + 1), hh(2 * (m + 1));
   auto Hs = [&](int i, int j) -> double& { return H[i * m + j]; };
@@ -149,14 +150,14 @@ static int gmres_solve(af_imex* h, const Apply& A, const double* invd, double* x
     g[0] = beta;
     int jend = -1;
     for (int j = 0; j < m; ++j) {
-      double* w = h->V + (long)(j + 1) * n;
-      IM_AF(A(h->V + (long)j * n, w));
+      double* w = h->V + (long)(j + 1) * ld;
+      IM_AF(A(h->V + (long)j * ld, w));
       IM_CU(dmul(invd, w, w, n, st));
       // classical Gram-Schmidt, twice
-      IM_CU(mdot(h->V, n, j + 1, w, n, h->part, h->d_h, st));
-      IM_CU(maxpy(h->V, n, j + 1, h->d_h, w, n, st));
-      IM_CU(mdot(h->V, n, j + 1, w, n, h->part, h->d_h + (m + 1), st));
-      IM_CU(maxpy(h->V, n, j + 1, h->d_h + (m + 1), w, n, st));
+      IM_CU(mdot(h->V, ld, j + 1, w, n, h->part, h->d_h, st));
+      IM_CU(maxpy(h->V, ld, j + 1, h->d_h, w, n, st));
+      IM_CU(mdot(h->V, ld, j + 1, w, n, h->part, h->d_h + (m + 1), st));
+      IM_CU(maxpy(h->V, ld, j + 1, h->d_h + (m + 1), w, n, st));
       IM_CU(dot(w, nullptr, n, h->part, h->scal, st));
       IM_CU(cudaMemcpyAsync(hh.data(), h->d_h, sizeof(double) * 2 * (m + 1), cudaMemcpyDeviceToHost, st));
       double hn2 = 0.0;
@@ -194,7 +195,7 @@ static int gmres_solve(af_imex* h, const Apply& A, const double* invd, double* x
       for (int l = i + 1; l < k; ++l) s -= Hs(i, l) * y[l];
       y[i] = s / Hs(i, i);
     }
-    IM_CU(mcombine(h->V, n, k, y.data(), x, n, st));
+    IM_CU(mcombine(h->V, ld, k, y.data(), x, n, st));
     h->op->launches += 1;
     if (res <= tol) { converged = true; break; }
     if (total >= h->opt.max_iterations) break;
@@ -858,7 +859,8 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   // scalar vectors: rho0 rho2 rho3 rhoc p0 p2 p3 pfix pfix_old rhs_rho rhs_p tmpp invd_M invd_D gw = 15
   // velocity vectors (2 ns): u0 u2 u3 uc ufix rhs_u tmp1 tmpu cg_r cg_z cg_p cg_Ap invd_u = 13
   r = AF_OK;
-  const long total = 15 * ns + 13 * 2 * ns + (long)(m + 1) * ns + 2 * (m + 1) + 8 + 4 * kMaxPartials + 16;
+  const long total = 15 * (ns + 1) + 13 * 2 * ns + (long)(m + 1) * krylov_stride(ns) + 2 * (m + 1) + 8 +
+                     4 * kMaxPartials + 16;
   if (cudaMalloc(&h->mem, total * sizeof(double)) != cudaSuccess) {
     af_destroy(h->op);
     delete h;
@@ -878,7 +880,7 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
   h->rhs_u = take(2 * ns); h->tmp1 = take(2 * ns); h->tmpu = take(2 * ns);
   h->cg_r = take(2 * ns); h->cg_z = take(2 * ns); h->cg_p = take(2 * ns); h->cg_Ap = take(2 * ns);
   h->invd_u = take(2 * ns);
-  h->V = take((long)(m + 1) * ns);
+  h->V = take((long)(m + 1) * krylov_stride(ns));
   h->d_h = take(2 * (m + 1));
   h->scal = take(8);
   h->part = take(4 * kMaxPartials);
@@ -1028,7 +1030,8 @@ int af_imex_gradient(af_imex* h, const double* rho0, const double* u0, const dou
   IM_CU(cudaSetDevice(h->op->device));
   af_operator* o = h->op;
   cudaStream_t st = o->stream;
-  const long ns = h->ns, S = 4 * ns;  // one state: rho, u (2), p
+  // one state: rho, u (2), p, each part starting on a 16-byte boundary
+  const long ns = h->ns, sp = krylov_stride(ns), S = 4 * sp;
   const int K = checkpoint_every, nck = (nsteps + K - 1) / K;
   double* mem = nullptr;
   // checkpoints, the states of one segment, and the running cotangent (+ a copy)
@@ -1038,8 +1041,8 @@ int af_imex_gradient(af_imex* h, const double* rho0, const double* u0, const dou
   double* bar = seg + (size_t)S * K;
   double* bar2 = bar + S;
   auto R = [](double* b) { return b; };
-  auto U = [ns](double* b) { return b + ns; };
-  auto Pp = [ns](double* b) { return b + 3 * ns; };
+  auto U = [sp](double* b) { return b + sp; };
+  auto Pp = [sp](double* b) { return b + 3 * sp; };
   int r = AF_OK;
   auto copy = [&](double* d, const double* s_, long n) {
     if (r == AF_OK && cudaMemcpyAsync(d, s_, n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)

@@ -500,8 +500,9 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
   if ((r = alloc(s, (void**)&s->part, sizeof(double) * 4 * kMaxPartials)) != AF_OK) return cleanup(r);
   if ((r = alloc(s, (void**)&s->scal, sizeof(double) * 8)) != AF_OK) return cleanup(r);
   if ((r = alloc(s, (void**)&s->dh, sizeof(double) * 2 * (o.restart + 1))) != AF_OK) return cleanup(r);
-  if ((r = alloc(s, (void**)&s->V, sizeof(double) * ns0 * (o.restart + 1))) != AF_OK) return cleanup(r);
-  if ((r = alloc(s, (void**)&s->Z, sizeof(double) * ns0 * o.restart)) != AF_OK) return cleanup(r);
+  const long ld0 = krylov_stride(ns0);
+  if ((r = alloc(s, (void**)&s->V, sizeof(double) * ld0 * (o.restart + 1))) != AF_OK) return cleanup(r);
+  if ((r = alloc(s, (void**)&s->Z, sizeof(double) * ld0 * o.restart)) != AF_OK) return cleanup(r);
   if ((r = alloc(s, (void**)&s->gw, sizeof(double) * ns0)) != AF_OK) return cleanup(r);
   if (o.preconditioner == AF_SCHUR_JACOBI) {
     if ((r = alloc(s, (void**)&s->invd, sizeof(double) * ns0)) != AF_OK) return cleanup(r);
@@ -611,6 +612,7 @@ int fgmres(af_schur_solver* s, const Apply& A, double* x, const double* b, doubl
   af_operator* o = s->op;
   cudaStream_t st = o->stream;
   const long n = o->n_scalar();
+  const long ld = krylov_stride(n);  // basis vectors start on 16-byte boundaries
   const int m = s->opt.restart;
   cudaEvent_t e0, e1;
   MG_CU(cudaEventCreate(&e0));
@@ -648,14 +650,14 @@ int fgmres(af_schur_solver* s, const Apply& A, double* x, const double* b, doubl
     g[0] = beta;
     int jend = -1;
     for (int j = 0; j < m; ++j) {
-      double* zj = s->Z + (long)j * n;
-      double* w = s->V + (long)(j + 1) * n;
-      MG_AF(precondition(s, zj, s->V + (long)j * n));
+      double* zj = s->Z + (long)j * ld;
+      double* w = s->V + (long)(j + 1) * ld;
+      MG_AF(precondition(s, zj, s->V + (long)j * ld));
       MG_AF(A(w, zj));
-      MG_CU(mdot(s->V, n, j + 1, w, n, s->part, s->dh, st));
-      MG_CU(maxpy(s->V, n, j + 1, s->dh, w, n, st));
-      MG_CU(mdot(s->V, n, j + 1, w, n, s->part, s->dh + (m + 1), st));
-      MG_CU(maxpy(s->V, n, j + 1, s->dh + (m + 1), w, n, st));
+      MG_CU(mdot(s->V, ld, j + 1, w, n, s->part, s->dh, st));
+      MG_CU(maxpy(s->V, ld, j + 1, s->dh, w, n, st));
+      MG_CU(mdot(s->V, ld, j + 1, w, n, s->part, s->dh + (m + 1), st));
+      MG_CU(maxpy(s->V, ld, j + 1, s->dh + (m + 1), w, n, st));
       MG_CU(dot(w, nullptr, n, s->part, s->scal, st));
       MG_CU(cudaMemcpyAsync(hh.data(), s->dh, sizeof(double) * 2 * (m + 1), cudaMemcpyDeviceToHost, st));
       double hn2 = 0.0;
@@ -691,7 +693,7 @@ int fgmres(af_schur_solver* s, const Apply& A, double* x, const double* b, doubl
       for (int l = i + 1; l < kk; ++l) sum -= Hs(i, l) * y[l];
       y[i] = sum / Hs(i, i);
     }
-    MG_CU(mcombine(s->Z, n, kk, y.data(), x, n, st));
+    MG_CU(mcombine(s->Z, ld, kk, y.data(), x, n, st));
     o->launches += 1;
   }
   MG_CU(cudaEventRecord(e1, st));

@@ -23,7 +23,16 @@ def _meshes():
         "hill": M.jitter_mesh(M.hill_mesh(10, 5), 0.15, seed=11),
         "hill_periodic": M.hill_mesh(9, 4, periodic_x=True),
         "annulus": M.annulus_mesh(24, 3, r0=6.37122e6, r1=6.37122e6 + 16e3),
+        # edge cases: a single cell; one column (both lateral faces are walls); one column
+        # that is its own periodic neighbour; two periodic cells (both lateral neighbours are
+        # the other cell); every block of cells per CTA is a partial one
+        "box_1x1": M.box_mesh(1, 1, -500.0, 500.0, 0.0, 1000.0),
+        "column_1x3": M.hill_mesh(1, 3),
+        "self_periodic_1x2": M.hill_mesh(1, 2, periodic_x=True),
+        "periodic_2x1": M.hill_mesh(2, 1, periodic_x=True),
     }
+
+TINY = ["box_1x1", "column_1x3", "self_periodic_1x2", "periodic_2x1"]
 
 
 def _setup(name, P, seed=5):
@@ -64,7 +73,7 @@ def _srcs(states, stage, kind):
 
 
 @pytest.mark.parametrize("P", DEGREES)
-@pytest.mark.parametrize("name", ["hill", "hill_periodic", "annulus"])
+@pytest.mark.parametrize("name", ["hill", "hill_periodic", "annulus"] + TINY)
 def test_rhs_parity(P, name):
     m, g, o, states = _setup(name, P)
     ns = m.n_cells * (P + 1) ** 2
@@ -82,9 +91,9 @@ def test_rhs_parity(P, name):
             assert err < TOL, (stage, kind, err)
 
 
-@pytest.mark.parametrize("P", [2, 4, 6])
-def test_fused_triple_and_host_path(P):
-    m, g, o, states = _setup("hill", P)
+@pytest.mark.parametrize("P,name", [(2, "hill"), (4, "hill"), (6, "hill")] + [(P, t) for t in TINY for P in (1, 4)])
+def test_fused_triple_and_host_path(P, name):
+    m, g, o, states = _setup(name, P)
     ns = m.n_cells * (P + 1) ** 2
     for stage in (1, 2, 3):
         g.set_HYPERBOLIC_stage(stage)
@@ -101,7 +110,7 @@ def test_fused_triple_and_host_path(P):
 
 
 @pytest.mark.parametrize("P", DEGREES)
-@pytest.mark.parametrize("name", ["hill", "annulus"])
+@pytest.mark.parametrize("name", ["hill", "annulus"] + TINY)
 def test_implicit_parity(P, name):
     m, g, o, states = _setup(name, P)
     ns = m.n_cells * (P + 1) ** 2
@@ -140,12 +149,12 @@ def test_implicit_parity(P, name):
         assert rel(_h(dst), o.vmult(p)) < 1e-10
 
 
-@pytest.mark.parametrize("P", [1, 2, 4, 6])
-def test_exact_inverse_and_schur_mode(P):
+@pytest.mark.parametrize("P,name", [(1, "hill"), (2, "hill"), (4, "hill"), (6, "hill")] + [(P, t) for t in TINY for P in (1, 4)])
+def test_exact_inverse_and_schur_mode(P, name):
     """af_vmult_inverse inverts the mass-type operators to rounding (checked against the
     oracle's forward operators), and the Schur apply with the exact cell-wise A^{-1} agrees
     with the reference's nested-CG form."""
-    m, g, o, states = _setup("hill", P)
+    m, g, o, states = _setup(name, P)
     ns = m.n_cells * (P + 1) ** 2
     rng = np.random.default_rng(11)
     for op in (g, o):
