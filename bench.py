@@ -598,6 +598,61 @@ def run_profile_case(kind):
     torch.cuda.synchronize()
 
 
+def run_timeline():
+    """One warm IMEX step (periodic 512x256 hill, degree 4, dt 0.5 s, eps 1e-8) with the mixed
+    and the FP64 solver, recorded by the CUDA activity tracer of torch.profiler: the device
+    time of every kernel and copy in the step, the span from the first start to the last end,
+    the busy time (union of the intervals), the idle gaps between them, and the kernels with
+    the most device time.  Warm-cache and in-stream, unlike an ncu launch list.  Prints one
+    JSON object; the tracer's own overhead makes the step a little longer than in the
+    timed bench."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    from atmospheric_flows_b200 import mesh as M
+    from atmospheric_flows_b200.imex import IMEXStepper
+    sc = M.Scaling()
+    m = M.hill_mesh(512, 256, periodic_x=True)
+    st = M.hill_state(m, DEGREE, seed=SEED, modes=4)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    out = {"config": "periodic hill 512x256, degree 4, dt=0.5 s, eps=1e-8, one warm step after one warm-up step"}
+    for label, pc in (("mixed", "cheb_fp32"), ("fp64", "jacobi")):
+        g = IMEXStepper(m, DEGREE, sc.Ma, sc.Fr, 0.5, eps=1e-8, schur_preconditioner=pc)
+        g.set_state(d(st.rho), d(st.u), d(st.p))
+        g.step(1)
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            g.step(1)
+            torch.cuda.synchronize()
+        iv = sorted((e.time_range.start, e.time_range.end, e.name) for e in prof.events()
+                    if e.device_type == torch.autograd.DeviceType.CUDA)
+        busy, cs, ce = 0.0, None, None
+        for s0, e0, _ in iv:
+            if ce is None or s0 > ce:
+                busy += 0.0 if ce is None else ce - cs
+                cs, ce = s0, e0
+            else:
+                ce = max(ce, e0)
+        busy += 0.0 if ce is None else ce - cs
+        gaps = np.array([iv[i + 1][0] - iv[i][1] for i in range(len(iv) - 1)])
+        agg = {}
+        for s0, e0, name in iv:
+            a = agg.setdefault(name, [0, 0.0])
+            a[0] += 1
+            a[1] += e0 - s0
+        span = iv[-1][1] - iv[0][0]
+        top = sorted(agg.items(), key=lambda kv: -kv[1][1])[:12]
+        out[label] = {
+            "device_events": len(iv), "span_ms": span / 1e3, "busy_ms": busy / 1e3,
+            "idle_ms": float(gaps[gaps > 0].sum()) / 1e3, "gap_median_us": float(np.median(gaps)),
+            "gaps_over_20us": int((gaps > 20).sum()),
+            "top": [{"kernel": k[:160], "launches": v[0], "total_ms": round(v[1] / 1e3, 3),
+                     "per_launch_us": round(v[1] / v[0], 1), "share": round(v[1] / busy, 4)} for k, v in top],
+        }
+        del g
+        torch.cuda.synchronize()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -608,9 +663,14 @@ def main():
     ap.add_argument("--no-solvers", action="store_true", help="skip the Schur-solve and IMEX-step measurements")
     ap.add_argument("--profile", choices=["rhs", "adjoint", "schur", "imex"],
                     help="run one workload briefly for an ncu capture and exit (no measurement)")
+    ap.add_argument("--timeline", action="store_true",
+                    help="trace one warm IMEX step (mixed and FP64) and print its kernel timeline summary")
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args.profile)
+        return
+    if args.timeline:
+        run_timeline()
         return
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
