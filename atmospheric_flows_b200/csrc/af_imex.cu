@@ -895,10 +895,10 @@ int af_imex_create(const af_mesh_desc* mesh, int degree, double Ma, double Fr, d
     af_schur_default_options(&so);
     so.preconditioner = o.schur_preconditioner;
     so.restart = o.gmres_restart;
-    // inside the time loop each solve starts from the previous iterate: a lower degree than
-    // the stand-alone default measured best (512x256 and 1024x256, degrees 4..16; 10 and 12
-    // tie at 512x256, 12 is 6 % faster at 1024x256)
-    so.poly_degree = o.schur_poly_degree > 0 ? o.schur_poly_degree : 12;
+    // degree 20 measured best over the periodic hill steps at 512x256 (dt 0.5 s) and 1024x256
+    // (dt 0.25 s), eps 1e-8 and 1e-10, degrees 8..24: 2.4 % less time in sum than degree 12,
+    // 4 % and 8 % at 512x256, within 2 % either way at 1024x256
+    so.poly_degree = o.schur_poly_degree > 0 ? o.schur_poly_degree : 20;
     r = af_schur_solver_create(h->op, &so, &h->schur);
   }
   if (r == AF_OK) r = af_synchronize(h->op);

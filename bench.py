@@ -378,7 +378,7 @@ def run_solvers(dev):
     out["imex"] = {
         "config": f"periodic hill {nx}x{nz}, degree {P}, dt={dt} s, 1 warm-up + {nsteps} timed steps; "
                   "fp64: Schur FGMRES + Jacobi (FP64); mixed: Schur FGMRES (FP64) + FP32 Chebyshev polynomial "
-                  "preconditioner (degree 12, cell inverses by change of basis), both to |b - S p| <= eps |b|; "
+                  "preconditioner (degree 20, cell inverses by change of basis), both to |b - S p| <= eps |b|; "
                   "reference_criterion: the reference's left-Jacobi GMRES stopping on |D^-1 r| <= eps |b| (a "
                   "looser criterion, shown for scale)",
         "eps": 1e-8,

@@ -221,7 +221,7 @@ typedef struct {
   int schur_preconditioner;        /* -1: the reference's GMRES + left Jacobi (default);
                                       AF_SCHUR_*: af_schur_solve (FGMRES, true residual <= eps |rhs_p|,
                                       preconditioner rebuilt once per stage) */
-  int schur_poly_degree;           /* AF_SCHUR_CHEB_*: polynomial degree (0: 12)                 */
+  int schur_poly_degree;           /* AF_SCHUR_CHEB_*: polynomial degree (0: 20)                 */
 } af_imex_options;
 typedef struct {
   int fixed_point_iterations[2];   /* stage 1, stage 2 of the last step                   */
