@@ -64,6 +64,8 @@ struct NfgOf<Phys, std::void_t<decltype(Phys::nfg_of(0))>> {
 //   2: the Chebyshev step on a residual increment y:  r += y;  d' = alpha d + s M_K^{-1} r;
 //      x = d' (first) or x += d'   (prm.r, prm.din, prm.dout, prm.x).  d' goes to its own
 //      array: other CTAs still read d's face nodes when the operator's input is d.
+//   3: the Chebyshev step on a preconditioned residual z (prm.r holds z):
+//      z' = z + g M_K^{-1} y - d;  d' = alpha d + s z';  x = d' (first) or x += d'.
 // The CTA's weights are brought in by a bulk copy issued at kernel start.
 template <class Phys, class = void>
 struct EpiOf {
@@ -271,8 +273,9 @@ struct Layout {
   // region E (epilogue policies): the CTA's Gauss-point inverse weights, 16-byte aligned
   static constexpr int EPI = EpiOf<Phys>::value;
   static constexpr int OE = (RA + RB + R_FLUX + R_GEO + R_S + ALIGN - 1) / ALIGN * ALIGN;
-  // EPI 2 also prefetches the residual, the previous direction and the iterate of its cells
-  static constexpr int NE = EPI == 2 ? 4 : 1;
+  // EPI 2 and 3 also prefetch the residual (or z), the previous direction and the iterate of
+  // their cells
+  static constexpr int NE = EPI >= 2 ? 4 : 1;
   static constexpr int TOTAL = EPI ? OE + NE * CB * ND : RA + RB + R_FLUX + R_GEO + R_S;
   // the epilogue's scratch (input rows and half-transformed values) lives in region A
   static_assert(EPI == 0 || RA >= (NOUT + 1) * CB * ND, "region A too small for the epilogue");
@@ -386,9 +389,9 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   if constexpr (L::EPI != 0) {
     const int c0e = mesh.cell0 + blockIdx.x * CB, ncbe = min(CB, ncell - c0e);
     const size_t bytes = sizeof(R) * (size_t)ncbe * ND;
-    // the chunks: weights (and for EPI 2: r, din, x), each [cell][node] over the CTA's cells
+    // the chunks: weights (and for EPI 2, 3: r, din, x), each [cell][node] over the CTA's cells
     const R* srcs[4] = {prm.inv + (size_t)c0e * ND, nullptr, nullptr, nullptr};
-    if constexpr (L::EPI == 2) {
+    if constexpr (L::EPI >= 2) {
       srcs[1] = prm.r + (size_t)c0e * ND;
       srcs[2] = prm.din + (size_t)c0e * ND;
       srcs[3] = prm.x + (size_t)c0e * ND;
@@ -977,6 +980,15 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         if constexpr (L::EPI == 1) {
           // one output array, NOUT components, [cell][comp][node]
           ptr.out[0][((size_t)(c0 + cc) * NOUT + o) * ND + iz * P1 + ix] = prm.scale * y;
+        } else if constexpr (L::EPI == 3) {  // z, din and x come from the prefetched chunks
+          const int l = cc * ND + iz * P1 + ix;
+          const size_t g = (size_t)c0 * ND + l;
+          const R dl = s_minv[2 * CB * ND + l];
+          const R zn = s_minv[CB * ND + l] + prm.g * y - dl;
+          const R nd = prm.alpha * dl + prm.s * zn;
+          prm.r[g] = zn;
+          prm.dout[g] = nd;
+          prm.x[g] = prm.first ? nd : s_minv[3 * CB * ND + l] + nd;
         } else {  // din and x come from the prefetched chunks
           const int l = cc * ND + iz * P1 + ix;
           const size_t g = (size_t)c0 * ND + l;

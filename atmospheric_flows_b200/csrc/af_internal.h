@@ -123,6 +123,12 @@ struct DegreeOps {
                              double* const* dy, const RhsParams&, int ncell, cudaStream_t);
   cudaError_t (*rhs_adjoint)(const MeshDev&, int stage, const double* const* in, const double* const* ybar,
                              double* const* xbar, double* scratch, const RhsParams&, int ncell, cudaStream_t);
+  // the smoother step on the preconditioned residual z = D^{-1} r, D^{-1} = g M_W^{-1}:
+  //   z += g M_W^{-1} C0 w - din;  dout = alpha din + s z;  x = dout (first) or x += dout.
+  // prm.g1 is unused (no D term in the kernel); reduced != 0 selects P+1 Gauss points.
+  cudaError_t (*res_chebz_f)(const MeshDev&, const float* w, const float* pf, const float* din,
+                             const CParamsT<float>&, const float* WM, float g, float alpha, float s, float* z,
+                             float* dout, float* x, int first, int reduced, int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

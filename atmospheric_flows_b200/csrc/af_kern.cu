@@ -990,6 +990,36 @@ cudaError_t res_cheb_fr(const MeshDev& mesh, const float* w, const float* pf, co
   return launch_cellop<P, ResChebRPhys<float>, kFusedCB, kResChebMinB>(mesh, a, q, ncell, st);
 }
 
+// the smoother step on the preconditioned residual z (ResChebZPhys): the kernel evaluates C0 w
+// alone; full (2P+1) or reduced (P+1) Gauss points per direction
+template <class Phys>
+cudaError_t res_chebz_launch(const MeshDev& mesh, const float* w, const float* pf, const float* din,
+                             const CParamsT<float>& prm, const float* WM, float g, float alpha, float s, float* z,
+                             float* dout, float* x, int first, int ncell, cudaStream_t st) {
+  if (din == dout) return cudaErrorInvalidValue;
+  ArgPtrs<2, 1, float> a{{w, pf}, {z}};
+  ResChebZParams<float> q;
+  static_cast<CParamsT<float>&>(q) = prm;
+  q.inv = WM;
+  q.g = g;
+  q.alpha = alpha;
+  q.s = s;
+  q.r = z;
+  q.din = din;
+  q.dout = dout;
+  q.x = x;
+  q.first = first;
+  return launch_cellop<P, Phys, kFusedCB, kResChebMinB>(mesh, a, q, ncell, st);
+}
+cudaError_t res_chebz_f(const MeshDev& mesh, const float* w, const float* pf, const float* din,
+                        const CParamsT<float>& prm, const float* WM, float g, float alpha, float s, float* z,
+                        float* dout, float* x, int first, int reduced, int ncell, cudaStream_t st) {
+  return reduced ? res_chebz_launch<ResChebZRPhys<float>>(mesh, w, pf, din, prm, WM, g, alpha, s, z, dout, x, first,
+                                                          ncell, st)
+                 : res_chebz_launch<ResChebZPhys<float>>(mesh, w, pf, din, prm, WM, g, alpha, s, z, dout, x, first,
+                                                         ncell, st);
+}
+
 cudaError_t op_A_rho_T(const MeshDev& mesh, const double* x, const double* y, double* rhobar, int ncell,
                        cudaStream_t st) {
   ArgPtrs<2, 1> a{{x, y}, {rhobar}};
@@ -1039,7 +1069,8 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         res_cheb<float>,   mg_res_fr,
                         b_inv_fr,          res_cheb_fr,
                         op_A_rho_T,        op_C_pf_T,
-                        rhs_tangent,       rhs_adjoint};
+                        rhs_tangent,       rhs_adjoint,
+                        res_chebz_f};
 
 }  // namespace
 

@@ -131,6 +131,13 @@ __global__ void k_normalize(const R* x, R* y, long n, const double* __restrict__
   if (i < n) y[i] = (R)((double)x[i] / sqrt(nrm2[0]));
 }
 
+// y = a x
+template <class R>
+__global__ void k_scale_to(const R* __restrict__ x, R a, R* __restrict__ y, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * x[i];
+}
+
 constexpr int kNormBlocks = 592;  // 4 x 148 SMs
 
 template <class R>
@@ -248,6 +255,13 @@ struct Prec<float> {
     CParamsT<float> q{(float)cdt, (float)kG1, (float)kGG};
     return (rq ? k->res_cheb_fr : k->res_cheb_f)(m, w, pf, din, q, LM, (float)a, (float)s, r, dout, x, 0, nc, st);
   }
+  // the same step on z = D^{-1} r:  z += g M^{-1} C0 w - din;  dout = a din + s z;  x += dout
+  static cudaError_t res_chebz(const DegreeOps* k, const MeshDev& m, const float* w, const float* pf,
+                               const float* din, double cdt, const float* LM, double g, double a, double s, float* z,
+                               float* dout, float* x, int nc, cudaStream_t st, bool rq) {
+    CParamsT<float> q{(float)cdt, (float)kG1, (float)kGG};
+    return k->res_chebz_f(m, w, pf, din, q, LM, (float)g, (float)a, (float)s, z, dout, x, 0, rq ? 1 : 0, nc, st);
+  }
   static cudaError_t prolong(const DegreeOps* k, const float* xc, float* xf, int nxc, int nzc, cudaStream_t st) {
     return k->prolong_f(xc, xf, nxc, nzc, st);
   }
@@ -288,6 +302,32 @@ int chebyshev(af_schur_solver* s, Level& L, int degree, double lo, double hi, bo
   const R* b = (const R*)L.b;
   const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
   const double ginv = 1.0 / kG1;  // D^{-1} = (gamma-1) M^{-1}
+  if constexpr (Prec<R>::kFused) {
+    if (zero_init && !final_residual) {
+      // FP32 levels, no residual wanted afterwards: carry z = D^{-1} r instead of r.  The
+      // cell inverse of D is exact for the level's D, so z' = z + D^{-1} C0 w - d: the step
+      // kernel needs no D term (ResChebZPhys).  Same iteration as below up to rounding.
+      R* z = r;
+      // d = x = D^{-1} b / theta;  z = D^{-1} b = theta d
+      MG_CU(Prec<R>::cheb(k, (const R*)L.LM, b, 0.0, ginv / theta, d, x, 1, L.ncell, o->stream));
+      k_scale_to<R><<<nblocks(L.ns), kThreads, 0, o->stream>>>(d, (R)theta, z, L.ns);
+      MG_CU(cudaGetLastError());
+      o->launches += 2;
+      double rho_old = 1.0 / sigma;
+      for (int it = 1; it < degree; ++it) {
+        const double rho = 1.0 / (2.0 * sigma - rho_old);
+        const double a = rho * rho_old, sc = 2.0 * rho / delta;
+        // w = A^{-1} B d;  z += D^{-1} C0 w - d;  dn = a d + sc z;  x += dn  (two launches)
+        MG_CU(Prec<R>::b_inv(k, L.mesh, d, s->cB, (const R*)L.LA, (R*)L.w, L.ncell, o->stream, s->rq));
+        MG_CU(Prec<R>::res_chebz(k, L.mesh, (const R*)L.w, (const R*)L.pfR, d, s->cdt, (const R*)L.LM, ginv, a, sc, z,
+                                 dn, x, L.ncell, o->stream, s->rq));
+        o->launches += 2;
+        std::swap(d, dn);
+        rho_old = rho;
+      }
+      return AF_OK;
+    }
+  }
   MG_CU(cudaMemcpyAsync(r, b, sizeof(R) * L.ns, cudaMemcpyDeviceToDevice, o->stream));
   if (!zero_init) MG_AF(residual_update<R>(s, L, x, r));
   MG_CU(Prec<R>::cheb(k, (const R*)L.LM, r, 0.0, ginv / theta, d, x, zero_init ? 1 : 0, L.ncell, o->stream));

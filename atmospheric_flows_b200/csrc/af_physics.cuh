@@ -389,6 +389,30 @@ struct ResChebPhys : CPhys<true, 1, R, false, true> {
   static constexpr int EPI = 2;
 };
 
+// The same smoother step carried on the preconditioned residual z = D^{-1} r (epilogue 3).
+// The cell inverse of D is exact for the D the level operator applies (both are M-type at the
+// same Gauss points; the change of basis inverts M exactly on bilinear cells), so
+//   z' = D^{-1} (r + C0 w - D d) = z + D^{-1} C0 w - d,
+// and the kernel evaluates C0 w alone: no D group, one field group fewer than ResChebPhys.
+// Then d' = alpha d + s z' and x = d' (first) or x += d'.  Inputs as CPhys<false, +1>: w,
+// p_fixed; r holds z on input and z' on output; D^{-1} = g M^{-1} with M's weights in inv.
+template <class R>
+struct ResChebZParams : CParamsT<R> {
+  const R* inv;  // [cell][(P+1)^2] Gauss-point inverse weights of M (1 / JxW)
+  R g;           // D^{-1} = g M^{-1}
+  R alpha, s;
+  R* r;          // the preconditioned residual z (read, then overwritten by z')
+  const R* din;  // the direction d (read for alpha d and for z' = z + ... - d)
+  R* dout;
+  R* x;
+  int first;
+};
+template <class R>
+struct ResChebZPhys : CPhys<false, 1, R, false, true> {
+  using Params = ResChebZParams<R>;
+  static constexpr int EPI = 3;
+};
+
 // Reduced-quadrature variants of the FP32 preconditioner's level operators: P+1 Gauss points
 // per direction instead of 2P+1.  On bilinear cells this integrates B (p div v: degree 2P+1
 // per direction with the adjugate of the Jacobian) and M, D exactly; C0 (p_fixed w . grad q,
@@ -403,6 +427,10 @@ struct ResChebRPhys : ResChebPhys<R> {
 };
 template <class R>
 struct CResRPhys : CPhys<true, 1, R, false, true> {
+  static constexpr bool REDUCED_Q = true;
+};
+template <class R>
+struct ResChebZRPhys : ResChebZPhys<R> {
   static constexpr bool REDUCED_Q = true;
 };
 

@@ -206,3 +206,41 @@ def test_reduced_quadrature_preconditioner_is_exact_on_affine_cells():
         out[name] = rel(z[1].cpu().numpy(), z[0].cpu().numpy())
     assert out["box"] < 1e-4, out
     assert out["hill"] > 10 * out["box"], out
+
+
+@pytest.mark.parametrize("P", [2, 4])
+def test_fp32_chebyshev_on_the_preconditioned_residual_matches_fp64(P):
+    """The FP32 Chebyshev preconditioner carries z = D^{-1} r (its step kernel has no D term:
+    z' = z + D^{-1} C0 w - d), the FP64 one the residual r itself (r' = r + C0 w - D d, then
+    D^{-1} r').  With the same quadrature (2P+1 points, reduced_quadrature = 0) and degree the
+    two are the same polynomial in D^{-1} S0.  rho_for_fixed is constant, so that the FP32
+    levels' change-of-basis A^{-1} (exact for a constant rho) and the FP64 levels' packed
+    A^{-1} invert the same A; pres_fixed is the hill state's.  The outputs then agree to FP32
+    rounding, amplified by the recurrence with the degree (degree 2: one z-step, 1e-5;
+    degree 16: 1e-3)."""
+    from atmospheric_flows_b200.operator import EULEROperator
+    from atmospheric_flows_b200.schur import SchurSolver
+    dt = 2.0
+    sc = M.Scaling()
+    m = M.hill_mesh(16, 8)
+    n = m.n_cells * (P + 1) ** 2
+    op = EULEROperator(m, P, sc.Ma, sc.Fr, dt)
+    op.set_stream(torch.cuda.current_stream())
+    op.set_HYPERBOLIC_stage(1)
+    st = M.hill_state(m, P, modes=4)
+    op.set_rho_for_fixed(torch.full((n,), 1.3, dtype=torch.float64, device="cuda"))
+    op.set_pres_fixed(torch.from_numpy(st.p).cuda())
+    op.set_NS_stage(2)
+    b = torch.from_numpy(np.random.default_rng(9).standard_normal(n)).cuda()
+    errs = {}
+    for degree, tol in ((2, 1e-5), (16, 1e-3)):
+        z = {}
+        for pc, opts in (("cheb_fp64", {}), ("cheb_fp32", {"reduced_quadrature": 0})):
+            s = SchurSolver(op, pc, poly_degree=degree, **opts)
+            s.setup()
+            z[pc] = torch.zeros(n, dtype=torch.float64, device="cuda")
+            s.precondition(z[pc], b)
+        torch.cuda.synchronize()
+        errs[degree] = rel(z["cheb_fp32"].cpu().numpy(), z["cheb_fp64"].cpu().numpy())
+        assert errs[degree] < tol, errs
+    print("fp32 z-form vs fp64 r-form, relative difference by degree:", errs)
