@@ -76,6 +76,13 @@ struct EpiOf<Phys, std::void_t<decltype(Phys::EPI)>> {
   static constexpr int value = Phys::EPI;
 };
 
+// Cell indices kept in the real-typed geometry block, stored bit for bit (a float holds
+// integers exactly only up to 2^24, fewer than the cells of a large mesh).
+__device__ __forceinline__ void put_index(float& s, int v) { s = __int_as_float(v); }
+__device__ __forceinline__ void put_index(double& s, int v) { s = __longlong_as_double((long long)v); }
+__device__ __forceinline__ int get_index(float s) { return __float_as_int(s); }
+__device__ __forceinline__ int get_index(double s) { return (int)__double_as_longlong(s); }
+
 template <int N, class F, int... I>
 __device__ __forceinline__ void sfor_impl(F& f, std::integer_sequence<int, I...>) {
   (f(std::integral_constant<int, I>{}), ...);
@@ -445,7 +452,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       const int nb1 = i < mesh.nx - 1 ? c + 1 : (mesh.periodic_x ? c - mesh.nx + 1 : -1);
       const int nb2 = j > 0 ? c - mesh.nx : -1;
       const int nb3 = j < mesh.nz - 1 ? c + mesh.nx : -1;
-      g[20] = (R)nb0; g[21] = (R)nb1; g[22] = (R)nb2; g[23] = (R)nb3;
+      put_index(g[20], nb0); put_index(g[21], nb1); put_index(g[22], nb2); put_index(g[23], nb3);
     } else {
       // faces: 0 (xi=0, edge v0->v2), 1 (xi=1, v1->v3), 2 (eta=0, v0->v1), 3 (eta=1, v2->v3);
       // a face's normal is formed from its two vertices the same way by both cells
@@ -535,7 +542,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       if (tid < CB * P1) {
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-          const int nb = (int)s_geo[cc * 24 + 20 + f];
+          const int nb = get_index(s_geo[cc * 24 + 20 + f]);
           const bool ok = nb >= 0 && cc < ncb;
           const int kk = f == 0 ? i * P1 + P : (f == 1 ? i * P1 : (f == 2 ? P * P1 + i : i));
           sfor<Gi::NARR>([&](auto ac) {
@@ -611,7 +618,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       const R* g = s_geo + cl * 24;
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
-        const int nb = (int)g[20 + f];
+        const int nb = get_index(g[20 + f]);
         R vp[NF], vm[NF];
 #pragma unroll
         for (int fi = 0; fi < NF; ++fi) {
