@@ -79,17 +79,20 @@ def profile_numbers():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling (every 100 ms, with timestamps) around the timed region; mark() the
+    region's start and end, and the summary keeps the samples taken inside it (all samples,
+    flagged, when the region was too short to hold one)."""
 
     def __init__(self, index):
         self.index = index
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+        q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
                                        "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
@@ -98,30 +101,43 @@ class Clocks:
         time.sleep(0.3)
         return self
 
+    def mark(self):
+        """Call at the start and at the end of the timed region (after a device sync)."""
+        if self.t0 is None:
+            self.t0 = time.time()
+        else:
+            self.t1 = time.time()
+
     def __exit__(self, *a):
         if self.p:
+            time.sleep(0.15)  # one more sample after the region
             self.p.terminate()
             self.p.wait()
 
     def summary(self):
+        import datetime
         self.f.flush()
         self.f.seek(0)
-        sm, mx, reasons = [], 0.0, set()
+        rows = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.f:
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[2]), float(parts[3]),
+                             {n for n, v in zip(names, parts[6:10]) if v.lower() == "active"}))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if self.t0 is not None and self.t1 is not None and self.t0 <= r[0] <= self.t1]
+        use = inside or rows
+        sm = [r[1] for r in use]
+        reasons = set().union(*(r[3] for r in use)) if use else set()
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max((r[2] for r in use), default=None),
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": "timed region" if inside else "around the timed region (shorter than the sampling interval)"}
 
 
 def cpu_baseline_oracle(rows, repeats, threads):
@@ -423,11 +439,13 @@ def run_ours(args, rank, world, local_rank):
     launches0 = op.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local_rank) as clk:
+        clk.mark()
         e0.record(stream)
         for _ in range(args.steps):
             op.vmult_rhs_fused(*bufs, src)
         e1.record(stream)
         e1.synchronize()
+        clk.mark()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -656,7 +674,7 @@ def run_timeline():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=2000)  # about 0.9 s of timed applies at 512x256, p = 4
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-sweep", action="store_true")
