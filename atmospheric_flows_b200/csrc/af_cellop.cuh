@@ -275,7 +275,10 @@ struct Layout {
   static constexpr int R_OUT = NOUT * CB * NDP;
   static constexpr int RB = (R_IN + R_NB) > R_OUT ? (R_IN + R_NB) : R_OUT;
   static constexpr int R_FLUX = Phys::FACES ? 4 * NOUT * CB * NQ : 0;
-  static constexpr int R_GEO = CB * 24;  // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb
+  // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb; an odd stride, so that a warp
+  // reading one slot of consecutive cells meets no bank conflicts (4- and 8-byte elements)
+  static constexpr int GS = 25;
+  static constexpr int R_GEO = CB * GS;
   static constexpr int R_S = NQ * P1 + NQ;
   // region E (epilogue policies): the CTA's Gauss-point inverse weights, 16-byte aligned
   static constexpr int EPI = EpiOf<Phys>::value;
@@ -440,7 +443,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   for (int k = tid; k < NQ; k += NT) s_w[k] = tb.w[k];
   for (int task = m; task < 5; task += NQ) {
     const int i = c % mesh.nx, j = c / mesh.nx, W = mesh.nx + 1;
-    R* g = s_geo + cl * 24;
+    R* g = s_geo + cl * L::GS;
     if (task == 4) {
       const double2 v0 = mesh.vtx[j * W + i], v1 = mesh.vtx[j * W + i + 1];
       const double2 v2 = mesh.vtx[(j + 1) * W + i], v3 = mesh.vtx[(j + 1) * W + i + 1];
@@ -542,7 +545,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       if (tid < CB * P1) {
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-          const int nb = get_index(s_geo[cc * 24 + 20 + f]);
+          const int nb = get_index(s_geo[cc * L::GS + 20 + f]);
           const bool ok = nb >= 0 && cc < ncb;
           const int kk = f == 0 ? i * P1 + P : (f == 1 ? i * P1 : (f == 2 ? P * P1 + i : i));
           sfor<Gi::NARR>([&](auto ac) {
@@ -615,7 +618,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
 #pragma unroll
       for (int i = 0; i < P1; ++i) sq[i] = s_S[q * P1 + i];
       const R wq = s_w[q];
-      const R* g = s_geo + cl * 24;
+      const R* g = s_geo + cl * L::GS;
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
         const int nb = get_index(g[20 + f]);
@@ -673,7 +676,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   }
   {
     const int qx = m;
-    const R* g = s_geo + cl * 24;
+    const R* g = s_geo + cl * L::GS;
     const R xi = tb.x[qx];
     const R wx = s_w[qx];
     const R J01 = fmaR(g[2], xi, g[4]);  // x_eta (x component)
