@@ -885,8 +885,21 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     }
     R* dst = s_out + (o * CB + cl) * L::NDP + iz * P1;
+    if constexpr (L::EPI == 1 || L::EPI == 3) {
+      // the epilogue's first change-of-basis pass on the row in registers:
+      // u[iz][qx] = sum_ix Vi[ix][qx] out[ix], stored in place of the row
+      const CobT<P, R>& cbx = cobr<P, R>();
 #pragma unroll
-    for (int ix = 0; ix < P1; ++ix) dst[ix] = out[ix];
+      for (int qx = 0; qx < P1; ++qx) {
+        R t = R(0);
+#pragma unroll
+        for (int ix = 0; ix < P1; ++ix) t = fmaR(cbx.Vi[ix][qx], out[ix], t);
+        dst[qx] = t;
+      }
+    } else {
+#pragma unroll
+      for (int ix = 0; ix < P1; ++ix) dst[ix] = out[ix];
+    }
   }
   __syncthreads();
   if constexpr (L::EPI == 0) {
@@ -916,8 +929,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       cp_async_wait_all();
       __syncthreads();
     }
-    // region A is free after the x-transpose pass: s_y = the (cell, component) input rows
-    // (EPI 2: the updated residual), s_u = the values between the passes
+    // EPI 2: region A is free after the x-transpose pass: s_y = the updated residual rows,
+    // s_u = the values between the passes
     constexpr int NC = L::EPI == 1 ? NOUT : 1;
     R* s_y = smem;
     R* s_u = smem + CB * ND;
@@ -933,29 +946,34 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
       __syncthreads();
     }
-    auto yin = [&](int o, int cc, int k) -> R {
-      if constexpr (L::EPI == 2) return s_y[cc * ND + k];
-      else return s_out[(o * CB + cc) * L::NDP + k];
+    // the half-transformed values u of component o of cell cc: EPI 1 and 3 formed them in the
+    // x-transpose pass (in place of the output rows), EPI 2 forms them here from the updated
+    // residual
+    auto ubase = [&](int o, int cc) -> R* {
+      if constexpr (L::EPI == 2) return s_u + (o * CB + cc) * ND;
+      else return s_out + (o * CB + cc) * L::NDP;
     };
-    // pass 1 (along x): u[iz][qx] = sum_ix Vi[ix][qx] y[iz][ix]; task (component, cell, row)
-    for (int e = tid; e < NC * ncb * P1; e += NT) {
-      const int o = e / (ncb * P1), cc = (e / P1) % ncb, iz = e % P1;
-      R yr[P1];
+    if constexpr (L::EPI == 2) {
+      // pass 1 (along x): u[iz][qx] = sum_ix Vi[ix][qx] y[iz][ix]; task (cell, row)
+      for (int e = tid; e < ncb * P1; e += NT) {
+        const int cc = e / P1, iz = e % P1;
+        R yr[P1];
 #pragma unroll
-      for (int ix = 0; ix < P1; ++ix) yr[ix] = yin(o, cc, iz * P1 + ix);
+        for (int ix = 0; ix < P1; ++ix) yr[ix] = s_y[cc * ND + iz * P1 + ix];
 #pragma unroll
-      for (int qx = 0; qx < P1; ++qx) {
-        R t = R(0);
+        for (int qx = 0; qx < P1; ++qx) {
+          R t = R(0);
 #pragma unroll
-        for (int ix = 0; ix < P1; ++ix) t = fmaR(cb.Vi[ix][qx], yr[ix], t);
-        s_u[(o * CB + cc) * ND + iz * P1 + qx] = t;
+          for (int ix = 0; ix < P1; ++ix) t = fmaR(cb.Vi[ix][qx], yr[ix], t);
+          s_u[cc * ND + iz * P1 + qx] = t;
+        }
       }
+      __syncthreads();
     }
-    __syncthreads();
     // pass 2 (along z, per column qx): to the Gauss points, times the weights, and back
     for (int e = tid; e < NC * ncb * P1; e += NT) {
       const int o = e / (ncb * P1), cc = (e / P1) % ncb, qx = e % P1;
-      R* col = s_u + (o * CB + cc) * ND + qx;
+      R* col = ubase(o, cc) + qx;
       R u[P1], t[P1];
 #pragma unroll
       for (int iz = 0; iz < P1; ++iz) u[iz] = col[iz * P1];
@@ -978,7 +996,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     // pass 3 (along x): x[iz][ix] = sum_qx Vi[ix][qx] v[iz][qx], then the store or update
     for (int e = tid; e < NC * ncb * P1; e += NT) {
       const int o = e / (ncb * P1), cc = (e / P1) % ncb, iz = e % P1;
-      const R* row = s_u + (o * CB + cc) * ND + iz * P1;
+      const R* row = ubase(o, cc) + iz * P1;
       R v[P1];
 #pragma unroll
       for (int qx = 0; qx < P1; ++qx) v[qx] = row[qx];
