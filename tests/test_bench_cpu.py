@@ -53,3 +53,29 @@ def test_single_rank_is_identity():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.reduce_max_over_ranks(3.25, 1, "cpu") == 3.25
+
+
+def test_clock_summary_keeps_the_samples_inside_the_timed_region():
+    """The nvidia-smi record is filtered by its timestamps: the median clock and the throttle
+    reasons come from the samples between the two marks; a region shorter than the sampling
+    interval falls back to all samples and says so."""
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.Clocks(0)  # not entered: no nvidia-smi process, the record is written here
+    now = time.time()
+    for k in range(12):
+        t = now - 0.6 + 0.1 * k
+        ts = datetime.datetime.fromtimestamp(t).strftime("%Y/%m/%d %H:%M:%S.%f")[:-3]
+        sm = 1965 if k < 4 else 1800                       # idle before, loaded inside
+        cap = "Active" if k == 11 else "Not Active"          # power cap only after the region
+        c.f.write(f"{ts}, 0, {sm}, 1965, 500.0, 0x0, Not Active, Not Active, Not Active, {cap}\n")
+    c.t0, c.t1 = now - 0.25, now + 0.35
+    s = c.summary()
+    assert s["window"] == "timed region"
+    assert s["samples"] == 6 and s["sm_mhz"] == 1800.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == []
+    c.t0, c.t1 = now + 5.0, now + 5.01
+    s = c.summary()
+    assert s["samples"] == 12 and s["window"].startswith("around")
+    assert s["reasons"] == ["sw_power_cap"]
