@@ -61,3 +61,40 @@ def test_cpp_header_compiles():
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
                         "-x", "c++", "-"], input=src, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_imex_options_are_checked_on_the_host_and_no_device_fails_loudly():
+    """af_imex_create rejects bad options before any device call; with valid arguments and no
+    CUDA device (this CPU run) the library returns AF_NO_DEVICE and no handle, with no CPU
+    fallback."""
+    from atmospheric_flows_b200 import operator as O
+    from atmospheric_flows_b200 import imex as I
+    from atmospheric_flows_b200 import mesh as M
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present: the no-device path is not reachable")
+    except ImportError:
+        pass
+    L = O.lib()
+    m = M.hill_mesh(4, 2)
+    v = np.ascontiguousarray(m.vertices)
+    desc = O._MeshDesc(4, 2, 0, v.ctypes.data, 0, 0.0)
+    d = I.Options()
+    L.af_imex_default_options(ctypes.byref(d))
+    assert d.schur_poly_degree == 0 and d.schur_preconditioner == -1 and d.eps == 1e-8
+    h = ctypes.c_void_p()
+    args = (ctypes.c_double(1.0), ctypes.c_double(1.0), ctypes.c_double(0.5))
+    for field, bad in (("eps", -1.0), ("gmres_restart", 61), ("schur_poly_degree", -1),
+                       ("schur_preconditioner", 9), ("mass_solver", 2), ("fixed_point_max_iterations", 0)):
+        o = I.Options()
+        L.af_imex_default_options(ctypes.byref(o))
+        setattr(o, field, bad)
+        assert L.af_imex_create(ctypes.byref(desc), 4, *args, ctypes.byref(o), ctypes.byref(h)) == O.AF_BAD_ARG, field
+        assert b"bad options" in L.af_last_error_message()
+        assert h.value is None
+    assert L.af_imex_create(ctypes.byref(desc), 4, *args, ctypes.byref(d), ctypes.byref(h)) == O.AF_NO_DEVICE
+    assert h.value is None
+    op = ctypes.c_void_p()
+    assert L.af_create(ctypes.byref(desc), 4, 9, *args, ctypes.byref(op)) == O.AF_NO_DEVICE
+    assert op.value is None
