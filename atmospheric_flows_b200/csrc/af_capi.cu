@@ -48,6 +48,34 @@ static int fail(int code, const char* fmt, ...) {
     if (e_ != cudaSuccess) return fail(AF_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
+// A code that an earlier kernel of the handle left in its status word is reported by the next
+// call (kernels run asynchronously: the call that queued them has returned by then).
+#define AF_PENDING(o)                              \
+  do {                                             \
+    const int r_ = af::take_kernel_status(o);     \
+    if (r_ != AF_OK) return r_;                   \
+  } while (0)
+
+namespace af {
+int take_kernel_status(af_operator* o) {
+  if (!o || !o->h_status) return AF_OK;
+  volatile int* w = o->h_status;
+  const int v = *w;
+  if (v == 0) return AF_OK;
+  *w = 0;
+  return fail(AF_TIMEOUT,
+              "a kernel gave up a bounded wait for its staged inputs (code %d) and did not write its outputs; "
+              "the results of the calls queued since the last check are invalid",
+              v);
+}
+
+int sync_checked(af_operator* o, cudaStream_t st) {
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(AF_CUDA, "cudaStreamSynchronize: %s", cudaGetErrorString(e));
+  return take_kernel_status(o);
+}
+}  // namespace af
+
 static void set_tableau(af_operator* o) {
   o->gamma = 2.0 - std::sqrt(2.0);
   o->a21 = o->gamma; o->a22 = 0.0; o->a31 = 0.5; o->a32 = 0.5; o->a33 = 0.0;
@@ -95,6 +123,7 @@ const char* af_error_string(int s) {
     case AF_NAN: return "NaN or Inf";
     case AF_UNSUPPORTED: return "unsupported degree";
     case AF_NO_DEVICE: return "no CUDA device";
+    case AF_TIMEOUT: return "a kernel gave up a bounded wait";
     default: return "unknown status";
   }
 }
@@ -142,6 +171,13 @@ int af_create(const af_mesh_desc* m, int degree, int nq, double Ma, double Fr, d
     return cleanup(fail(AF_CUDA, "device allocation failed"));
   if (cudaMemcpy(o->d_vtx, m->vertices, nv * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
     return cleanup(fail(AF_CUDA, "vertex upload failed"));
+  int* d_status = nullptr;
+  if (cudaHostAlloc((void**)&o->h_status, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+    return cleanup(fail(AF_CUDA, "status word allocation failed"));
+  *o->h_status = 0;
+  if (cudaHostGetDevicePointer((void**)&d_status, o->h_status, 0) != cudaSuccess)
+    return cleanup(fail(AF_CUDA, "status word mapping failed"));
+  o->mesh.status = d_status;
   o->mesh.vtx = o->d_vtx;
   o->mesh.nx = m->nx;
   o->mesh.nz = m->nz;
@@ -167,6 +203,7 @@ int af_destroy(af_operator* o) {
   cudaFree(o->d_stage);
   cudaFree(o->d_Wm);
   cudaFree(o->d_La);
+  if (o->h_status) cudaFreeHost(o->h_status);
   if (o->own_stream) cudaStreamDestroy(o->own_stream);
   if (o->copy_in) cudaStreamDestroy(o->copy_in);
   if (o->copy_out) cudaStreamDestroy(o->copy_out);
@@ -187,7 +224,12 @@ int af_set_stream(af_operator* o, void* s) {
 
 int af_synchronize(af_operator* o) {
   if (!o) return fail(AF_BAD_ARG, "null handle");
-  AF_CU(cudaStreamSynchronize(o->stream));
+  return sync_checked(o, o->stream);
+}
+
+int af_set_stage_wait_test(af_operator* o, int polls) {
+  if (!o || polls < 0) return fail(AF_BAD_ARG, "af_set_stage_wait_test: bad handle or negative poll count");
+  o->mesh.test_wait_polls = polls;
   return AF_OK;
 }
 
@@ -220,6 +262,7 @@ int af_set_NS_stage(af_operator* o, int s) {  // AssertIndexRange(stage, 7), sta
 static int copy_fixed(af_operator* o, double* dst, const double* src, long n) {
   if (!o || !src) return fail(AF_BAD_ARG, "null argument");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, o->stream));
   return AF_OK;
 }
@@ -246,6 +289,7 @@ static int run_rhs(af_operator* o, int mask, const RhsSources& s, double* d_rho,
   for (const double* p : ptrs)
     if (p && !aligned16(p)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   const RhsParams prm = rhs_params(o, o->hs);
   MeshDev m = o->mesh;
   m.cell0 = cbeg;
@@ -330,6 +374,7 @@ int af_vmult_rhs_fused_backward(af_operator* o, const double* const* src, int n,
     if (!src[k] || !xbar[k] || !aligned16(src[k]) || !aligned16(xbar[k]))
       return fail(AF_BAD_ARG, "af_vmult_rhs_fused_backward: null or unaligned vector");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   const double* yb[3] = {ybar_rho, ybar_u, ybar_p};
   if (o->hs == 1) {
     AF_CU(o->ops->rhs_adjoint1(o->mesh, src, yb, xbar, rhs_params(o, 1), o->ncell, o->stream));
@@ -350,6 +395,7 @@ int af_vmult_rhs_fused_tangent(af_operator* o, const double* const* src, int n, 
     if (!src[k] || !dsrc[k] || !aligned16(src[k]) || !aligned16(dsrc[k]))
       return fail(AF_BAD_ARG, "af_vmult_rhs_fused_tangent: null or unaligned vector");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   double* dy[3] = {d_rho, d_u, d_p};
   if (o->hs == 1)
     AF_CU(o->ops->rhs_tangent1(o->mesh, src, dsrc, dy, rhs_params(o, 1), o->ncell, o->stream));
@@ -373,6 +419,7 @@ int af_vmult_rhs_fused_host(af_operator* o, double* h_rho, double* h_u, double* 
   size_t total = up2(ns) + 2 * ns + up2(ns);         // outputs: rho, u (2), p
   for (long l : len) total += up2(l);
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   if (o->stage_len < total) {
     cudaFree(o->d_stage);
     o->d_stage = nullptr;
@@ -426,8 +473,10 @@ int af_vmult_rhs_fused_host(af_operator* o, double* h_rho, double* h_u, double* 
     const long c0 = (long)c * rpc * nx, c1 = std::min<long>((long)(c + 1) * rpc, nz) * nx;
     AF_CU(cudaStreamWaitEvent(o->stream, o->ev_in[std::min(c + 1, K - 1)], 0));
     const int r = rhs_fused_range(o, d_rho, d_u, d_p, d_srcc.data(), n, (int)c0, (int)c1);
-    if (r != AF_OK) {
+    if (r != AF_OK) {  // nothing may still read or write the caller's host buffers
       cudaStreamSynchronize(o->copy_in);
+      cudaStreamSynchronize(o->stream);
+      cudaStreamSynchronize(o->copy_out);
       return r;
     }
     AF_CU(cudaEventRecord(o->ev_done[c], o->stream));
@@ -443,8 +492,7 @@ int af_vmult_rhs_fused_host(af_operator* o, double* h_rho, double* h_u, double* 
       AF_CU(cudaMemcpyAsync(h_p + c0 * nd, d_p + c0 * nd, cnt * sizeof(double), cudaMemcpyDeviceToHost, o->copy_out));
   }
   AF_CU(cudaStreamSynchronize(o->copy_out));
-  AF_CU(cudaStreamSynchronize(o->stream));
-  return AF_OK;
+  return sync_checked(o, o->stream);
 }
 
 static double coeff_BC(const af_operator* o) { return o->hs == 1 ? o->a22t : o->a33t; }  // :1428, 1526
@@ -453,6 +501,7 @@ int af_vmult_pressure(af_operator* o, double* dst, const double* src) {
   if (!o || !dst || !src) return fail(AF_BAD_ARG, "null argument");
   if (!aligned16(dst) || !aligned16(src)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(o->ops->op_B(o->mesh, src, coeff_BC(o) * o->dt / (o->Ma * o->Ma), dst, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -471,6 +520,7 @@ int af_vmult_enthalpy(af_operator* o, double* dst, const double* src) {
   if (!o->pres_fixed_set) return fail(AF_BAD_ARG, "vmult_enthalpy: set_pres_fixed first");
   if (!aligned16(dst) || !aligned16(src)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(o->ops->op_C(o->mesh, src, o->d_pres_fixed, nullptr, c_params(o), dst, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -505,7 +555,8 @@ static int solve_A(af_operator* o, double* x, const double* b) {
       o->launches += 6;
     }
     AF_CU(cudaMemcpyAsync(&hs, o->d_kst, sizeof(hs), cudaMemcpyDeviceToHost, o->stream));
-    AF_CU(cudaStreamSynchronize(o->stream));
+    const int rs = sync_checked(o, o->stream);
+    if (rs != AF_OK) return rs;
     if (hs.done) break;
   }
   o->last_inner_its = hs.its;
@@ -542,10 +593,11 @@ int af_vmult_inverse(af_operator* o, double* dst, const double* src) {
   const int ns = o->ns;
   if (ns == 2) return fail(AF_BAD_ARG, "af_vmult_inverse: NS_stage 2 (Schur complement) has no cell-wise inverse");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   if (ns == 3 || ns == 5) {  // A: packed exact inverses (rho-weighted, rebuilt per rho_for_fixed)
     const int r = ensure_factor(o);
     if (r != AF_OK) return r;
-    AF_CU(o->ops->mass_solve(o->d_La, 2, src, 1.0, dst, o->ncell, o->stream));
+    AF_CU(o->ops->mass_solve(o->d_La, 2, src, 1.0, dst, o->ncell, o->mesh.status, o->stream));
   } else {  // M (NS 1/4) and D = M/(gamma-1) (NS 6): change of basis, no stored matrices
     const int r = ensure_mass_weights(o);
     if (r != AF_OK) return r;
@@ -559,6 +611,7 @@ int af_vmult(af_operator* o, double* dst, const double* src) {
   if (!o || !dst || !src) return fail(AF_BAD_ARG, "null argument");
   if (!aligned16(dst) || !aligned16(src)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   const int ns = o->ns;
   if (ns == 1 || ns == 4) {
     AF_CU(o->ops->mass(o->mesh, 1, src, nullptr, 1.0, dst, o->ncell, o->stream));
@@ -589,7 +642,7 @@ int af_vmult(af_operator* o, double* dst, const double* src) {
   if (o->schur_mode == 1) {  // exact cell-wise A^{-1}
     r = ensure_factor(o);
     if (r != AF_OK) return r;
-    AF_CU(o->ops->mass_solve(o->d_La, 2, t1, 1.0, t2, o->ncell, o->stream));
+    AF_CU(o->ops->mass_solve(o->d_La, 2, t1, 1.0, t2, o->ncell, o->mesh.status, o->stream));
     o->launches += 1;
     o->last_inner_its = 0;
   } else {
@@ -604,6 +657,7 @@ int af_vmult(af_operator* o, double* dst, const double* src) {
 int af_compute_diagonal(af_operator* o, double* inv_diag) {
   if (!o || !inv_diag) return fail(AF_BAD_ARG, "null argument");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   const int ns = o->ns;
   if (ns == 1 || ns == 4) AF_CU(o->ops->inv_diag(o->mesh, 1, nullptr, 1.0, inv_diag, o->ncell, o->stream));
   else if (ns == 2 || ns == 6) AF_CU(o->ops->inv_diag(o->mesh, 1, nullptr, 1.0 / (1.4 - 1.0), inv_diag, o->ncell, o->stream));
@@ -651,6 +705,7 @@ int af_vmult_pressure_transpose(af_operator* o, double* pbar, const double* ubar
   if (!o || !pbar || !ubar) return fail(AF_BAD_ARG, "null argument");
   if (!aligned16(pbar) || !aligned16(ubar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(o->ops->op_BT(o->mesh, ubar, coeff_BC(o) * o->dt / (o->Ma * o->Ma), pbar, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -661,6 +716,7 @@ int af_vmult_enthalpy_tangent(af_operator* o, double* dst, const double* w, cons
   if (!o->pres_fixed_set) return fail(AF_BAD_ARG, "set_pres_fixed first");
   if (!aligned16(dst) || !aligned16(w) || !aligned16(dw)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(o->ops->op_C_tangent(o->mesh, w, dw, o->d_pres_fixed, c_params(o), dst, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -671,6 +727,7 @@ int af_vmult_enthalpy_transpose(af_operator* o, double* wbar, const double* w, c
   if (!o->pres_fixed_set) return fail(AF_BAD_ARG, "set_pres_fixed first");
   if (!aligned16(wbar) || !aligned16(w) || !aligned16(pbar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(o->ops->op_CT(o->mesh, w, o->d_pres_fixed, pbar, c_params(o), wbar, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -680,6 +737,7 @@ int af_vmult_velocity_mass_rho_transpose(af_operator* o, double* rhobar, const d
   if (!o || !rhobar || !x || !y) return fail(AF_BAD_ARG, "null argument");
   if (!aligned16(rhobar) || !aligned16(x) || !aligned16(y)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(o->ops->op_A_rho_T(o->mesh, x, y, rhobar, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -689,6 +747,7 @@ int af_vmult_enthalpy_pf_transpose(af_operator* o, double* pfbar, const double* 
   if (!o || !pfbar || !w || !pbar) return fail(AF_BAD_ARG, "null argument");
   if (!aligned16(pfbar) || !aligned16(w) || !aligned16(pbar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   AF_CU(o->ops->op_C_pf_T(o->mesh, w, pbar, c_params(o), pfbar, o->ncell, o->stream));
   o->launches += 1;
   return AF_OK;
@@ -699,7 +758,7 @@ static int schur_w(af_operator* o, const double* p, double* w, double* t) {
   AF_CU(o->ops->op_B(o->mesh, p, coeff_BC(o) * o->dt / (o->Ma * o->Ma), t, o->ncell, o->stream));
   int r = ensure_factor(o);
   if (r != AF_OK) return r;
-  AF_CU(o->ops->mass_solve(o->d_La, 2, t, 1.0, w, o->ncell, o->stream));
+  AF_CU(o->ops->mass_solve(o->d_La, 2, t, 1.0, w, o->ncell, o->mesh.status, o->stream));
   o->launches += 2;
   return AF_OK;
 }
@@ -709,6 +768,7 @@ int af_schur_tangent(af_operator* o, double* dst, const double* p, const double*
   if (!o->rho_fixed_set || !o->pres_fixed_set) return fail(AF_BAD_ARG, "set rho_for_fixed and pres_fixed first");
   if (!aligned16(dst) || !aligned16(p) || !aligned16(dp)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   const long n = o->n_scalar();
   double *w = o->d_ws, *z = o->d_ws + 2 * n, *t = o->d_ws + 4 * n, *c = o->d_ws + 6 * n;
   int r = schur_w(o, p, w, t);
@@ -726,12 +786,13 @@ int af_schur_transpose(af_operator* o, double* dst, const double* p, const doubl
   if (!o->rho_fixed_set || !o->pres_fixed_set) return fail(AF_BAD_ARG, "set rho_for_fixed and pres_fixed first");
   if (!aligned16(dst) || !aligned16(p) || !aligned16(pbar)) return fail(AF_BAD_ARG, "device pointers must be 16-byte aligned");
   AF_CU(cudaSetDevice(o->device));
+  AF_PENDING(o);
   const long n = o->n_scalar();
   double *w = o->d_ws, *t = o->d_ws + 2 * n, *t2 = o->d_ws + 4 * n, *q = o->d_ws + 6 * n;
   int r = schur_w(o, p, w, t);
   if (r != AF_OK) return r;
   AF_CU(o->ops->op_CT(o->mesh, w, o->d_pres_fixed, pbar, c_params(o), t, o->ncell, o->stream));  // J_C^T pbar
-  AF_CU(o->ops->mass_solve(o->d_La, 2, t, 1.0, t2, o->ncell, o->stream));                        // A^{-1} (A = A^T)
+  AF_CU(o->ops->mass_solve(o->d_La, 2, t, 1.0, t2, o->ncell, o->mesh.status, o->stream));                        // A^{-1} (A = A^T)
   AF_CU(o->ops->op_BT(o->mesh, t2, coeff_BC(o) * o->dt / (o->Ma * o->Ma), q, o->ncell, o->stream));
   AF_CU(o->ops->mass(o->mesh, 1, pbar, nullptr, 1.0 / (1.4 - 1.0), dst, o->ncell, o->stream));    // D = D^T
   AF_CU(axpby(-1.0, q, 1.0, dst, n, o->stream));

@@ -24,6 +24,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <type_traits>
 #include <utility>
 
@@ -37,7 +38,16 @@ struct MeshDev {
   double radial_a;
   int cell0;  // cell kernels: the first cell of the launch (a multiple of its cells per CTA);
               // the launch covers [cell0, ncell).  0 for whole-mesh launches
+  // Status word of the caller (host-visible; null: not reported).  A kernel that gives up a
+  // bounded wait writes kStatusStageTimeout there and leaves without writing its outputs.
+  int* status;
+  // Test hook (0 in normal use): when > 0, each CTA of a cell kernel first waits on a barrier
+  // phase that never completes and gives up after this many polls, before it issues any copy.
+  int test_wait_polls;
 };
+
+// Codes a kernel leaves in MeshDev::status.
+constexpr int kStatusStageTimeout = 1;
 
 struct PointGeo {
   double X[2];  // physical position (valid when Phys::NEED_X)
@@ -132,8 +142,9 @@ constexpr int odd(int n) { return n | 1; }
 constexpr bool kBulkStaging = AF_BULK_STAGING != 0;
 
 // Bounded wait on a shared-memory mbarrier phase; false when the bound was reached.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned phase) {
-  for (int it = 0; it < (1 << 20); ++it) {
+constexpr int kStageWaitPolls = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned phase, int polls = kStageWaitPolls) {
+  for (int it = 0; it < polls; ++it) {
     unsigned ok;
     asm volatile(
         "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
@@ -145,9 +156,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned phase) {
   return false;
 }
 
-// Set when a kernel of this translation unit gave up waiting for its bulk copies (never
-// expected; the kernel then returns without writing its outputs).
-static __device__ int g_af_stage_timeout = 0;
+// Records a given-up wait in the caller's status word (mapped host memory or device memory;
+// every CTA that gives up writes the same code, so a plain store is enough).
+__device__ __forceinline__ void report_status(int* status, int code) {
+  if (status) {
+    *reinterpret_cast<volatile int*>(status) = code;
+    __threadfence_system();
+  }
+}
 
 // Unroll factor of the z-pass loop over quadrature-point pairs (see the kernel).
 #ifndef AF_Z_UNROLL
@@ -383,6 +399,18 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
 
   __shared__ alignas(8) unsigned long long s_bar;  // bulk-copy completion (Layout::BULK)
   const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_bar);
+  if (mesh.test_wait_polls > 0) {
+    // test hook: the bounded wait gives up on a phase that nobody completes (s_bar is armed
+    // with an arrival count of 1 and nobody arrives), then the CTA leaves as after a real
+    // staging timeout; no copy has been issued yet
+    bool ok = true;
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+      ok = mbar_wait(bar, 0, mesh.test_wait_polls);
+      if (!ok) report_status(mesh.status, kStatusStageTimeout);
+    }
+    if (__syncthreads_or(!ok)) return;
+  }
   if constexpr (L::BULK) {
     if (threadIdx.x == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
@@ -567,7 +595,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     if (bulk) {
       const bool ok = mbar_wait(bar, bar_phase);
       bar_phase ^= 1u;
-      if (!ok) atomicExch(&g_af_stage_timeout, 1);
+      if (!ok) report_status(mesh.status, kStatusStageTimeout);
       if (__syncthreads_or(!ok)) {  // every thread leaves together, nothing waits on a barrier
         abort = true;
         return;
@@ -920,7 +948,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     // ---- cell-local epilogue: the inverse weights (copied since kernel start)
     if (epi_bulk) {
       const bool ok = mbar_wait(bar_e, 0);
-      if (!ok) atomicExch(&g_af_stage_timeout, 1);
+      if (!ok) report_status(mesh.status, kStatusStageTimeout);
       if (__syncthreads_or(!ok)) {
         if (tid == 0) mbar_wait(bar_e, 0);
         return;
@@ -1034,12 +1062,18 @@ cudaError_t launch_cellop(const MeshDev& mesh,
                           const ArgPtrs<PhysInfo<Phys>::NARR_TOTAL, Phys::NOUT_ARR, RealOf<Phys>>& ptr,
                           const typename Phys::Params& prm, int ncell, cudaStream_t stream) {
   using L = Layout<P, Phys, CB_>;
-  static bool configured = false;  // per instantiation; the attribute is per device function
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_cellop<P, Phys, CB_, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)L::BYTES);
+  // The shared-memory attribute belongs to the function on the current device: one bit per
+  // device (devices 0..63; beyond that it is set on every launch), set by whichever thread gets
+  // there first (setting it twice is harmless).
+  static std::atomic<unsigned long long> configured{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (bit == 0 || (configured.load(std::memory_order_acquire) & bit) == 0) {
+    e = cudaFuncSetAttribute(k_cellop<P, Phys, CB_, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
     if (e != cudaSuccess) return e;
-    configured = true;
+    configured.fetch_or(bit, std::memory_order_release);
   }
   if (mesh.cell0 % L::CB != 0 || mesh.cell0 < 0) return cudaErrorInvalidValue;
   if (ncell <= mesh.cell0) return cudaSuccess;

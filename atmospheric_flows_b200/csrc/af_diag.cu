@@ -170,7 +170,10 @@ int af_compute_diagnostics(af_operator* o, const double* rho, const double* rho_
   DG_CU(cudaGetLastError());
   double h[kNV];
   DG_CU(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, o->stream));
-  DG_CU(cudaStreamSynchronize(o->stream));
+  {
+    const int r_ = sync_checked(o, o->stream);
+    if (r_ != AF_OK) return r_;
+  }
   o->launches += 2;
   out->max_velocity = h[0];
   out->min_density = -h[1];
@@ -205,7 +208,10 @@ int af_l2_norm(af_operator* o, int ncomp, const double* v, double* norm) {
   DG_CU(cudaGetLastError());
   double h = 0.0;
   DG_CU(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, o->stream));
-  DG_CU(cudaStreamSynchronize(o->stream));
+  {
+    const int r_ = sync_checked(o, o->stream);
+    if (r_ != AF_OK) return r_;
+  }
   o->launches += 2;
   *norm = std::sqrt(h);
   return AF_OK;

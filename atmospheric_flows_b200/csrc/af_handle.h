@@ -49,10 +49,18 @@ struct af_operator {
   size_t stage_len = 0;
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_start = nullptr, ev_in[kHostChunks] = {}, ev_done[kHostChunks] = {};
+  // status word of the handle's kernels (mapped pinned host memory; mesh.status is its device
+  // address): a kernel that gives up a bounded wait leaves a code there
+  int* h_status = nullptr;
 
   long n_scalar() const { return (long)ncell * nd; }
 };
 
 namespace af {
 int mass_inverse_A(af_operator* o, const double** out);
+// AF_TIMEOUT (with a message) when a kernel of the handle left a code in its status word since
+// the last report, which also clears the word; AF_OK otherwise.  Reads host memory, no sync.
+int take_kernel_status(af_operator* o);
+// cudaStreamSynchronize(st), then take_kernel_status(o)
+int sync_checked(af_operator* o, cudaStream_t st);
 }

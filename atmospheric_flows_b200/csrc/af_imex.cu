@@ -105,7 +105,7 @@ static int cg_solve(af_imex* h, const Apply& A, const double* invd, double* x, c
   const int maxit = h->opt.max_iterations;
   for (int it = 0;; it += 8) {
     IM_CU(cudaMemcpyAsync(&hs, h->kst, sizeof(hs), cudaMemcpyDeviceToHost, st));
-    IM_CU(cudaStreamSynchronize(st));
+    IM_AF(sync_checked(h->op, st));
     if (hs.done || it >= maxit) break;
     for (int k = 0; k < 8; ++k) {
       IM_AF(A(h->cg_p, h->cg_Ap));
@@ -138,7 +138,7 @@ static int gmres_solve(af_imex* h, const Apply& A, const double* invd, double* x
     IM_CU(dot(h->gw, nullptr, n, h->part, h->scal, st));
     double beta2 = 0.0;
     IM_CU(cudaMemcpyAsync(&beta2, h->scal, sizeof(double), cudaMemcpyDeviceToHost, st));
-    IM_CU(cudaStreamSynchronize(st));
+    IM_AF(sync_checked(h->op, st));
     h->op->launches += 4;
     const double beta = std::sqrt(beta2);
     res = beta;
@@ -162,7 +162,7 @@ static int gmres_solve(af_imex* h, const Apply& A, const double* invd, double* x
       IM_CU(cudaMemcpyAsync(hh.data(), h->d_h, sizeof(double) * 2 * (m + 1), cudaMemcpyDeviceToHost, st));
       double hn2 = 0.0;
       IM_CU(cudaMemcpyAsync(&hn2, h->scal, sizeof(double), cudaMemcpyDeviceToHost, st));
-      IM_CU(cudaStreamSynchronize(st));
+      IM_AF(sync_checked(h->op, st));
       h->op->launches += 10;
       for (int i = 0; i <= j; ++i) Hs(i, j) = hh[i] + hh[(m + 1) + i];
       const double hn = std::sqrt(hn2);
@@ -343,7 +343,7 @@ static int fixed_point(af_imex* h, int stage, double* p_out, double* u_out) {
     IM_CU(maxabs2(h->pfix, h->pfix_old, ns, h->part, h->scal, o->stream));
     double mm[2];
     IM_CU(cudaMemcpyAsync(mm, h->scal, sizeof(mm), cudaMemcpyDeviceToHost, o->stream));
-    IM_CU(cudaStreamSynchronize(o->stream));
+    IM_AF(sync_checked(o, o->stream));
     o->launches += 2;
     err = mm[1] / (mm[0] + 1e-10);
     if (err < h->opt.fixed_point_tol) break;
@@ -750,7 +750,7 @@ static int step_tangent(af_imex* h, const double* const* dx, double* const* dy, 
   IM_AF(fp_tangent(c, 2, dE, t[3], t[4], t[5], tol, maxit));
   dE[6] = t[3]; dE[7] = t[4]; dE[8] = t[5];
   IM_AF(s3_tangent(c, dE, dy[0], dy[1], dy[2]));
-  IM_CU(cudaStreamSynchronize(c.st));
+  IM_AF(sync_checked(c.o, c.st));
   return AF_OK;
 }
 
@@ -766,7 +766,7 @@ static int step_backward(af_imex* h, const double* const* ybar, double* const* x
   IM_AF(fp_backward(c, 2, Eb[6], Eb[7], Eb[8], Eb, tol, maxit));
   IM_AF(fp_backward(c, 1, Eb[3], Eb[4], Eb[5], Eb, tol, maxit));
   for (int j = 0; j < 3; ++j) IM_AF(ad_copy(c, xbar[j], Eb[j], comp_len(c.ns, j)));
-  IM_CU(cudaStreamSynchronize(c.st));
+  IM_AF(sync_checked(c.o, c.st));
   return AF_OK;
 }
 
@@ -774,7 +774,7 @@ static int s1_tangent(af_imex* h, const double* const* dx, double* const* dy, do
   Ctx c;
   IM_AF(ctx_init(h, c, 1));
   IM_AF(fp_tangent(c, 1, dx, dy[0], dy[1], dy[2], tol, maxit));
-  IM_CU(cudaStreamSynchronize(c.st));
+  IM_AF(sync_checked(c.o, c.st));
   return AF_OK;
 }
 
@@ -783,7 +783,7 @@ static int s1_backward(af_imex* h, const double* const* ybar, double* const* xba
   IM_AF(ctx_init(h, c, 1));
   for (int j = 0; j < 3; ++j) IM_AF(ad_zero(c, xbar[j], comp_len(c.ns, j)));
   IM_AF(fp_backward(c, 1, ybar[0], ybar[1], ybar[2], xbar, tol, maxit));
-  IM_CU(cudaStreamSynchronize(c.st));
+  IM_AF(sync_checked(c.o, c.st));
   return AF_OK;
 }
 
@@ -931,7 +931,7 @@ int af_imex_set_state(af_imex* h, const double* rho, const double* u, const doub
   IM_CU(cudaMemcpyAsync(h->rho0, rho, h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(h->u0, u, 2 * h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(h->p0, p, h->ns * 8, cudaMemcpyDeviceToDevice, st));
-  IM_CU(cudaStreamSynchronize(st));
+  IM_AF(sync_checked(h->op, st));
   return AF_OK;
 }
 
@@ -941,7 +941,7 @@ int af_imex_get_state(const af_imex* h, double* rho, double* u, double* p) {
   IM_CU(cudaMemcpyAsync(rho, h->rho0, h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(u, h->u0, 2 * h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(p, h->p0, h->ns * 8, cudaMemcpyDeviceToDevice, st));
-  IM_CU(cudaStreamSynchronize(st));
+  IM_AF(sync_checked(h->op, st));
   return AF_OK;
 }
 
@@ -966,7 +966,7 @@ int af_imex_stage1_forward(af_imex* h, const double* rho0, const double* u0, con
   IM_CU(cudaMemcpyAsync(rho2, h->rho2, h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(u2, h->u2, 2 * h->ns * 8, cudaMemcpyDeviceToDevice, st));
   IM_CU(cudaMemcpyAsync(p2, h->p2, h->ns * 8, cudaMemcpyDeviceToDevice, st));
-  IM_CU(cudaStreamSynchronize(st));
+  IM_AF(sync_checked(h->op, st));
   return AF_OK;
 }
 
@@ -1082,7 +1082,8 @@ int af_imex_gradient(af_imex* h, const double* rho0, const double* u0, const dou
   copy(rho0bar, R(bar), ns);
   copy(u0bar, U(bar), 2 * ns);
   copy(p0bar, Pp(bar), ns);
-  cudaStreamSynchronize(st);
+  if (r == AF_OK) r = sync_checked(o, st);
+  else cudaStreamSynchronize(st);
   cudaFree(mem);
   return r;
 }

@@ -42,7 +42,7 @@ struct DegreeOps {
   cudaError_t (*mass_factor)(const MeshDev&, const double* weight, double* L, int ncell, cudaStream_t);
   // x = scale * M^{-1} b (block diagonal, exact), ncomp components per cell
   cudaError_t (*mass_solve)(const double* L, int ncomp, const double* b, double scale, double* x, int ncell,
-                            cudaStream_t);
+                            int* status, cudaStream_t);
   int cells_per_block;
   int factor_len;  // (p+1)^2 ((p+1)^2 + 1) / 2
 
@@ -56,7 +56,7 @@ struct DegreeOps {
   // Chebyshev update with the packed cell-wise inverse D^{-1} = s M^{-1} (FP64 levels):
   //   d = alpha d + s M^{-1} r  (alpha == 0: d not read);  x = d (first) or x += d
   cudaError_t (*cheb_d)(const double* L, const double* r, double alpha, double s, double* d, double* x, int first,
-                        int ncell, cudaStream_t);
+                        int ncell, int* status, cudaStream_t);
   // xf += P xc (coarse nx_c x nz_c cells, fine 2nx_c x 2nz_c); rc = P^T rf
   cudaError_t (*prolong_d)(const double* xc, double* xf, int nxc, int nzc, cudaStream_t);
   cudaError_t (*prolong_f)(const float* xc, float* xf, int nxc, int nzc, cudaStream_t);

@@ -365,7 +365,7 @@ constexpr int kSolveWarps = 4;
 template <class R, int MODE>
 __global__ void __launch_bounds__(32 * kSolveWarps)
     k_mass_solve(const R* __restrict__ Minv, const R* __restrict__ b, R* __restrict__ x, R* __restrict__ dv,
-                 const R scale, const R alpha, const int first, const int ncomp, const int ncell) {
+                 const R scale, const R alpha, const int first, const int ncomp, const int ncell, int* status) {
   constexpr int ND = kND, NPK = kNPK;
   __shared__ alignas(16) R sM[kSolveWarps * NPK];
   __shared__ alignas(16) R sb[kSolveWarps * 2 * ND];
@@ -396,7 +396,11 @@ __global__ void __launch_bounds__(32 * kSolveWarps)
     }
     __syncthreads();  // barrier initialised before anyone waits on it
     const bool ok = mbar_wait(bar, 0);
-    if (__syncthreads_or(!ok)) return;  // never expected; every thread leaves together
+    if (!ok) report_status(status, kStatusStageTimeout);
+    if (__syncthreads_or(!ok)) {  // never expected; every thread leaves together
+      if (threadIdx.x == 0) mbar_wait(bar, 0);  // (bounded) for the copies still in flight
+      return;
+    }
   } else {
     if (c >= ncell) return;  // whole warps only; no block-wide barrier on this path
     const R* mp = Minv + (size_t)c * NPK;
@@ -433,10 +437,10 @@ __global__ void __launch_bounds__(32 * kSolveWarps)
 
 template <class R, int MODE>
 cudaError_t launch_mass_solve(const R* L, int ncomp, const R* b, R scale, R* x, R* d, R alpha, int first, int ncell,
-                              cudaStream_t st) {
+                              int* status, cudaStream_t st) {
   if (ncomp < 1 || ncomp > 2) return cudaErrorInvalidValue;
   k_mass_solve<R, MODE><<<(ncell + kSolveWarps - 1) / kSolveWarps, 32 * kSolveWarps, 0, st>>>(L, b, x, d, scale, alpha,
-                                                                                             first, ncomp, ncell);
+                                                                                             first, ncomp, ncell, status);
   return cudaGetLastError();
 }
 
@@ -551,9 +555,9 @@ cudaError_t mass_factor(const MeshDev& mesh, const double* weight, double* L, in
   return cudaGetLastError();
 }
 
-cudaError_t mass_solve(const double* L, int ncomp, const double* b, double scale, double* x, int ncell,
+cudaError_t mass_solve(const double* L, int ncomp, const double* b, double scale, double* x, int ncell, int* status,
                        cudaStream_t st) {
-  return launch_mass_solve<double, 0>(L, ncomp, b, scale, x, nullptr, 0.0, 0, ncell, st);
+  return launch_mass_solve<double, 0>(L, ncomp, b, scale, x, nullptr, 0.0, 0, ncell, status, st);
 }
 
 // ------------------------------------------------------------------ multigrid kernels
@@ -568,8 +572,9 @@ cudaError_t mg_res(const MeshDev& mesh, const R* w, const R* pf, const R* p, con
 }
 
 template <class R>
-cudaError_t cheb(const R* L, const R* r, R alpha, R s, R* d, R* x, int first, int ncell, cudaStream_t st) {
-  return launch_mass_solve<R, 1>(L, 1, r, s, x, d, alpha, first, ncell, st);
+cudaError_t cheb(const R* L, const R* r, R alpha, R s, R* d, R* x, int first, int ncell, int* status,
+                 cudaStream_t st) {
+  return launch_mass_solve<R, 1>(L, 1, r, s, x, d, alpha, first, ncell, status, st);
 }
 
 template <class R>

@@ -215,12 +215,12 @@ struct Prec<double> {
     return k->mg_res_d(m, w, pf, p, q, r, nc, st);
   }
   static cudaError_t solve(const DegreeOps* k, const double* L, int ncomp, const double* b, double s, double* x,
-                           int nc, cudaStream_t st) {
-    return k->mass_solve(L, ncomp, b, s, x, nc, st);
+                           int nc, int* status, cudaStream_t st) {
+    return k->mass_solve(L, ncomp, b, s, x, nc, status, st);
   }
   static cudaError_t cheb(const DegreeOps* k, const double* L, const double* r, double a, double s, double* d,
-                          double* x, int first, int nc, cudaStream_t st) {
-    return k->cheb_d(L, r, a, s, d, x, first, nc, st);
+                          double* x, int first, int nc, int* status, cudaStream_t st) {
+    return k->cheb_d(L, r, a, s, d, x, first, nc, status, st);
   }
   static cudaError_t prolong(const DegreeOps* k, const double* xc, double* xf, int nxc, int nzc, cudaStream_t st) {
     return k->prolong_d(xc, xf, nxc, nzc, st);
@@ -238,11 +238,11 @@ struct Prec<float> {
     return rq ? k->mg_res_fr(m, w, pf, p, q, r, nc, st) : k->mg_res_f(m, w, pf, p, q, r, nc, st);
   }
   static cudaError_t solve(const DegreeOps* k, const float* W, int ncomp, const float* b, double s, float* x, int nc,
-                           cudaStream_t st) {
+                           int* /*status: no bounded waits in the change-of-basis kernels*/, cudaStream_t st) {
     return k->cob_solve_f(W, ncomp, b, (float)s, x, nc, st);
   }
   static cudaError_t cheb(const DegreeOps* k, const float* W, const float* r, double a, double s, float* d, float* x,
-                          int first, int nc, cudaStream_t st) {
+                          int first, int nc, int* /*status*/, cudaStream_t st) {
     return k->cob_cheb_f(W, r, (float)a, (float)s, d, x, first, nc, st);
   }
   static cudaError_t b_inv(const DegreeOps* k, const MeshDev& m, const float* p, double c, const float* LA, float* w,
@@ -280,7 +280,7 @@ int residual_update(af_schur_solver* s, Level& L, const R* v, R* r) {
     o->launches += 1;
   } else {
     MG_CU(Prec<R>::B(k, L.mesh, v, s->cB, (R*)L.u, L.ncell, o->stream));
-    MG_CU(Prec<R>::solve(k, (const R*)L.LA, 2, (const R*)L.u, 1.0, (R*)L.w, L.ncell, o->stream));
+    MG_CU(Prec<R>::solve(k, (const R*)L.LA, 2, (const R*)L.u, 1.0, (R*)L.w, L.ncell, L.mesh.status, o->stream));
     o->launches += 2;
   }
   MG_CU(Prec<R>::res(k, L.mesh, (const R*)L.w, (const R*)L.pfR, v, s->cdt, r, L.ncell, o->stream, s->rq));
@@ -309,7 +309,7 @@ int chebyshev(af_schur_solver* s, Level& L, int degree, double lo, double hi, bo
       // kernel needs no D term (ResChebZPhys).  Same iteration as below up to rounding.
       R* z = r;
       // d = x = D^{-1} b / theta;  z = D^{-1} b = theta d
-      MG_CU(Prec<R>::cheb(k, (const R*)L.LM, b, 0.0, ginv / theta, d, x, 1, L.ncell, o->stream));
+      MG_CU(Prec<R>::cheb(k, (const R*)L.LM, b, 0.0, ginv / theta, d, x, 1, L.ncell, L.mesh.status, o->stream));
       k_scale_to<R><<<nblocks(L.ns), kThreads, 0, o->stream>>>(d, (R)theta, z, L.ns);
       MG_CU(cudaGetLastError());
       o->launches += 2;
@@ -330,7 +330,7 @@ int chebyshev(af_schur_solver* s, Level& L, int degree, double lo, double hi, bo
   }
   MG_CU(cudaMemcpyAsync(r, b, sizeof(R) * L.ns, cudaMemcpyDeviceToDevice, o->stream));
   if (!zero_init) MG_AF(residual_update<R>(s, L, x, r));
-  MG_CU(Prec<R>::cheb(k, (const R*)L.LM, r, 0.0, ginv / theta, d, x, zero_init ? 1 : 0, L.ncell, o->stream));
+  MG_CU(Prec<R>::cheb(k, (const R*)L.LM, r, 0.0, ginv / theta, d, x, zero_init ? 1 : 0, L.ncell, L.mesh.status, o->stream));
   o->launches += 1;
   double rho_old = 1.0 / sigma;
   for (int it = 1; it < degree; ++it) {
@@ -345,7 +345,7 @@ int chebyshev(af_schur_solver* s, Level& L, int degree, double lo, double hi, bo
       std::swap(d, dn);
     } else {
       MG_AF(residual_update<R>(s, L, d, r));
-      MG_CU(Prec<R>::cheb(k, (const R*)L.LM, r, a, sc, d, x, 0, L.ncell, o->stream));
+      MG_CU(Prec<R>::cheb(k, (const R*)L.LM, r, a, sc, d, x, 0, L.ncell, L.mesh.status, o->stream));
       o->launches += 1;
     }
     rho_old = rho;
@@ -388,14 +388,14 @@ int estimate_lmax(af_schur_solver* s, Level& L) {
   for (int it = 0; it < s->opt.eig_iterations; ++it) {
     MG_CU(cudaMemsetAsync(r, 0, sizeof(R) * L.ns, o->stream));
     MG_AF(residual_update<R>(s, L, v, r));  // r = -S0 v
-    MG_CU(Prec<R>::solve(k, (const R*)L.LM, 1, r, -1.0 / kG1, v, L.ncell, o->stream));  // v = D^{-1} S0 v
+    MG_CU(Prec<R>::solve(k, (const R*)L.LM, 1, r, -1.0 / kG1, v, L.ncell, L.mesh.status, o->stream));  // v = D^{-1} S0 v
     MG_CU(norm2<R>(v, L.ns, s->part, s->scal, o->stream));
     k_normalize<R><<<nblocks(L.ns), kThreads, 0, o->stream>>>(v, v, L.ns, s->scal);
     o->launches += 7;
   }
   double n2 = 0.0;
   MG_CU(cudaMemcpyAsync(&n2, s->scal, sizeof(double), cudaMemcpyDeviceToHost, o->stream));
-  MG_CU(cudaStreamSynchronize(o->stream));
+  MG_AF(sync_checked(o, o->stream));
   if (!std::isfinite(n2) || n2 <= 0.0) return merr(AF_NAN, "multigrid: eigenvalue estimate failed");
   L.lmax = std::sqrt(n2);
   return AF_OK;
@@ -662,7 +662,7 @@ int fgmres(af_schur_solver* s, const Apply& A, double* x, const double* b, doubl
   auto Hs = [&](int i, int j) -> double& { return H[i * m + j]; };
   auto read_scalar = [&](double* v) -> int {
     MG_CU(cudaMemcpyAsync(v, s->scal, sizeof(double), cudaMemcpyDeviceToHost, st));
-    MG_CU(cudaStreamSynchronize(st));
+    MG_AF(sync_checked(o, st));
     return AF_OK;
   };
   double bb = 0.0;

@@ -16,6 +16,10 @@
 // previous call's contents, so this file clears what must start at zero (the CG iterate)
 // and overwrites everything else before reading it.
 //
+// The call returns once its work is done on the stream: the inner CG reads its state back every
+// 8 iterations, and a last read of the kernels' status word (a bounded wait that gave up:
+// AF_TIMEOUT) waits for C.
+//
 // Set-up: the first call on a device (with that device current) looks up the array's
 // device address with cudaGetSymbolAddress and uploads the degree's basis tables; make
 // that first call before any other work that must not be interrupted by set-up.
@@ -46,6 +50,9 @@ static __device__ __align__(256) double g_schur_scratch[kScratchDoubles];
 std::mutex g_mu;
 double* g_scratch_ptr[kMaxDevices] = {nullptr};
 bool g_tables_ready[kMaxDevices][8] = {{false}};
+
+constexpr const char* kTimeoutMessage =
+    "af_schur_apply_noalloc: a kernel gave up a bounded wait for its staged inputs; dst is not valid";
 
 int err(int code, const char* msg) {
   set_last_error(msg);
@@ -105,19 +112,26 @@ extern "C" int af_schur_apply_noalloc(int nx, int nz, int periodic_x, const doub
   double* invd = scratch + 6 * nu;  // inverse diagonal of A
   double* part = scratch + 7 * nu;  // reduction partials (4 * kMaxPartials)
   KrylovState* kst = reinterpret_cast<KrylovState*>(part + 4 * kMaxPartials);
+  // the kernels' status word (a bounded wait that gave up), after the solver state in the
+  // 16 reserved doubles
+  static_assert(sizeof(KrylovState) <= 14 * sizeof(double), "solver state overlaps the status word");
+  int* status = reinterpret_cast<int*>(part + 4 * kMaxPartials + 14);
+  int h_status = 0;
 
   MeshDev mesh{};
   mesh.vtx = reinterpret_cast<const double2*>(vertices);
   mesh.nx = nx;
   mesh.nz = nz;
   mesh.periodic_x = periodic_x ? 1 : 0;
+  mesh.status = status;
   const int ncell = nx * nz;
   // euler_operator.h:1428, 1526 and the tableau at :233-240
   const double gamma = 2.0 - std::sqrt(2.0);
   const double coeff = hyperbolic_stage == 1 ? 0.5 * gamma : 1.0 - std::sqrt(2.0) / 2.0;
   const int maxit = 10000;
   cudaError_t e;
-  if ((e = ops->inv_diag(mesh, 2, rho_for_fixed, 1.0, invd, ncell, st)) != cudaSuccess ||
+  if ((e = cudaMemsetAsync(status, 0, sizeof(int), st)) != cudaSuccess ||
+      (e = ops->inv_diag(mesh, 2, rho_for_fixed, 1.0, invd, ncell, st)) != cudaSuccess ||
       (e = ops->op_B(mesh, src, coeff * dt / (Mach * Mach), t1, ncell, st)) != cudaSuccess ||
       (e = cudaMemsetAsync(t2, 0, nu * sizeof(double), st)) != cudaSuccess ||
       (e = cg_start(kst, t1, nullptr, invd, rv, zv, pv, nu, part, 1e-12, 1, st)) != cudaSuccess)
@@ -130,8 +144,10 @@ extern "C" int af_schur_apply_noalloc(int nx, int nz, int periodic_x, const doub
         return err(AF_CUDA, cudaGetErrorString(e));
     }
     if ((e = cudaMemcpyAsync(&hs, kst, sizeof(hs), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
       return err(AF_CUDA, cudaGetErrorString(e));
+    if (h_status != 0) return err(AF_TIMEOUT, kTimeoutMessage);
     if (hs.done) break;
   }
   if (inner_iterations) *inner_iterations = hs.its;
@@ -141,7 +157,10 @@ extern "C" int af_schur_apply_noalloc(int nx, int nz, int periodic_x, const doub
   cp.cdt = coeff * dt;
   cp.g1 = 1.0 / (1.4 - 1.0);
   cp.gg = 1.4 / (1.4 - 1.0);
-  if ((e = ops->op_C(mesh, t2, pres_fixed, src, cp, dst, ncell, st)) != cudaSuccess)
+  if ((e = ops->op_C(mesh, t2, pres_fixed, src, cp, dst, ncell, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
     return err(AF_CUDA, cudaGetErrorString(e));
+  if (h_status != 0) return err(AF_TIMEOUT, kTimeoutMessage);
   return AF_OK;
 }

@@ -16,7 +16,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libaf_gpu.so")
 
-AF_OK, AF_BAD_ARG, AF_CUDA, AF_NO_CONVERGENCE, AF_NAN, AF_UNSUPPORTED, AF_NO_DEVICE = range(7)
+AF_OK, AF_BAD_ARG, AF_CUDA, AF_NO_CONVERGENCE, AF_NAN, AF_UNSUPPORTED, AF_NO_DEVICE, AF_TIMEOUT = range(8)
 
 _lib = None
 
@@ -66,6 +66,7 @@ def lib():
             getattr(L, name).argtypes = [vp, dp, dp, dp]
         L.af_compute_diagnostics.argtypes = [vp, dp, dp, dp, dp, ctypes.POINTER(Diagnostics)]
         L.af_l2_norm.argtypes = [vp, ip, dp, ctypes.POINTER(ctypes.c_double)]
+        L.af_set_stage_wait_test.argtypes = [vp, ip]
         L.af_error_string.restype = ctypes.c_char_p
         L.af_error_string.argtypes = [ip]
         L.af_last_error_message.restype = ctypes.c_char_p
@@ -271,6 +272,11 @@ class EULEROperator:
         out = ctypes.c_double()
         check(lib().af_l2_norm(self._h, ncomp, _ptr(v), ctypes.byref(out)))
         return out.value
+
+    def set_stage_wait_test(self, polls):
+        """Test hook: polls > 0 makes the handle's cell kernels give up a bounded wait (before any
+        copy is issued) after that many polls; 0 restores normal operation."""
+        check(lib().af_set_stage_wait_test(self._h, polls))
 
     def set_schur_mode(self, mode=0, rel_tol=1e-12, max_iter=10000):
         check(lib().af_set_schur_mode(self._h, mode, rel_tol, max_iter))

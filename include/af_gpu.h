@@ -27,7 +27,11 @@ enum {
   AF_NO_CONVERGENCE = 3,   /* SolverControl::NoConvergence of the reference       */
   AF_NAN = 4,              /* NaN/Inf met in a Krylov recurrence                  */
   AF_UNSUPPORTED = 5,      /* degree not compiled into this library               */
-  AF_NO_DEVICE = 6         /* no CUDA device available                            */
+  AF_NO_DEVICE = 6,        /* no CUDA device available                            */
+  AF_TIMEOUT = 7           /* a kernel gave up a bounded wait for its staged
+                              inputs and left its outputs unwritten (reported by
+                              the next call on the handle, or by the call that
+                              synchronizes; see af_synchronize)                    */
 };
 
 typedef struct af_operator af_operator;
@@ -140,6 +144,17 @@ int af_last_inner_iterations(const af_operator* op, int* its);
 int af_n_dofs(const af_operator* op, int space, long long* n);
 /* Number of kernels this library launched on the handle since creation. */
 int af_launch_count(const af_operator* op, long long* n);
+
+/* Failure detection (no counterpart in the reference, whose deal.II loops have no waits):
+ * the cell kernels wait for their bulk copies with a bounded number of polls.  A kernel that
+ * gives up leaves a code in the handle's status word and returns without writing its
+ * outputs; the next call on the handle (any call that queues work, af_synchronize, and every
+ * call that synchronizes internally: solves, IMEX steps, host-buffer applies, diagnostics)
+ * then returns AF_TIMEOUT once and clears the word.
+ * Test hook: polls > 0 makes every cell kernel of this handle first wait on a barrier phase
+ * that nothing completes and give up after that many polls, before it issues any copy (the
+ * timeout path without copies in flight); 0 restores normal operation. */
+int af_set_stage_wait_test(af_operator* op, int polls);
 
 /* ---------------------------------------------------------------- Schur pressure solver
  * Solves the NS_stage-2 system (D - C A^{-1} B) p = b of af_vmult, the linear solve of the

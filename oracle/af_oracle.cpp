@@ -176,6 +176,11 @@ struct Op {
   N gamma, a21, a22, a31, a32, a33, a21t, a22t, a31t, a32t, a33t, b1, b2, b3;
   int hyperbolic_stage = 1, ns_stage = 1;
   std::vector<N> rho_for_fixed, pres_fixed, u_fixed;
+  // exact_inverse = 1: the mass-type systems (M, A, D) and the A^{-1} inside the Schur apply
+  // are solved by dense cell-wise Cholesky factors instead of CG (the library's default
+  // configuration); factors of M and of A(rho_for_fixed), rebuilt when emptied
+  int exact_inverse = 0;
+  std::vector<N> M_chol, A_chol;
   int ncell() const { return nx * nz; }
   int nd() const { return (P + 1) * (P + 1); }
   long nscalar() const { return (long)ncell() * nd(); }
@@ -982,13 +987,92 @@ static int vmult(Op<N>& o, N* dst, const N* src) {
     mass_apply(o, y.data(), x.data(), 2, o.rho_for_fixed.data(), (N)1);
   };
   auto jac = [&](std::vector<N>& z, const std::vector<N>& r) { for (long i = 0; i < nu; ++i) z[i] = invd[i] * r[i]; };
-  int its = pcg<N>(Aop, jac, tmp2, tmp1, tol, 10000);
+  int its = 0;
+  if (o.exact_inverse) inverse_exact(o, 3, tmp2.data(), tmp1.data());
+  else its = pcg<N>(Aop, jac, tmp2, tmp1, tol, 10000);
   apply_C(o, tmp3.data(), tmp2.data());
   for (long i = 0; i < o.nscalar(); ++i) dst[i] -= tmp3[i];
   o.ns_stage = saved;
   return its;
 }
 
+
+/* Exact cell-wise inverses of the block-diagonal mass-type operators (no counterpart in the
+ * reference, which solves them with CG + Jacobi or multigrid; the library solves them exactly
+ * per cell).  The cell matrix of mass_apply on the same quadrature, M_ij = sum_q JxW_q w_q
+ * phi_i(q) phi_j(q), factored by Cholesky; the factors of all cells are stored in L. */
+template <typename N>
+static void mass_factor_exact(const Op<N>& o, const N* weight_field, std::vector<N>& L) {
+  const int nd = o.nd(), P1 = o.P + 1, NQ = o.NQ, n2 = NQ * NQ;
+  L.assign((size_t)o.ncell() * nd * nd, (N)0);
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < o.ncell(); ++c) {
+    CellQ<N> cq; cell_quad(o, c, cq);
+    std::vector<N> w;
+    if (weight_field) eval_scalar(o, weight_field, c, w);
+    N* A = L.data() + (size_t)c * nd * nd;
+    for (int i = 0; i < nd; ++i)
+      for (int j = 0; j <= i; ++j) {
+        N s = 0;
+        for (int q = 0; q < n2; ++q) {
+          const int qz = q / NQ, qx = q % NQ;
+          const N pi = o.B.S[qz * P1 + i / P1] * o.B.S[qx * P1 + i % P1];
+          const N pj = o.B.S[qz * P1 + j / P1] * o.B.S[qx * P1 + j % P1];
+          s += cq.JxW[q] * (weight_field ? w[q] : (N)1) * pi * pj;
+        }
+        A[i * nd + j] = s;
+      }
+    for (int k = 0; k < nd; ++k) {  // in place: the lower triangle becomes the Cholesky factor
+      N d = A[k * nd + k];
+      for (int m = 0; m < k; ++m) d -= A[k * nd + m] * A[k * nd + m];
+      d = std::sqrt(d);
+      A[k * nd + k] = d;
+      for (int i = k + 1; i < nd; ++i) {
+        N v = A[i * nd + k];
+        for (int m = 0; m < k; ++m) v -= A[i * nd + m] * A[k * nd + m];
+        A[i * nd + k] = v / d;
+      }
+    }
+  }
+}
+
+/* x = scale * M_K^{-1} b per cell and component with the factors of mass_factor_exact */
+template <typename N>
+static void mass_solve_exact(const Op<N>& o, const std::vector<N>& L, N* x, const N* b, int ncomp, N scale) {
+  const int nd = o.nd();
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < o.ncell(); ++c) {
+    const N* A = L.data() + (size_t)c * nd * nd;
+    std::vector<N> y(nd);
+    for (int d = 0; d < ncomp; ++d) {
+      const N* bb = b + ((long)c * ncomp + d) * nd;
+      N* xx = x + ((long)c * ncomp + d) * nd;
+      for (int i = 0; i < nd; ++i) {
+        N v = bb[i];
+        for (int m = 0; m < i; ++m) v -= A[i * nd + m] * y[m];
+        y[i] = v / A[i * nd + i];
+      }
+      for (int i = nd - 1; i >= 0; --i) {
+        N v = y[i];
+        for (int m = i + 1; m < nd; ++m) v -= A[m * nd + i] * xx[m];
+        xx[i] = v / A[i * nd + i];
+      }
+      for (int i = 0; i < nd; ++i) xx[i] *= scale;
+    }
+  }
+}
+
+/* x = Op^{-1} b exactly for the mass-type operator of NS stage ns (1/4: M, 3/5: A, 6: D) */
+template <typename N>
+static void inverse_exact(Op<N>& o, int ns, N* x, const N* b) {
+  if (ns == 3 || ns == 5) {
+    if (o.A_chol.empty()) mass_factor_exact(o, o.rho_for_fixed.data(), o.A_chol);
+    mass_solve_exact(o, o.A_chol, x, b, 2, (N)1);
+  } else {
+    if (o.M_chol.empty()) mass_factor_exact(o, (const N*)nullptr, o.M_chol);
+    mass_solve_exact(o, o.M_chol, x, b, 1, ns == 6 ? (N)CP_CV - 1 : (N)1);
+  }
+}
 
 template <typename N>
 static void rhs_rho_fn(const Op<N>& o, std::vector<N>& dst, const std::vector<const N*>& src) {
@@ -1020,6 +1104,10 @@ static std::vector<N> invdiag_of(Op<N>& o, int ns) {
 // SolverCG with Jacobi, tol = eps*|b|
 template <typename N>
 static int cg_abs(Op<N>& o, int ns, std::vector<N>& x, const std::vector<N>& b, N eps, int maxit) {
+  if (o.exact_inverse) {  // the library's default: exact cell-wise inverses
+    inverse_exact(o, ns, x.data(), b.data());
+    return 0;
+  }
   std::vector<N> invd = invdiag_of(o, ns);
   int saved = o.ns_stage;
   o.ns_stage = ns;
@@ -1175,16 +1263,19 @@ static void imex_step(Op<N>& o, Imex& im, std::vector<N>& rho0, std::vector<N>& 
   };
   density(1, rho2, rho0);
   o.rho_for_fixed = rho2;
+  o.A_chol.clear();
   pfix_old = p0;
   ufix = u0;
   fixed_point(1, p2, u2);
   density(2, rho3, rho2);
   o.rho_for_fixed = rho3;
+  o.A_chol.clear();
   pfix_old = p2;
   ufix = u2;
   fixed_point(2, p3, u3);
   density(3, rhoc, rho3);
   o.rho_for_fixed = rhoc;
+  o.A_chol.clear();
   o.hyperbolic_stage = 3;
   {
     std::vector<const N*> su = {rho0.data(), u0.data(), p0.data(), rho2.data(), u2.data(), p2.data(), rho3.data(),
@@ -1382,7 +1473,7 @@ extern "C" {
 /* nsteps IMEX steps on (rho, u, p) in place (double instance only); fp_iters receives the
    fixed-point iteration counts of stages 1 and 2 of the last step. */
 int orc_imex_steps(void* h, double* rho, double* u, double* p, int nsteps, double eps, int maxit, double fp_tol,
-                   int fp_max, int restart, int* fp_iters, int true_residual) {
+                   int fp_max, int restart, int* fp_iters, int true_residual, int exact_inverse) {
   OrcHandle* H = (OrcHandle*)h;
   if (H->ld) return -1;
   Op<double>& o = *H->d;
@@ -1391,7 +1482,11 @@ int orc_imex_steps(void* h, double* rho, double* u, double* p, int nsteps, doubl
   Imex im;
   im.eps = eps; im.maxit = maxit; im.fp_tol = fp_tol; im.fp_max = fp_max; im.restart = restart;
   im.true_residual = true_residual;
+  o.exact_inverse = exact_inverse;
+  o.A_chol.clear();
   for (int k = 0; k < nsteps; ++k) imex_step(o, im, r, uu, pp);
+  o.exact_inverse = 0;
+  o.A_chol.clear();
   std::copy(r.begin(), r.end(), rho);
   std::copy(uu.begin(), uu.end(), u);
   std::copy(pp.begin(), pp.end(), p);

@@ -51,7 +51,7 @@ def lib():
         L.orc_imex_steps.restype = ctypes.c_int
         L.orc_imex_steps.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                      ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
-                                     ctypes.c_int]
+                                     ctypes.c_int, ctypes.c_int]
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         L.orc_get_num_threads.restype = ctypes.c_int
         _lib = L
@@ -180,14 +180,17 @@ class OracleOperator:
 
 
 def imex_steps(op: OracleOperator, rho, u, p, nsteps, eps=1e-8, max_iterations=30000, fixed_point_tol=1e-10,
-               fixed_point_max_iterations=100, gmres_restart=28, true_residual=False):
+               fixed_point_max_iterations=100, gmres_restart=28, true_residual=False, exact_inverse=False):
     """EulerSolver::run time steps (Atmospheric_Flow.cc:1110-1251) on the CPU; returns the new
     (rho, u, p) and the fixed-point iteration counts of stages 1 and 2 of the last step.
     true_residual: the pressure GMRES is right-preconditioned and stops on |b - S x| (the
-    criterion of the library's af_schur_solve) instead of the reference's |P^{-1} r|."""
+    criterion of the library's af_schur_solve) instead of the reference's |P^{-1} r|.
+    exact_inverse: the mass-type systems and the A^{-1} inside the Schur apply are solved by
+    dense cell-wise Cholesky factors (the library's default) instead of CG + Jacobi."""
     rho, u, p = _c(rho).copy(), _c(u).copy(), _c(p).copy()
     fp = (ctypes.c_int * 2)()
     r = lib().orc_imex_steps(op._h, _p(rho), _p(u), _p(p), nsteps, eps, max_iterations, fixed_point_tol,
-                             fixed_point_max_iterations, gmres_restart, fp, int(bool(true_residual)))
+                             fixed_point_max_iterations, gmres_restart, fp, int(bool(true_residual)),
+                             int(bool(exact_inverse)))
     assert r == 0
     return rho, u, p, (fp[0], fp[1])

@@ -33,6 +33,15 @@ def test_error_strings():
     L = O.lib()
     assert L.af_error_string(O.AF_OK) == b"ok"
     assert L.af_error_string(O.AF_NO_CONVERGENCE) == b"no convergence"
+    assert L.af_error_string(O.AF_TIMEOUT) == b"a kernel gave up a bounded wait"
+
+
+def test_stage_wait_test_hook_validates_on_host():
+    """The failure-detection test hook rejects a null handle and negative poll counts
+    without touching a device."""
+    from atmospheric_flows_b200 import operator as O
+    L = O.lib()
+    assert L.af_set_stage_wait_test(None, 4) == O.AF_BAD_ARG
 
 
 def test_create_rejects_bad_arguments_on_host():

@@ -41,42 +41,51 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.mark.parametrize("stage", [1, 2])
-def test_noalloc_schur_matches_handle_path(stage):
+@pytest.mark.parametrize("degree,periodic,stage", [(4, 0, 1), (4, 0, 2), (4, 1, 1), (2, 1, 2), (5, 0, 1),
+                                                    (5, 1, 2)])
+def test_noalloc_schur_matches_handle_path(degree, periodic, stage):
+    """The no-allocation call runs first, before this test creates a handle of the degree, so
+    that in a fresh process its own per-device set-up (symbol address, basis tables) is the
+    path under test."""
     from atmospheric_flows_b200.operator import EULEROperator, AF_OK
     L = _lib()
-    P = 4
-    m = M.jitter_mesh(M.hill_mesh(12, 6), 0.15, seed=21)
+    P = degree
+    nx, nz = (12, 6) if P <= 4 else (8, 6)  # 8x6 cells at degree 5: 1728 pressure DoFs
+    m = M.jitter_mesh(M.hill_mesh(nx, nz, periodic_x=bool(periodic)), 0.15, seed=21)
     sc = M.Scaling()
     dt = 3.0
     ns = m.n_cells * (P + 1) ** 2
-    rng = np.random.default_rng(7 + stage)
+    rng = np.random.default_rng(7 + stage + 10 * P + 100 * periodic)
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     rho_f = dev(1.0 + 0.05 * rng.standard_normal(ns))
     p_f = dev(1.0 + 0.05 * rng.standard_normal(ns))
     vtx = dev(m.vertices.reshape(-1))
+    stream = torch.cuda.current_stream()
+    srcs = [dev(1.0 + 0.1 * rng.standard_normal(ns)) for _ in range(2)]
+    got, its = [], []
+    for call in range(2):  # two calls in a row, different inputs
+        out = torch.full((ns,), np.nan, dtype=torch.float64, device="cuda")
+        it = ctypes.c_int(-1)
+        torch.cuda.synchronize()
+        st = L.af_schur_apply_noalloc(m.nx, m.nz, int(m.periodic_x), _p(vtx), P, sc.Ma, dt, stage, _p(rho_f),
+                                      _p(p_f), _p(srcs[call]), _p(out), ctypes.c_void_p(stream.cuda_stream),
+                                      ctypes.byref(it))
+        assert st == AF_OK, L.af_last_error_message()
+        torch.cuda.synchronize()
+        got.append(out.cpu().numpy())
+        its.append(it.value)
 
     op = EULEROperator(m, P, sc.Ma, sc.Fr, dt)
     op.set_rho_for_fixed(rho_f)
     op.set_pres_fixed(p_f)
     op.set_HYPERBOLIC_stage(stage)
     op.set_NS_stage(2)
-    stream = torch.cuda.current_stream()
-    for call in range(2):  # two calls in a row, different inputs
-        src = dev(1.0 + 0.1 * rng.standard_normal(ns))
+    for call in range(2):
         want = torch.zeros(ns, dtype=torch.float64, device="cuda")
-        op.vmult(want, src)
+        op.vmult(want, srcs[call])
         op.synchronize()
-        got = torch.full((ns,), np.nan, dtype=torch.float64, device="cuda")
-        its = ctypes.c_int(-1)
-        torch.cuda.synchronize()
-        st = L.af_schur_apply_noalloc(m.nx, m.nz, int(m.periodic_x), _p(vtx), P, sc.Ma, dt, stage, _p(rho_f),
-                                      _p(p_f), _p(src), _p(got), ctypes.c_void_p(stream.cuda_stream),
-                                      ctypes.byref(its))
-        assert st == AF_OK, L.af_last_error_message()
-        torch.cuda.synchronize()
-        assert its.value == op.last_inner_iterations() > 0
-        err = rel(got.cpu().numpy(), want.cpu().numpy())
+        assert its[call] == op.last_inner_iterations() > 0
+        err = rel(got[call], want.cpu().numpy())
         assert err < TOL, (call, err)
 
 
