@@ -9,8 +9,9 @@ all four outputs copied back, every step).  The inputs (7 scalar FP64 fields, 18
 outputs (105 MB) exceed the 126 MB L2, so no L2 flush is needed between steps.
 N > 1: one process per GPU (torchrun), independent replicas ("replicas only": the
 operator apply has no cross-GPU exchange in this library), max time over ranks.
---impl reference: the CPU restatement of the reference operators (the reference itself
-needs deal.II, which is not installable here) on the host cores, same metric.
+--impl reference: the tuned CPU port of the same apply (oracle/af_cpu_port.cpp, checked against
+the CPU oracle; the reference itself needs deal.II, which is not installable here) on all host
+cores, on the same 512x32 strip as the cpu_baseline leg, same metric.
 Rank 0 also reports the second half of the metric (`imex`: s per IMEX step, FP64 vs mixed
 precision at the same solver tolerance) and the Schur pressure solve (`schur_solve`).
 """
@@ -140,66 +141,82 @@ class Clocks:
                 "window": "timed region" if inside else "around the timed region (shorter than the sampling interval)"}
 
 
-def cpu_baseline_oracle(rows, repeats, threads):
-    """The oracle (CPU restatement) on a horizontal strip of the workload mesh."""
-    from oracle.oracle import OracleOperator, set_num_threads
+CPU_ROWS = 32  # the CPU sample: a 512x32 strip of the workload mesh, 1/8 of its cells
+
+
+def cpu_sample(rows=CPU_ROWS):
+    """The strip both CPU measurements and the parity check run on: the bottom `rows` rows of
+    the hill domain (same x extent and cell width, top at 16 km * rows / 256), the workload's
+    state construction."""
     from atmospheric_flows_b200 import mesh as M
-    set_num_threads(threads)
     m = M.hill_mesh(NX, rows, top=16000.0 * rows / NZ)
     st = M.hill_state(m, DEGREE, seed=SEED)
-    st2 = M.hill_state(m, DEGREE, seed=SEED + 1)
+    st2 = M.hill_state(m, DEGREE, seed=SEED + 1, modes=4)
+    return m, [st.rho, st.u, st.p, st2.rho, st2.u]
+
+
+def cpu_sample_label(rows=CPU_ROWS):
+    return (f"{NX}x{rows} strip of the {NX}x{NZ} workload mesh (1/{NZ // rows} of its cells) per step, the same "
+            f"strip in the reference arm and in the cpu_baseline leg")
+
+
+def time_cpu_port(m, src, warmup, steps, threads):
+    """Mean seconds per fused stage-1 apply of the tuned CPU port (oracle/af_cpu_port.cpp:
+    sum factorisation vectorised over cells, each face once, OpenMP) on the host cores."""
+    from oracle.oracle import cpu_port_rhs_fused_stage1, set_num_threads
+    from atmospheric_flows_b200 import mesh as M
+    set_num_threads(threads)
     sc = M.Scaling()
-    o = OracleOperator(m, DEGREE, sc.Ma, sc.Fr, 2.0)
-    o.set_HYPERBOLIC_stage(STAGE)
-    src = [st.rho, st.u, st.p, st2.rho, st2.u]
+    f = lambda: cpu_port_rhs_fused_stage1(m, DEGREE, sc.Ma, sc.Fr, 2.0, src)
+    for _ in range(max(1, warmup)):
+        f()
+    t = time.perf_counter()
+    for _ in range(steps):
+        f()
+    return (time.perf_counter() - t) / steps
 
-    def one():
-        o.vmult_rhs_rho_update(src[:2])
-        o.vmult_rhs_velocity_fixed(src[:4])
-        o.vmult_rhs_pressure(src)
 
-    one()
-    best = 1e30
-    for _ in range(repeats):
-        t = time.perf_counter()
-        one()
-        best = min(best, time.perf_counter() - t)
-    dofs = 4 * m.n_cells * (DEGREE + 1) ** 2
-    return dofs / best / 1e9, m
+CPU_NOTE = ("tuned CPU port of the fused stage-1 rhs (oracle/af_cpu_port.cpp: sum factorisation vectorised over "
+            "batches of 4 cells, each face once, OpenMP; checked against the oracle at 1e-12); the reference "
+            "itself needs deal.II >= 9.3 + MPI + p4est, unavailable here")
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    from oracle.oracle import OracleOperator, set_num_threads
-    from atmospheric_flows_b200 import mesh as M
-    set_num_threads(threads)
-    rows = 16
-    m = M.hill_mesh(NX, rows, top=16000.0 * rows / NZ)
-    st = M.hill_state(m, DEGREE, seed=SEED)
-    st2 = M.hill_state(m, DEGREE, seed=SEED + 1)
-    sc = M.Scaling()
-    o = OracleOperator(m, DEGREE, sc.Ma, sc.Fr, 2.0)
-    o.set_HYPERBOLIC_stage(STAGE)
-    src = [st.rho, st.u, st.p, st2.rho, st2.u]
-    for _ in range(args.warmup):
-        o.vmult_rhs_rho_update(src[:2]); o.vmult_rhs_velocity_fixed(src[:4]); o.vmult_rhs_pressure(src)
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        o.vmult_rhs_rho_update(src[:2]); o.vmult_rhs_velocity_fixed(src[:4]); o.vmult_rhs_pressure(src)
-    dt = (time.perf_counter() - t) / args.steps
+    m, src = cpu_sample()
+    dt = time_cpu_port(m, src, args.warmup, args.steps, threads)
     dofs = 4 * m.n_cells * (DEGREE + 1) ** 2
     v = dofs / dt / 1e9
-    sample = f"{NX}x{rows} strip of the {NX}x{NZ} mesh (1/{NZ // rows} of the workload) per step"
     line = {"metric": METRIC, "value": v, "unit": "GDoF/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(),
-            "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": threads, "kind": "port", "sample": sample,
-                             "note": "CPU restatement of euler_operator.h (oracle/af_oracle.cpp); the reference "
-                                     "needs deal.II >= 9.3 + MPI + p4est, unavailable here"},
+            "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": threads, "kind": "port",
+                             "sample": cpu_sample_label(), "note": CPU_NOTE},
             "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def strip_parity(dev, stream):
+    """GPU fused apply vs the oracle on the identical CPU-sample strip: the largest relative L2
+    difference over the density, velocity and pressure outputs."""
+    import torch
+    from atmospheric_flows_b200 import mesh as M
+    from atmospheric_flows_b200.operator import EULEROperator
+    from oracle.oracle import OracleOperator
+    m, src = cpu_sample()
+    sc = M.Scaling()
+    ns = m.n_cells * (DEGREE + 1) ** 2
+    op = EULEROperator(m, DEGREE, sc.Ma, sc.Fr, 2.0, stream=stream)
+    op.set_HYPERBOLIC_stage(STAGE)
+    out = [torch.empty(k * ns, dtype=torch.float64, device=dev) for k in (1, 2, 1)]
+    op.vmult_rhs_fused(*out, [torch.from_numpy(a).to(dev) for a in src])
+    stream.synchronize()
+    o = OracleOperator(m, DEGREE, sc.Ma, sc.Fr, 2.0)
+    o.set_HYPERBOLIC_stage(STAGE)
+    want = [o.vmult_rhs_rho_update(src[:2]), o.vmult_rhs_velocity_fixed(src[:4]), o.vmult_rhs_pressure(src)]
+    return max(float(np.linalg.norm(g.cpu().numpy() - w) / np.linalg.norm(w)) for g, w in zip(out, want))
 
 
 def time_device(op, bufs, src, stream, K, W):
@@ -292,7 +309,7 @@ def run_solvers(dev):
             if name != "fp64":  # max over the density, velocity and pressure fields
                 steps[name]["rel_error_vs_fp64"] = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
                                                        for a, b in zip(states[name], states["fp64"]))
-        return steps
+        return steps, states
 
     # ---- stage-1 tangent-linear and adjoint (af_imex_stage1_*), same mesh, wall clock
     g = IMEXStepper(m, P, sc.Ma, sc.Fr, dt, eps=1e-10, schur_preconditioner="cheb_fp32")
@@ -389,22 +406,30 @@ def run_solvers(dev):
         "speedup_mixed_vs_fp64": prod["fp64"]["s_per_step"] / prod["mixed"]["s_per_step"],
     }
     del pstates
-    steps = imex_case(1e-8, (("fp64", "jacobi"), ("mixed", "cheb_fp32"), ("reference_criterion", -1)))
-    tight = imex_case(1e-10, (("fp64", "jacobi"), ("mixed", "cheb_fp32")))
+    steps, _ = imex_case(1e-8, (("fp64", "jacobi"), ("fp64_cheb", "cheb_fp64"), ("mixed", "cheb_fp32"),
+                                ("reference_criterion", -1)))
+    tight, tight_states = imex_case(1e-10, (("fp64", "jacobi"), ("fp64_cheb", "cheb_fp64"), ("mixed", "cheb_fp32")))
     out["imex"] = {
         "config": f"periodic hill {nx}x{nz}, degree {P}, dt={dt} s, 1 warm-up + {nsteps} timed steps; "
-                  "fp64: Schur FGMRES + Jacobi (FP64); mixed: Schur FGMRES (FP64) + FP32 Chebyshev polynomial "
-                  "preconditioner (degree 20, cell inverses by change of basis), both to |b - S p| <= eps |b|; "
+                  "fp64: Schur FGMRES + Jacobi (FP64); fp64_cheb: Schur FGMRES + the same Chebyshev polynomial "
+                  "preconditioner in FP64 (like for like: precision is the only difference to mixed); mixed: "
+                  "Schur FGMRES (FP64) + FP32 Chebyshev polynomial preconditioner (degree 20, cell inverses by "
+                  "change of basis), all to |b - S p| <= eps |b|; "
                   "reference_criterion: the reference's left-Jacobi GMRES stopping on |D^-1 r| <= eps |b| (a "
                   "looser criterion, shown for scale)",
         "eps": 1e-8,
         "results": steps,
         "speedup_mixed_vs_fp64": steps["fp64"]["s_per_step"] / steps["mixed"]["s_per_step"],
+        "speedup_mixed_vs_fp64_cheb": steps["fp64_cheb"]["s_per_step"] / steps["mixed"]["s_per_step"],
         "tight": {
             "eps": 1e-10,
             "results": tight,
             "speedup_mixed_vs_fp64": tight["fp64"]["s_per_step"] / tight["mixed"]["s_per_step"],
+            "speedup_mixed_vs_fp64_cheb": tight["fp64_cheb"]["s_per_step"] / tight["mixed"]["s_per_step"],
             "field_error_mixed_vs_fp64": tight["mixed"]["rel_error_vs_fp64"],
+            "field_error_mixed_vs_fp64_cheb": max(
+                float(torch.linalg.norm(a_ - b_) / torch.linalg.norm(b_))
+                for a_, b_ in zip(tight_states["mixed"], tight_states["fp64_cheb"])),
         },
     }
     return out
@@ -535,7 +560,11 @@ def run_ours(args, rank, world, local_rank):
                     "note": "af_vmult_rhs_fused_tangent / _backward on the bench workload (one launch each)"}
         solvers = {} if (args.no_solvers or not extras) else run_solvers(dev)
         threads = os.cpu_count() or 1
-        cpu_v, cpu_m = cpu_baseline_oracle(64, 3, threads) if extras else (None, None)
+        cpu_v = None
+        if extras:
+            cm, csrc = cpu_sample()
+            cpu_v = 4 * cm.n_cells * (DEGREE + 1) ** 2 / time_cpu_port(cm, csrc, 2, 20, threads) / 1e9
+        parity = strip_parity(dev, stream)
         line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64",
@@ -546,8 +575,10 @@ def run_ours(args, rank, world, local_rank):
                 "roofline": roofline, "gpu_launches": launches,
                 "clocks": clk.summary(),
                 "cpu_baseline": ({"value": cpu_v, "unit": "GDoF/s", "cores": threads, "kind": "port",
-                                  "sample": f"{NX}x64 strip of the workload mesh, best of 3 (1/4 of the work)"}
-                                 if extras else None),
+                                  "sample": cpu_sample_label(), "note": CPU_NOTE} if extras else None),
+                "parity_rel_l2": parity,
+                "parity_check": f"GPU fused apply vs the oracle on the {NX}x{CPU_ROWS} CPU-sample strip (same mesh "
+                                "and inputs on both sides), largest relative L2 error over the three outputs",
                 "degree_sweep": sweep, "autodiff": autodiff, **solvers}
         print(json.dumps(line), flush=True)
     return line

@@ -43,7 +43,7 @@
  * p4est is required by CMakeLists.txt:29-51 and is absent; no golden vectors exist in
  * the reference).  The restatement is instead pinned by the exact known-answer tests in
  * tests/test_oracle_kat.py (rational polynomial integration, divergence theorem,
- * conservation, symmetry) and the fixtures in tests/golden/.
+ * conservation, symmetry); no golden vectors of the reference exist to pin it further.
  */
 #include <algorithm>
 #include <cmath>

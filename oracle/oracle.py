@@ -194,3 +194,26 @@ def imex_steps(op: OracleOperator, rho, u, p, nsteps, eps=1e-8, max_iterations=3
                              int(bool(exact_inverse)))
     assert r == 0
     return rho, u, p, (fp[0], fp[1])
+
+
+def cpu_port_rhs_fused_stage1(mesh, P, Ma, Fr, dt, src):
+    """The tuned CPU port (af_cpu_port.cpp) of the fused stage-1 rhs triple: src = [rho0, u0,
+    p0, rho_tmp_2, u_fixed]; returns (rho, u, p).  Gravity e_z only (the hill meshes)."""
+    L = lib()
+    if not getattr(L, "_port_bound", False):
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.cpu_rhs_fused_stage1.restype = ctypes.c_int
+        L.cpu_rhs_fused_stage1.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.POINTER(dp),
+                                           dp, dp, dp]
+        L._port_bound = True
+    assert mesh.gravity == 0, "the CPU port implements the hill's vertical gravity only"
+    src = [_c(s) for s in src]
+    ns = mesh.n_cells * (P + 1) ** 2
+    out = [np.empty(ns), np.empty(2 * ns), np.empty(ns)]
+    arr = (ctypes.POINTER(ctypes.c_double) * 5)(*[_p(s) for s in src])
+    vtx = _c(mesh.vertices)
+    r = L.cpu_rhs_fused_stage1(P, mesh.nx, mesh.nz, int(mesh.periodic_x), _p(vtx), Ma, Fr, dt, arr,
+                               _p(out[0]), _p(out[1]), _p(out[2]))
+    assert r == 0, f"degree {P} not supported by the CPU port"
+    return out
