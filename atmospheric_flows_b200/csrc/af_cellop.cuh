@@ -67,6 +67,33 @@ struct NfgOf<Phys, std::void_t<decltype(Phys::nfg_of(0))>> {
   static constexpr int get(int g) { return Phys::nfg_of(g); }
 };
 
+// Policies may map their integrand to the reference cell themselves (Phys::MAPPED): their
+// point_mapped<G>(prm, v, pg, A, dw, fv, fx, fe) adds, per output o, fv[o] = value * |J| w and
+// (fx[o], fe[o]) = (A0 g0 - A1 g1, A3 g1 - A2 g0) for the output's flux g, with
+// A = (J11, J01, J10, J00) w = adj(J) w.  A policy that knows the structure of its fluxes can
+// share products of the Jacobian between outputs (contravariant velocities); the others return
+// physical values and fluxes and the kernel maps them.
+template <class Phys, class = void>
+struct MappedOf {
+  static constexpr bool value = false;
+};
+template <class Phys>
+struct MappedOf<Phys, std::void_t<decltype(Phys::MAPPED)>> {
+  static constexpr bool value = Phys::MAPPED;
+};
+
+// Whether a policy's point functions read the physical position: Phys::NEED_X, and for
+// parameters with a `radial` gravity flag only when that flag is set (the vertical gravity of
+// the hill needs no position).
+template <class Prm, class = void>
+struct PositionUse {
+  __device__ static bool get(const Prm&) { return true; }
+};
+template <class Prm>
+struct PositionUse<Prm, std::void_t<decltype(Prm::radial)>> {
+  __device__ static bool get(const Prm& p) { return p.radial != 0; }
+};
+
 // Policies may declare a cell-local epilogue (Phys::EPI) that replaces the plain store.  Both
 // apply a cell-wise inverse mass matrix by the change of basis to the Gauss points (CobT):
 //   M_K^{-1} y = Vi (W_K (Vi^T y)),  W_K = prm.inv[cell][q] = 1 / (rho(g_q) JxW(g_q)),
@@ -92,6 +119,15 @@ __device__ __forceinline__ void put_index(float& s, int v) { s = __int_as_float(
 __device__ __forceinline__ void put_index(double& s, int v) { s = __longlong_as_double((long long)v); }
 __device__ __forceinline__ int get_index(float s) { return __float_as_int(s); }
 __device__ __forceinline__ int get_index(double s) { return (int)__double_as_longlong(s); }
+
+// Face neighbours of cell c (faces 0: xi=0, 1: xi=1, 2: eta=0, 3: eta=1); -1 on a wall.
+__device__ __forceinline__ void cell_neighbours(const MeshDev& mesh, int c, int nb[4]) {
+  const int i = c % mesh.nx, j = c / mesh.nx;
+  nb[0] = i > 0 ? c - 1 : (mesh.periodic_x ? c + mesh.nx - 1 : -1);
+  nb[1] = i < mesh.nx - 1 ? c + 1 : (mesh.periodic_x ? c - mesh.nx + 1 : -1);
+  nb[2] = j > 0 ? c - mesh.nx : -1;
+  nb[3] = j < mesh.nz - 1 ? c + mesh.nx : -1;
+}
 
 template <int N, class F, int... I>
 __device__ __forceinline__ void sfor_impl(F& f, std::integer_sequence<int, I...>) {
@@ -296,16 +332,32 @@ struct Layout {
   static constexpr int GS = 25;
   static constexpr int R_GEO = CB * GS;
   static constexpr int R_S = NQ * P1 + NQ;
-  // region E (epilogue policies): the CTA's Gauss-point inverse weights, 16-byte aligned
+  // bulk staging of several groups: the own-cell chunks of group G+1 are copied into a second
+  // input buffer while group G is computed (group 0's at kernel entry); buffers alternate.
+  // Only where the second buffer leaves the number of resident CTAs per SM unchanged (228 KB
+  // of shared memory per SM, 1 KB reserved per CTA).
+  static constexpr int RBA = (RB + ALIGN - 1) / ALIGN * ALIGN;
+  static constexpr int R_IN_A = (R_IN + ALIGN - 1) / ALIGN * ALIGN;
   static constexpr int EPI = EpiOf<Phys>::value;
-  static constexpr int OE = (RA + RB + R_FLUX + R_GEO + R_S + ALIGN - 1) / ALIGN * ALIGN;
-  // EPI 2 and 3 also prefetch the residual (or z), the previous direction and the iterate of
-  // their cells
   static constexpr int NE = EPI >= 2 ? 4 : 1;
-  static constexpr int TOTAL = EPI ? OE + NE * CB * ND : RA + RB + R_FLUX + R_GEO + R_S;
+  static constexpr int total_with(int rin2) {
+    const int base = RA + RBA + rin2 + R_FLUX + R_GEO + R_S;
+    return EPI ? (base + ALIGN - 1) / ALIGN * ALIGN + NE * CB * ND : base;
+  }
+  static constexpr int ctas_per_sm(int total) { return (228 * 1024) / ((int)sizeof(R) * total + 1024); }
+  static constexpr bool PREFETCH = BULK && Phys::NG > 1 && (int)sizeof(R) * total_with(R_IN_A) <= 227 * 1024 &&
+                                   ctas_per_sm(total_with(R_IN_A)) >= ctas_per_sm(total_with(0));
+  static constexpr int R_IN2 = PREFETCH ? R_IN_A : 0;
+  static constexpr int RB2 = RBA + R_IN2;
+  // region E (epilogue policies): the CTA's Gauss-point inverse weights, 16-byte aligned
+  static constexpr int OE = (RA + RB2 + R_FLUX + R_GEO + R_S + ALIGN - 1) / ALIGN * ALIGN;
+  // (EPI 2 and 3 also prefetch the residual (or z), the previous direction and the iterate of
+  // their cells: NE chunks)
+  static constexpr int TOTAL = EPI ? OE + NE * CB * ND : RA + RB2 + R_FLUX + R_GEO + R_S;
   // the epilogue's scratch (input rows and half-transformed values) lives in region A
   static_assert(EPI == 0 || RA >= (NOUT + 1) * CB * ND, "region A too small for the epilogue");
   static constexpr size_t BYTES = sizeof(R) * TOTAL;
+  static_assert(BYTES <= 227 * 1024, "shared memory of one CTA above the sm_100 limit");
 };
 
 // even/odd contraction of a P1-vector r along one direction to NQ values
@@ -389,16 +441,19 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   R* smem = reinterpret_cast<R*>(smem_raw);
   R* s_eo = smem;             // region A
   R* s_acc = smem;            //   (after the z pass)
-  R* s_in = smem + L::RA;     // region B
-  R* s_nb = s_in + L::R_IN;
-  R* s_out = s_in;            //   (after the last group)
-  R* s_flux = smem + L::RA + L::RB;
+  R* s_in0 = smem + L::RA;    // region B
+  R* s_nb = s_in0 + L::R_IN;
+  R* s_out = s_in0;           //   (after the last group)
+  R* s_in2 = smem + L::RA + (L::RB2 - L::R_IN2);  // second input buffer (Layout::PREFETCH)
+  R* s_flux = smem + L::RA + L::RB2;
   R* s_geo = s_flux + L::R_FLUX;
   R* s_S = s_geo + L::R_GEO;
   R* s_w = s_S + NQ * P1;
 
-  __shared__ alignas(8) unsigned long long s_bar;  // bulk-copy completion (Layout::BULK)
-  const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_bar);
+  // bulk-copy completion (Layout::BULK), one barrier per input buffer
+  __shared__ alignas(8) unsigned long long s_bar[2];
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_bar[0]);
+  const unsigned bar2 = (unsigned)__cvta_generic_to_shared(&s_bar[1]);
   if (mesh.test_wait_polls > 0) {
     // test hook: the bounded wait gives up on a phase that nobody completes (s_bar is armed
     // with an arrival count of 1 and nobody arrives), then the CTA leaves as after a real
@@ -411,13 +466,81 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     }
     if (__syncthreads_or(!ok)) return;
   }
+  const int c0 = mesh.cell0 + blockIdx.x * CB;
+  const int ncb = min(CB, ncell - c0);  // valid cells in this block
+  // own cells of a group: the contiguous chunk of each array, by one bulk copy per array (TMA)
+  // when the layout allows (uniform per CTA), otherwise by coalesced per-element copies
+  const bool bulk = L::BULK && ((size_t)ncb * ND * sizeof(R)) % 16 == 0;
+  // issued by thread 0: group G's chunks into input buffer G % 2 (buffer 0 without prefetch)
+  auto issue_group = [&](auto gc) {
+    constexpr int G = decltype(gc)::value;
+    using Gi = GroupInfo<Phys, G>;
+    using Gr = typename Phys::template Grp<G>;
+    R* buf = (L::PREFETCH && (G & 1)) ? s_in2 : s_in0;
+    const unsigned gbar = (L::PREFETCH && (G & 1)) ? bar2 : bar;
+    unsigned bytes = 0;
+    sfor<Gi::NARR>([&](auto ac) { bytes += (unsigned)(ncb * Gr::ncomp(decltype(ac)::value) * ND * sizeof(R)); });
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(gbar), "r"(bytes) : "memory");
+    sfor<Gi::NARR>([&](auto ac) {
+      constexpr int A = decltype(ac)::value;
+      constexpr int NC = Gr::ncomp(A);
+      constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+      const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + fb * CB * ND);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+          "l"(src), "r"((unsigned)(ncb * NC * ND * sizeof(R))), "r"(gbar)
+          : "memory");
+    });
+  };
+  // neighbours' face nodes of a face group (L2-resident), ordered along the face parameter, by
+  // per-element asynchronous copies; one element per thread for each (face, field):
+  // CB * P1 <= NT for every degree
+  auto gather_neighbours = [&](auto gc) {
+    constexpr int G = decltype(gc)::value;
+    using Gi = GroupInfo<Phys, G>;
+    using Gr = typename Phys::template Grp<G>;
+    constexpr int NF = Gi::NF;
+    static_assert(CB * P1 <= NT, "neighbour staging assumes one element per thread");
+    const int tid = threadIdx.x;
+    const int cc = tid / P1, i = tid % P1;
+    if (tid < CB * P1) {
+      int nbs[4];
+      cell_neighbours(mesh, c0 + (cc < ncb ? cc : ncb - 1), nbs);
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const int nb = nbs[f];
+        const bool ok = nb >= 0 && cc < ncb;
+        const int kk = f == 0 ? i * P1 + P : (f == 1 ? i * P1 : (f == 2 ? P * P1 + i : i));
+        sfor<Gi::NARR>([&](auto ac) {
+          constexpr int A = decltype(ac)::value;
+          constexpr int NC = Gr::ncomp(A);
+          constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+          const R* base = ptr.in[Gi::arr_base() + A];
+#pragma unroll
+          for (int d = 0; d < NC; ++d) {
+            R* dst = &s_nb[((f * NF + fb + d) * CB + cc) * L::P1P + i];
+            if (ok) cp_async_el(dst, base + (size_t)nb * NC * ND + d * ND + kk);
+            else *dst = 0.0;
+          }
+        });
+      }
+    }
+  };
+  // per barrier: the phase a wait expects, and whether copies were issued and not yet waited for
+  unsigned ph[2] = {0u, 0u};
+  bool pending[2] = {false, false};
   if constexpr (L::BULK) {
     if (threadIdx.x == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+      if (L::PREFETCH) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar2) : "memory");
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      if (bulk) issue_group(std::integral_constant<int, 0>{});  // group 0 overlaps the geometry
     }
+    pending[0] = bulk;
   }
-  unsigned bar_phase = 0;
+
   bool abort = false;
   // epilogue policies: the CTA's inverse weights, copied from kernel start on
   __shared__ alignas(8) unsigned long long s_bar_e;
@@ -461,8 +584,6 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   const int tid = threadIdx.x;
   const int m = tid / CB;   // member: row / column / face point
   const int cl = tid % CB;  // cell within the block
-  const int c0 = mesh.cell0 + blockIdx.x * CB;
-  const int ncb = min(CB, ncell - c0);  // valid cells in this block
   const int c = c0 + (cl < ncb ? cl : ncb - 1);
 
   // ---- per-cell geometry and neighbours, spread over the cell's threads (task f < 4: face f,
@@ -479,11 +600,9 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       g[2] = v3.x - v2.x - v1.x + v0.x; g[3] = v3.y - v2.y - v1.y + v0.y;  // B (bilinear term)
       g[4] = v2.x - v0.x; g[5] = v2.y - v0.y;                        // C = x_eta at xi = 0
       g[6] = v0.x; g[7] = v0.y;
-      const int nb0 = i > 0 ? c - 1 : (mesh.periodic_x ? c + mesh.nx - 1 : -1);
-      const int nb1 = i < mesh.nx - 1 ? c + 1 : (mesh.periodic_x ? c - mesh.nx + 1 : -1);
-      const int nb2 = j > 0 ? c - mesh.nx : -1;
-      const int nb3 = j < mesh.nz - 1 ? c + mesh.nx : -1;
-      put_index(g[20], nb0); put_index(g[21], nb1); put_index(g[22], nb2); put_index(g[23], nb3);
+      int nb[4];
+      cell_neighbours(mesh, c, nb);
+      put_index(g[20], nb[0]); put_index(g[21], nb[1]); put_index(g[22], nb[2]); put_index(g[23], nb[3]);
     } else {
       // faces: 0 (xi=0, edge v0->v2), 1 (xi=1, v1->v3), 2 (eta=0, v0->v1), 3 (eta=1, v2->v3);
       // a face's normal is formed from its two vertices the same way by both cells
@@ -493,8 +612,9 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       const double2 a = mesh.vtx[ja * W + ia], b = mesh.vtx[jb * W + ib];
       const double tx = b.x - a.x, tz = b.y - a.y, len = sqrt(tx * tx + tz * tz);
       const double sg = (f == 0 || f == 3) ? 1.0 : -1.0;  // outward: (-tz, tx) on faces 0 and 3
-      g[8 + 3 * f] = sg * (-tz / len);
-      g[9 + 3 * f] = sg * (tx / len);
+      const double il = sg / len;
+      g[8 + 3 * f] = -tz * il;
+      g[9 + 3 * f] = tx * il;
       g[10 + 3 * f] = len;
     }
   }
@@ -511,28 +631,22 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     constexpr int EOFF = PhysInfo<Phys>::eo_offset(G);
     constexpr bool GFACE = Phys::FACES && Gr::FACE;
 
+    constexpr int B = (L::PREFETCH && (G & 1)) ? 1 : 0;  // this group's input buffer and barrier
+    R* const s_in = B ? s_in2 : s_in0;
+
     if (abort) return;
-    __syncthreads();  // region B free (previous group done) / geometry visible
-    // own cells: the contiguous chunk of each array, by one bulk copy per array (TMA) when
-    // the layout allows, otherwise by coalesced per-element asynchronous copies
-    const bool bulk = L::BULK && ((size_t)ncb * ND * sizeof(R)) % 16 == 0;
+    __syncthreads();  // the buffer of group G-1 and the neighbour area free / geometry visible
     if (bulk) {
-      if (tid == 0) {
-        unsigned bytes = 0;
-        sfor<Gi::NARR>([&](auto ac) { bytes += (unsigned)(ncb * Gr::ncomp(decltype(ac)::value) * ND * sizeof(R)); });
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-        sfor<Gi::NARR>([&](auto ac) {
-          constexpr int A = decltype(ac)::value;
-          constexpr int NC = Gr::ncomp(A);
-          constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
-          const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
-          const unsigned dst = (unsigned)__cvta_generic_to_shared(s_in + fb * CB * ND);
-          asm volatile(
-              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-              "l"(src), "r"((unsigned)(ncb * NC * ND * sizeof(R))), "r"(bar)
-              : "memory");
-        });
+      // group 0 was issued at kernel entry; with prefetch, group G+1 goes into the other buffer
+      // now (group G-1 has finished reading it), otherwise group G is issued here
+      if constexpr (L::PREFETCH) {
+        if constexpr (G + 1 < Phys::NG) {
+          if (tid == 0) issue_group(std::integral_constant<int, G + 1>{});
+          pending[B ^ 1] = true;
+        }
+      } else if constexpr (G > 0) {
+        if (tid == 0) issue_group(std::integral_constant<int, G>{});
+        pending[0] = true;
       }
     } else {
       sfor<Gi::NARR>([&](auto ac) {
@@ -565,36 +679,14 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         return off;
       }
     };
-    // neighbours' face nodes (L2-resident), ordered along the face parameter;
-    // one element per thread for each (face, field): CB * P1 <= NT for every degree
-    if constexpr (GFACE) {
-      static_assert(CB * P1 <= NT, "neighbour staging assumes one element per thread");
-      const int cc = tid / P1, i = tid % P1;
-      if (tid < CB * P1) {
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          const int nb = get_index(s_geo[cc * L::GS + 20 + f]);
-          const bool ok = nb >= 0 && cc < ncb;
-          const int kk = f == 0 ? i * P1 + P : (f == 1 ? i * P1 : (f == 2 ? P * P1 + i : i));
-          sfor<Gi::NARR>([&](auto ac) {
-            constexpr int A = decltype(ac)::value;
-            constexpr int NC = Gr::ncomp(A);
-            constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
-            const R* base = ptr.in[Gi::arr_base() + A];
-#pragma unroll
-            for (int d = 0; d < NC; ++d) {
-              R* dst = &s_nb[((f * NF + fb + d) * CB + cc) * L::P1P + i];
-              if (ok) cp_async_el(dst, base + (size_t)nb * NC * ND + d * ND + kk);
-              else *dst = 0.0;
-            }
-          });
-        }
-      }
-    }
+    if constexpr (GFACE) gather_neighbours(gc);
     cp_async_wait_all();
     if (bulk) {
-      const bool ok = mbar_wait(bar, bar_phase);
-      bar_phase ^= 1u;
+      const bool ok = mbar_wait(B ? bar2 : bar, ph[B]);
+      if (ok) {
+        ph[B] ^= 1u;
+        pending[B] = false;
+      }
       if (!ok) report_status(mesh.status, kStatusStageTimeout);
       if (__syncthreads_or(!ok)) {  // every thread leaves together, nothing waits on a barrier
         abort = true;
@@ -679,7 +771,8 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   });
   if (abort) {  // a staging wait gave up: wait (bounded) for this CTA's copies before leaving
     if (tid == 0) {
-      if (L::BULK) mbar_wait(bar, bar_phase ^ 1u);
+      if (pending[0]) mbar_wait(bar, ph[0]);
+      if (pending[1]) mbar_wait(bar2, ph[1]);
       if (epi_bulk) mbar_wait(bar_e, 0);
     }
     return;
@@ -709,6 +802,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     const R wx = s_w[qx];
     const R J01 = fmaR(g[2], xi, g[4]);  // x_eta (x component)
     const R J11 = fmaR(g[3], xi, g[5]);  // x_eta (z component)
+    const bool need_x = Phys::NEED_X && PositionUse<typename Phys::Params>::get(prm);
     constexpr int NFG_ALL = PhysInfo<Phys>::NFG_TOTAL;
     // the mapped integrands of one point: fv (tested with phi), fx, fe (with d/dxi, d/deta phi)
     auto integrand = [&](const R* v, const R* deta, const int qz, R* fvo, R* fxo, R* feo) {
@@ -718,12 +812,22 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       const R w = wx * tb.w[qz];
       const R dw = (J00 * J11 - J01 * J10) * w;
       PointGeo pg;
-      if (Phys::NEED_X) {
+      if (need_x) {
         pg.X[0] = g[6] + g[0] * xi + g[4] * eta + g[2] * xi * eta;
         pg.X[1] = g[7] + g[1] * xi + g[5] * eta + g[3] * xi * eta;
       }
       if constexpr (NFG_ALL > 0) {
         pg.J[0] = J00; pg.J[1] = J01; pg.J[2] = J10; pg.J[3] = J11;
+      }
+      if constexpr (MappedOf<Phys>::value) {  // the policy maps its own integrand
+        const R A[4] = {J11 * w, J01 * w, J10 * w, J00 * w};
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) fvo[o] = fxo[o] = feo[o] = R(0);
+        sfor<Phys::NG>([&](auto gc) {
+          constexpr int G = decltype(gc)::value;
+          Phys::template point_mapped<G>(prm, v + PhysInfo<Phys>::eo_offset(G), pg, A, dw, fvo, fxo, feo);
+        });
+        return;
       }
       R val[NOUT], gr[NOUT][2];
 #pragma unroll

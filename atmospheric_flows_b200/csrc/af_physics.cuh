@@ -113,11 +113,21 @@ struct RhsPhys {
     static constexpr bool face_only(int a) { return EXPL && a == 3; }
   };
 
+  // The hill's vertical gravity (e_z, |g| constant) and the reference's radial one are two
+  // compiled paths (a uniform branch): on the vertical path the terms with e_x = 0 and the
+  // factor 1 are left out, which gives bit for bit the same values with fewer operations.
   template <int G, class T>
   __device__ __forceinline__ static void point_t(const Params& prm, const T* v, const PointGeo& pg, T* val,
                                                  T (*gr)[2]) {
-    double e0, e1, fac;
-    gravity_dir(prm, pg, e0, e1, fac);
+    if (prm.radial) point_g<G, T, true>(prm, v, pg, val, gr);
+    else point_g<G, T, false>(prm, v, pg, val, gr);
+  }
+
+  template <int G, class T, bool RADIAL>
+  __device__ __forceinline__ static void point_g(const Params& prm, const T* v, const PointGeo& pg, T* val,
+                                                 T (*gr)[2]) {
+    double e0 = 0.0, e1 = 1.0, fac = 1.0;
+    if constexpr (RADIAL) gravity_dir(prm, pg, e0, e1, fac);
     if constexpr (G < STAGE) {
       const T rho = v[0], ux = v[1], uz = v[2];
       const double ca = prm.ca[G] * prm.dt, cg = prm.cg[G] * prm.dt;
@@ -131,9 +141,13 @@ struct RhsPhys {
         const double ct = prm.ct[G] * prm.dt;
         if constexpr (VEL) {  // :1686-1691
           if (G == 0) { val[O_U] += rho * ux; val[O_U + 1] += rho * uz; }
-          const T gfac = cg * prm.invFr2 * rho * fac;
-          val[O_U] -= gfac * e0;
-          val[O_U + 1] -= gfac * e1;
+          if constexpr (RADIAL) {
+            const T gfac = cg * prm.invFr2 * rho * fac;
+            val[O_U] -= gfac * e0;
+            val[O_U + 1] -= gfac * e1;
+          } else {
+            val[O_U + 1] -= cg * prm.invFr2 * rho;
+          }
           const T cr = ca * rho, pt = ct * prm.invMa2 * p;
           gr[O_U][0] += cr * ux * ux + pt;
           gr[O_U][1] += cr * ux * uz;
@@ -143,7 +157,8 @@ struct RhsPhys {
         if constexpr (PRES) {  // :806-813: rho E = p/(g-1) + Ma^2 rho |u|^2 / 2
           const T uu = ux * ux + uz * uz;
           if (G == 0) val[O_P] += p * prm.g1 + 0.5 * prm.Ma2 * rho * uu;
-          val[O_P] -= cg * prm.Ma2Fr2 * rho * (ux * e0 + uz * e1) * fac;
+          if constexpr (RADIAL) val[O_P] -= cg * prm.Ma2Fr2 * rho * (ux * e0 + uz * e1) * fac;
+          else val[O_P] -= cg * prm.Ma2Fr2 * rho * uz;
           const T s = 0.5 * ca * prm.Ma2 * uu * rho + ct * prm.gg * p;
           gr[O_P][0] += s * ux;
           gr[O_P][1] += s * uz;
@@ -153,14 +168,107 @@ struct RhsPhys {
       const T rc = v[0];
       const double cgI = prm.cgI * prm.dt;
       if constexpr (VEL && STAGE < 3) {
-        const T gfac = cgI * prm.invFr2 * rc * fac;
-        val[O_U] -= gfac * e0;
-        val[O_U + 1] -= gfac * e1;
+        if constexpr (RADIAL) {
+          const T gfac = cgI * prm.invFr2 * rc * fac;
+          val[O_U] -= gfac * e0;
+          val[O_U + 1] -= gfac * e1;
+        } else {
+          val[O_U + 1] -= cgI * prm.invFr2 * rc;
+        }
       }
       if constexpr (PRES) {
         const T fx = v[1], fz = v[2];
         val[O_P] -= 0.5 * rc * prm.Ma2 * (fx * fx + fz * fz);
-        if (STAGE < 3) val[O_P] -= cgI * prm.Ma2Fr2 * rc * (fx * e0 + fz * e1) * fac;
+        if (STAGE < 3) {
+          if constexpr (RADIAL) val[O_P] -= cgI * prm.Ma2Fr2 * rc * (fx * e0 + fz * e1) * fac;
+          else val[O_P] -= cgI * prm.Ma2Fr2 * rc * fz;
+        }
+      }
+    }
+  }
+
+  // The integrand of point_t mapped to the reference cell (see MappedOf in af_cellop.cuh):
+  // every flux of the explicit group is a multiple of the velocity u_j plus pressure times the
+  // identity, so its mapped form shares the contravariant velocity (U1, U2) = adj(J) w u_j:
+  //   rho:       ca rho (U1, U2)
+  //   rho u_x:   ca rho u_x (U1, U2) + pt (A0, -A2)      rho u_z: ca rho u_z (U1, U2) + pt (-A1, A3)
+  //   pressure:  s (U1, U2)
+  // (ca = a_j dt, pt = a~_j dt p_j / Ma^2, s as in point_t); values are multiplied by |J| w.
+  static constexpr bool MAPPED = true;
+  template <int G>
+  __device__ __forceinline__ static void point_mapped(const Params& prm, const double* v, const PointGeo& pg,
+                                                      const double (&A)[4], double dw, double* fv, double* fx,
+                                                      double* fe) {
+    if (prm.radial) point_mapped_g<G, true>(prm, v, pg, A, dw, fv, fx, fe);
+    else point_mapped_g<G, false>(prm, v, pg, A, dw, fv, fx, fe);
+  }
+  template <int G, bool RADIAL>
+  __device__ __forceinline__ static void point_mapped_g(const Params& prm, const double* v, const PointGeo& pg,
+                                                        const double (&A)[4], double dw, double* fv, double* fx,
+                                                        double* fe) {
+    double e0 = 0.0, e1 = 1.0, fac = 1.0;
+    if constexpr (RADIAL) gravity_dir(prm, pg, e0, e1, fac);
+    if constexpr (G < STAGE) {
+      const double rho = v[0], ux = v[1], uz = v[2];
+      const double ca = prm.ca[G] * prm.dt, cg = prm.cg[G] * prm.dt;
+      const double U1 = A[0] * ux - A[1] * uz, U2 = A[3] * uz - A[2] * ux;
+      const double cr = ca * rho;
+      if constexpr (RHO) {
+        if (G == 0) fv[O_RHO] += rho * dw;
+        fx[O_RHO] += cr * U1;
+        fe[O_RHO] += cr * U2;
+      }
+      if constexpr (VEL || PRES) {
+        const double p = v[3];
+        const double ct = prm.ct[G] * prm.dt;
+        if constexpr (VEL) {
+          const double rdw = rho * dw;
+          if (G == 0) { fv[O_U] += rdw * ux; fv[O_U + 1] += rdw * uz; }
+          if constexpr (RADIAL) {
+            const double gfac = cg * prm.invFr2 * rdw * fac;
+            fv[O_U] -= gfac * e0;
+            fv[O_U + 1] -= gfac * e1;
+          } else {
+            fv[O_U + 1] -= cg * prm.invFr2 * rdw;
+          }
+          const double pt = ct * prm.invMa2 * p;
+          const double cx = cr * ux, cz = cr * uz;
+          fx[O_U] += cx * U1 + pt * A[0];
+          fe[O_U] += cx * U2 - pt * A[2];
+          fx[O_U + 1] += cz * U1 - pt * A[1];
+          fe[O_U + 1] += cz * U2 + pt * A[3];
+        }
+        if constexpr (PRES) {
+          const double uu = ux * ux + uz * uz;
+          double val = G == 0 ? p * prm.g1 + 0.5 * prm.Ma2 * rho * uu : 0.0;
+          if constexpr (RADIAL) val -= cg * prm.Ma2Fr2 * rho * (ux * e0 + uz * e1) * fac;
+          else val -= cg * prm.Ma2Fr2 * rho * uz;
+          fv[O_P] += val * dw;
+          const double s = 0.5 * ca * prm.Ma2 * uu * rho + ct * prm.gg * p;
+          fx[O_P] += s * U1;
+          fe[O_P] += s * U2;
+        }
+      }
+    } else {
+      const double rc = v[0];
+      const double cgI = prm.cgI * prm.dt;
+      if constexpr (VEL && STAGE < 3) {
+        if constexpr (RADIAL) {
+          const double gfac = cgI * prm.invFr2 * rc * fac * dw;
+          fv[O_U] -= gfac * e0;
+          fv[O_U + 1] -= gfac * e1;
+        } else {
+          fv[O_U + 1] -= cgI * prm.invFr2 * rc * dw;
+        }
+      }
+      if constexpr (PRES) {
+        const double fxv = v[1], fzv = v[2];
+        double val = 0.5 * rc * prm.Ma2 * (fxv * fxv + fzv * fzv);
+        if (STAGE < 3) {
+          if constexpr (RADIAL) val += cgI * prm.Ma2Fr2 * rc * (fxv * e0 + fzv * e1) * fac;
+          else val += cgI * prm.Ma2Fr2 * rc * fzv;
+        }
+        fv[O_P] -= val * dw;
       }
     }
   }

@@ -121,6 +121,7 @@ class EULEROperator:
         torch.cuda.current_device()  # make the context current before the library uses it
         check(lib().af_create(ctypes.byref(desc), degree, self.n_q, Ma, Fr, dt, ctypes.byref(h)))
         self._h = h
+        self._destroy = lib().af_destroy  # kept: module globals may be gone when __del__ runs at exit
         self.Ma, self.Fr, self.dt = Ma, Fr, dt
         self.HYPERBOLIC_stage, self.NS_stage = 1, 1
         if stream is not None:
@@ -129,7 +130,7 @@ class EULEROperator:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().af_destroy(h)
+            self._destroy(h)
             self._h = None
 
     # --- plumbing ---

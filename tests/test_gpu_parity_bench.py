@@ -7,11 +7,16 @@
 * The implicit operators on the same mesh at degree 4: the mass-type operators, B
   (vmult_pressure), C (vmult_enthalpy), the inverse diagonals, and the NS-stage-2 Schur apply
   D p - C A^{-1} B p with the nested CG to 1e-12 on both sides (1e-10).
-* 100 IMEX steps on the 40x16 hill mesh at degree 4 (the plain FP64 hill case, periodic
-  lateral boundaries, dt = 2 s), the library's default solver configuration (the reference's
-  left-Jacobi GMRES criterion at eps = 1e-12, exact cell-wise inverses of the mass-type
-  systems) on both sides.  Stated tolerance for the states after 100 steps: 1e-9 relative L2
-  per field.
+* IMEX steps on the 40x16 hill mesh at degree 4 (the plain FP64 hill case, periodic lateral
+  boundaries, dt = 2 s, exact cell-wise inverses of the mass-type systems on both sides):
+  - 100 steps with the library's default pressure solve, the reference's left-Jacobi GMRES
+    stopping on |D^-1 r| <= eps |b| at eps = 1e-12.  That criterion leaves each solve far
+    less accurate than eps: D^-1 scales the residual by about 1e-4 on this mesh, and the
+    oracle's own states after 10 steps lie 5e-6 (velocity) from those of accurate solves.
+    Two implementations that round differently stop at different iterates inside that
+    band, so the stated tolerance after 100 steps is 1e-6 relative L2 per field.
+  - 10 steps with accurate solves (GMRES stopping on the true residual |b - S p| <= 1e-12
+    |b| on both sides): stated tolerance 1e-9.
 """
 import numpy as np
 import pytest
@@ -126,22 +131,31 @@ def test_implicit_parity_on_the_bench_mesh():
         assert rel(_h(dst), o.vmult(st3.p)) < 1e-10, ("Schur", hs)
 
 
-def test_imex_100_steps_on_the_40x16_hill():
+def _imex_40x16(nsteps, eps, accurate):
     from atmospheric_flows_b200.imex import IMEXStepper
     from oracle.oracle import OracleOperator, imex_steps
-    P, nsteps, dt = 4, 100, 2.0
+    P, dt = 4, 2.0
     m = M.hill_mesh(40, 16, periodic_x=True)
     sc = M.Scaling()
     st = M.hill_state(m, P, amplitude=1e-3)
     o = OracleOperator(m, P, sc.Ma, sc.Fr, dt)
-    r_ref, u_ref, p_ref, fp_ref = imex_steps(o, st.rho, st.u, st.p, nsteps, eps=1e-12, exact_inverse=True)
-    g = IMEXStepper(m, P, sc.Ma, sc.Fr, dt, eps=1e-12)
+    ref = imex_steps(o, st.rho, st.u, st.p, nsteps, eps=eps, exact_inverse=True, true_residual=accurate)
+    g = IMEXStepper(m, P, sc.Ma, sc.Fr, dt, eps=eps, schur_preconditioner="jacobi" if accurate else None)
     g.set_state(_d(st.rho), _d(st.u), _d(st.p))
     g.step(nsteps)
-    r, u, p = (t.cpu().numpy() for t in g.get_state())
-    errs = {"rho": rel(r, r_ref), "u": rel(u, u_ref), "p": rel(p, p_ref)}
-    print("imex 40x16 p=4, 100 steps, state errors vs oracle:", errs, "fixed point", g.stats()["fixed_point_iterations"],
-          fp_ref)
-    assert np.abs(u_ref).max() > 10.0  # the flow has moved over the hill (not a trivial state)
-    for k, e in errs.items():
+    got = [t.cpu().numpy() for t in g.get_state()]
+    errs = {k: rel(a, b) for k, a, b in zip(("rho", "u", "p"), got, ref[:3])}
+    print(f"imex 40x16 p=4, {nsteps} steps, eps {eps}, accurate solves {accurate}: state errors vs oracle {errs}, "
+          f"fixed point {g.stats()['fixed_point_iterations']} / {ref[3]}")
+    assert np.abs(ref[1]).max() > 10.0  # the flow has moved over the hill (not a trivial state)
+    return errs
+
+
+def test_imex_100_steps_on_the_40x16_hill():
+    for k, e in _imex_40x16(100, 1e-12, False).items():
+        assert e < 1e-6, (k, e)
+
+
+def test_imex_10_accurate_steps_on_the_40x16_hill():
+    for k, e in _imex_40x16(10, 1e-12, True).items():
         assert e < 1e-9, (k, e)
