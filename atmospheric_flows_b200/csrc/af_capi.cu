@@ -97,6 +97,10 @@ static RhsParams rhs_params(const af_operator* o, int stage) {
   r.g1 = 1.0 / (1.4 - 1.0);
   r.gg = 1.4 / (1.4 - 1.0);
   r.radial = o->mesh.gravity == 1;
+  r.sponge = (o->sp_rate > 0 || o->sp_rate_lat > 0) ? 1 : 0;
+  r.sp_z0 = o->sp_z0; r.sp_z1 = o->sp_z1; r.sp_rate = o->sp_rate;
+  r.sp_x0 = o->sp_x0; r.sp_x1 = o->sp_x1; r.sp_width = o->sp_width; r.sp_rate_lat = o->sp_rate_lat;
+  r.sp_u = o->sp_u;
   if (stage == 1) {
     r.ca[0] = o->a21; r.ct[0] = o->a21t;
     r.cg[0] = o->a21t; r.cgI = o->a22t;
@@ -225,6 +229,19 @@ int af_set_stream(af_operator* o, void* s) {
 int af_synchronize(af_operator* o) {
   if (!o) return fail(AF_BAD_ARG, "null handle");
   return sync_checked(o, o->stream);
+}
+
+int af_set_sponge(af_operator* o, double z_start, double z_top, double rate_top, double x_left, double x_right,
+                  double width_lateral, double rate_lateral, double u_ref) {
+  if (!o) return fail(AF_BAD_ARG, "null handle");
+  if (!(rate_top >= 0) || !(rate_lateral >= 0) || (rate_top > 0 && !(z_top > z_start)) ||
+      (rate_lateral > 0 && (!(width_lateral > 0) || !(x_right > x_left))))
+    return fail(AF_BAD_ARG, "af_set_sponge: need rates >= 0, z_top > z_start and width > 0, x_right > x_left "
+                            "for the layers that are on");
+  o->sp_z0 = z_start; o->sp_z1 = z_top; o->sp_rate = rate_top;
+  o->sp_x0 = x_left; o->sp_x1 = x_right; o->sp_width = width_lateral; o->sp_rate_lat = rate_lateral;
+  o->sp_u = u_ref;
+  return AF_OK;
 }
 
 int af_set_stage_wait_test(af_operator* o, int polls) {
@@ -375,6 +392,8 @@ int af_vmult_rhs_fused_backward(af_operator* o, const double* const* src, int n,
       return fail(AF_BAD_ARG, "af_vmult_rhs_fused_backward: null or unaligned vector");
   AF_CU(cudaSetDevice(o->device));
   AF_PENDING(o);
+  if (o->hs == 1 && (o->sp_rate > 0 || o->sp_rate_lat > 0))
+    return fail(AF_UNSUPPORTED, "af_vmult_rhs_fused_backward: the stage-1 adjoint kernel has no sponge term");
   const double* yb[3] = {ybar_rho, ybar_u, ybar_p};
   if (o->hs == 1) {
     AF_CU(o->ops->rhs_adjoint1(o->mesh, src, yb, xbar, rhs_params(o, 1), o->ncell, o->stream));
@@ -396,6 +415,8 @@ int af_vmult_rhs_fused_tangent(af_operator* o, const double* const* src, int n, 
       return fail(AF_BAD_ARG, "af_vmult_rhs_fused_tangent: null or unaligned vector");
   AF_CU(cudaSetDevice(o->device));
   AF_PENDING(o);
+  if (o->hs == 1 && (o->sp_rate > 0 || o->sp_rate_lat > 0))
+    return fail(AF_UNSUPPORTED, "af_vmult_rhs_fused_tangent: the stage-1 tangent kernel has no sponge term");
   double* dy[3] = {d_rho, d_u, d_p};
   if (o->hs == 1)
     AF_CU(o->ops->rhs_tangent1(o->mesh, src, dsrc, dy, rhs_params(o, 1), o->ncell, o->stream));

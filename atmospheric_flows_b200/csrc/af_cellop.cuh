@@ -83,15 +83,15 @@ struct MappedOf<Phys, std::void_t<decltype(Phys::MAPPED)>> {
 };
 
 // Whether a policy's point functions read the physical position: Phys::NEED_X, and for
-// parameters with a `radial` gravity flag only when that flag is set (the vertical gravity of
-// the hill needs no position).
+// parameters that say so (needs_position()) only when they do (the vertical gravity of the hill
+// needs no position, radial gravity and the sponge do).
 template <class Prm, class = void>
 struct PositionUse {
   __device__ static bool get(const Prm&) { return true; }
 };
 template <class Prm>
-struct PositionUse<Prm, std::void_t<decltype(Prm::radial)>> {
-  __device__ static bool get(const Prm& p) { return p.radial != 0; }
+struct PositionUse<Prm, std::void_t<decltype(std::declval<const Prm&>().needs_position())>> {
+  __device__ static bool get(const Prm& p) { return p.needs_position(); }
 };
 
 // Policies may declare a cell-local epilogue (Phys::EPI) that replaces the plain store.  Both
@@ -210,14 +210,17 @@ constexpr int kZUnroll = AF_Z_UNROLL;
 // Cells per CTA and the CTAs-per-SM hint of __launch_bounds__, per degree.  Measured on
 // B200 for the fused stage-1 right-hand side at 512x256 cells, degree 4 (CB, MINB):
 // (16,1) 781 us, (16,2) 502 us, (32,1) 529 us, (8,3) 592 us, (8,4) 588 us (z loop not
-// unrolled; fully unrolled: 764 / 521 / 567 / 554 / 550 us).
+// unrolled; fully unrolled: 764 / 521 / 567 / 554 / 550 us).  Degree 5: (8,3) 822 us,
+// (8,2) 842, (12,2) 863, (16,2) 995 (one CTA per SM: 128 KB of shared memory).  Degree 6:
+// (8,2) 1070 us, (4,4) 1153, (6,3) 1406.  Degree 3: (16,3) 244 us, (16,2) 266, (24,2) 273,
+// (32,1) 299.
 template <int P>
 constexpr int cells_per_block() {
-  return P <= 1 ? 64 : (P == 2 ? 32 : (P == 3 ? 32 : (P == 4 ? 16 : (P == 5 ? 16 : 8))));
+  return P <= 1 ? 64 : (P == 2 ? 32 : (P <= 4 ? 16 : 8));
 }
 template <int P>
 constexpr int min_blocks_per_sm() {
-  return P == 3 ? 1 : 2;
+  return P == 3 || P == 5 ? 3 : 2;
 }
 
 template <int MAXARR, int MAXOUT, class R = double>
@@ -251,8 +254,21 @@ struct GroupInfo {
   }();
 };
 
+template <class Phys, int... G>
+constexpr int count_face_groups(std::integer_sequence<int, G...>) {
+  return ((Phys::FACES && Phys::template Grp<G>::FACE ? 1 : 0) + ... + 0);
+}
+template <class Phys, int... G>
+constexpr int last_face_group(std::integer_sequence<int, G...>) {
+  int r = -1;
+  ((r = (Phys::FACES && Phys::template Grp<G>::FACE) ? G : r), ...);
+  return r;
+}
+
 template <class Phys>
 struct PhysInfo {
+  static constexpr int NFACEG = count_face_groups<Phys>(std::make_integer_sequence<int, Phys::NG>{});
+  static constexpr int FACE_G = last_face_group<Phys>(std::make_integer_sequence<int, Phys::NG>{});
   static constexpr int NFMAX = [] {
     int m = 0;
     for (int g = 0; g < Phys::NG; ++g) m = m > Phys::nf_of(g) ? m : Phys::nf_of(g);
@@ -326,7 +342,18 @@ struct Layout {
   static constexpr int R_NB = Phys::FACES ? 4 * NF * CB * P1P : 0;
   static constexpr int R_OUT = NOUT * CB * NDP;
   static constexpr int RB = (R_IN + R_NB) > R_OUT ? (R_IN + R_NB) : R_OUT;
-  static constexpr int R_FLUX = Phys::FACES ? 4 * NOUT * CB * NQ : 0;
+  // z-face folding: with one face group whose staged nodes and neighbour face nodes are still in
+  // place after the z pass (no later group reuses its buffer), the fluxes of the z-faces are
+  // evaluated at the end of the z pass by the thread of quadrature column q and added to its
+  // accumulators of node rows 0 and P (the face term of node (iz, ix) on face 2 is
+  // delta(iz, 0) sum_q S(q, ix) F(q), the x-transpose pass's contraction of row 0); the
+  // x-transpose pass then has no edge rows with extra work
+  // (two input buffers: FACE_G + 2 >= NG; one buffer: FACE_G is the last group)
+  static constexpr int FACE_G = PhysInfo<Phys>::FACE_G;
+  static constexpr bool FOLD_2BUF = Phys::FACES && PhysInfo<Phys>::NFACEG == 1 && FACE_G + 2 >= Phys::NG;
+  static constexpr bool FOLD_1BUF = Phys::FACES && PhysInfo<Phys>::NFACEG == 1 && FACE_G == Phys::NG - 1;
+  static constexpr int flux_size(bool fold) { return Phys::FACES ? (fold ? 2 : 4) * NOUT * CB * NQ : 0; }
+
   // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb; an odd stride, so that a warp
   // reading one slot of consecutive cells meets no bank conflicts (4- and 8-byte elements)
   static constexpr int GS = 25;
@@ -340,14 +367,18 @@ struct Layout {
   static constexpr int R_IN_A = (R_IN + ALIGN - 1) / ALIGN * ALIGN;
   static constexpr int EPI = EpiOf<Phys>::value;
   static constexpr int NE = EPI >= 2 ? 4 : 1;
-  static constexpr int total_with(int rin2) {
-    const int base = RA + RBA + rin2 + R_FLUX + R_GEO + R_S;
+  static constexpr int total_with(int rin2, int rflux) {
+    const int base = RA + RBA + rin2 + rflux + R_GEO + R_S;
     return EPI ? (base + ALIGN - 1) / ALIGN * ALIGN + NE * CB * ND : base;
   }
   static constexpr int ctas_per_sm(int total) { return (228 * 1024) / ((int)sizeof(R) * total + 1024); }
-  static constexpr bool PREFETCH = BULK && Phys::NG > 1 && (int)sizeof(R) * total_with(R_IN_A) <= 227 * 1024 &&
-                                   ctas_per_sm(total_with(R_IN_A)) >= ctas_per_sm(total_with(0));
+  static constexpr int T_PF = total_with(R_IN_A, flux_size(FOLD_2BUF)), T_NOPF = total_with(0, flux_size(FOLD_1BUF));
+  static constexpr bool PREFETCH =
+      BULK && Phys::NG > 1 && (int)sizeof(R) * T_PF <= 227 * 1024 && ctas_per_sm(T_PF) >= ctas_per_sm(T_NOPF);
   static constexpr int R_IN2 = PREFETCH ? R_IN_A : 0;
+  static constexpr bool FOLD_Z = PREFETCH ? FOLD_2BUF : FOLD_1BUF;
+  // the flux accumulators of the x-faces (0, 1) and, unless folded, of the z-faces (2, 3)
+  static constexpr int R_FLUX = flux_size(FOLD_Z);
   static constexpr int RB2 = RBA + R_IN2;
   // region E (epilogue policies): the CTA's Gauss-point inverse weights, 16-byte aligned
   static constexpr int OE = (RA + RB2 + R_FLUX + R_GEO + R_S + ALIGN - 1) / ALIGN * ALIGN;
@@ -528,6 +559,58 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     }
   };
+  // shared-memory offset of field fi (group-local) of cell cl_ in the staged nodes of group G
+  auto field_offset = [&](auto gc, int fi, int cl_) -> int {
+    constexpr int G = decltype(gc)::value;
+    using Gi = GroupInfo<Phys, G>;
+    using Gr = typename Phys::template Grp<G>;
+    if constexpr (!L::BULK) {
+      return (fi * CB + cl_) * L::NDP;
+    } else {
+      int off = 0, fb = 0;
+#pragma unroll
+      for (int a = 0; a < Gi::NARR; ++a) {
+        const int nc = Gr::ncomp(a);
+        if (fi >= fb && fi < fb + nc) off = fb * CB * ND + cl_ * nc * ND + (fi - fb) * ND;
+        fb += nc;
+      }
+      return off;
+    }
+  };
+  // numerical flux of face group G on face f of this thread's cell at face point q, times the
+  // face JxW: the own trace from the group's staged nodes, the neighbour's from its gathered
+  // face nodes; sq = the basis at point q
+  auto face_flux = [&](auto gc, int f, int q, const R* sq, R* fo) {
+    constexpr int G = decltype(gc)::value;
+    constexpr int NF = GroupInfo<Phys, G>::NF;
+    const R* sin = (L::PREFETCH && (G & 1)) ? s_in2 : s_in0;
+    const int cl_ = threadIdx.x % CB;
+    const R* g = s_geo + cl_ * L::GS;
+    const int nb = get_index(g[20 + f]);
+    R vp[NF], vm[NF];
+#pragma unroll
+    for (int fi = 0; fi < NF; ++fi) {
+      const R* cell = sin + field_offset(gc, fi, cl_);
+      const R* nbv = s_nb + ((f * NF + fi) * CB + cl_) * L::P1P;
+      R a = 0.0, b = 0.0;
+#pragma unroll
+      for (int i = 0; i < P1; ++i) {
+        const int kk = f == 0 ? i * P1 : (f == 1 ? i * P1 + P : (f == 2 ? i : P * P1 + i));
+        a = fmaR(sq[i], cell[kk], a);
+        b = fmaR(sq[i], nbv[i], b);
+      }
+      vp[fi] = a;
+      vm[fi] = b;
+    }
+    const R n[2] = {g[8 + 3 * f], g[9 + 3 * f]};
+    const R jxw = g[10 + 3 * f] * s_w[q];
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) fo[o] = 0.0;
+    if (nb >= 0) Phys::template face<G>(prm, vp, vm, n, fo);
+    else Phys::template boundary<G>(prm, vp, n, fo);
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) fo[o] *= jxw;
+  };
   // per barrier: the phase a wait expects, and whether copies were issued and not yet waited for
   unsigned ph[2] = {0u, 0u};
   bool pending[2] = {false, false};
@@ -664,21 +747,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         }
       });
     }
-    // shared-memory offset of field fi (group-local) of cell cl
-    auto foff = [&](int fi, int cl_) -> int {
-      if constexpr (!L::BULK) {
-        return (fi * CB + cl_) * L::NDP;
-      } else {
-        int off = 0, fb = 0;
-#pragma unroll
-        for (int a = 0; a < Gi::NARR; ++a) {
-          const int nc = Gr::ncomp(a);
-          if (fi >= fb && fi < fb + nc) off = fb * CB * ND + cl_ * nc * ND + (fi - fb) * ND;
-          fb += nc;
-        }
-        return off;
-      }
-    };
+    auto foff = [&](int fi, int cl_) -> int { return field_offset(gc, fi, cl_); };
     if constexpr (GFACE) gather_neighbours(gc);
     cp_async_wait_all();
     if (bulk) {
@@ -731,41 +800,19 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         }
       }
     }
-    // ---- faces (same phase: reads region B only): member = face quadrature point
+    // ---- faces (same phase: reads region B only): member = face quadrature point; the
+    //      z-faces of a folding layout come after the z pass
     if constexpr (GFACE) {
       const int q = m;
       R sq[P1];
 #pragma unroll
       for (int i = 0; i < P1; ++i) sq[i] = s_S[q * P1 + i];
-      const R wq = s_w[q];
-      const R* g = s_geo + cl * L::GS;
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        const int nb = get_index(g[20 + f]);
-        R vp[NF], vm[NF];
+      for (int f = 0; f < (L::FOLD_Z ? 2 : 4); ++f) {
+        R fo[NOUT];
+        face_flux(gc, f, q, sq, fo);
 #pragma unroll
-        for (int fi = 0; fi < NF; ++fi) {
-          const R* cell = s_in + foff(fi, cl);
-          const R* nbv = s_nb + ((f * NF + fi) * CB + cl) * L::P1P;
-          R a = 0.0, b = 0.0;
-#pragma unroll
-          for (int i = 0; i < P1; ++i) {
-            const int kk = f == 0 ? i * P1 : (f == 1 ? i * P1 + P : (f == 2 ? i : P * P1 + i));
-            a = fmaR(sq[i], cell[kk], a);
-            b = fmaR(sq[i], nbv[i], b);
-          }
-          vp[fi] = a;
-          vm[fi] = b;
-        }
-        const R n[2] = {g[8 + 3 * f], g[9 + 3 * f]};
-        const R jxw = g[10 + 3 * f] * wq;
-        R flux[NOUT];
-#pragma unroll
-        for (int o = 0; o < NOUT; ++o) flux[o] = 0.0;
-        if (nb >= 0) Phys::template face<G>(prm, vp, vm, n, flux);
-        else Phys::template boundary<G>(prm, vp, n, flux);
-#pragma unroll
-        for (int o = 0; o < NOUT; ++o) s_flux[((f * NOUT + o) * CB + cl) * NQ + q] += flux[o] * jxw;
+        for (int o = 0; o < NOUT; ++o) s_flux[((f * NOUT + o) * CB + cl) * NQ + q] += fo[o];
       }
     }
   });
@@ -941,6 +988,18 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       acc_b[o][P / 2] = bM[o];
     }
   }
+  if constexpr (L::FOLD_Z) {  // z-faces at face point qx = m, into node rows 0 (face 2) and P (3)
+    R sq[P1];
+#pragma unroll
+    for (int i = 0; i < P1; ++i) sq[i] = s_S[m * P1 + i];
+#pragma unroll
+    for (int f = 2; f < 4; ++f) {
+      R fo[NOUT];
+      face_flux(std::integral_constant<int, L::FACE_G>{}, f, m, sq, fo);
+#pragma unroll
+      for (int o = 0; o < NOUT; ++o) acc_a[o][f == 2 ? 0 : P] += fo[o];
+    }
+  }
   __syncthreads();  // region A: x-contracted rows consumed -> accumulators
   {
     const int qx = m;
@@ -1005,7 +1064,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
       out[0] += l;
       out[P] += r;
-      if (iz == 0 || iz == P) {
+      if (!L::FOLD_Z && (iz == 0 || iz == P)) {
         const R* F = s_flux + (((iz == 0 ? 2 : 3) * NOUT + o) * CB + cl) * NQ;
 #pragma unroll
         for (int ix = 0; ix < P1; ++ix) {

@@ -17,6 +17,8 @@ struct af_operator {
   MeshDev mesh{};
   double2* d_vtx = nullptr;
   double Ma = 1, Fr = 1, dt = 1;
+  // Rayleigh damping of the momentum (af_set_sponge; off when both rates are 0)
+  double sp_z0 = 0, sp_z1 = 1, sp_rate = 0, sp_x0 = 0, sp_x1 = 1, sp_width = 1, sp_rate_lat = 0, sp_u = 0;
   int hs = 1, ns = 1;
   // IMEX-ARK tableau, euler_operator.h:233-240
   double gamma, a21, a22, a31, a32, a33, a21t, a22t, a31t, a32t, a33t, b1, b2, b3;

@@ -31,7 +31,30 @@ struct RhsParams {
   double ca[3], ct[3];    // explicit weights a_j and a~_j of the stage's explicit terms
   double cg[3], cgI;      // gravity weights of the explicit terms and of the implicit one
   int radial;             // 0: e_z, |g| const; 1: e_r = X/|X|, factor a^2/|X|^2
+  // Rayleigh damping of the momentum towards (sp_u, 0) (the 2D hill case's upper sponge and
+  // lateral relaxation zones; no counterpart in the reference): rate tau(x, z) of sponge_rate
+  int sponge;
+  double sp_z0, sp_z1, sp_rate, sp_x0, sp_x1, sp_width, sp_rate_lat, sp_u;
+  // the point functions read the physical position for radial gravity and for the sponge
+  __device__ bool needs_position() const { return radial != 0 || sponge != 0; }
 };
+
+// tau(x, z) = rate sin^2(pi/2 (z - z0)/(z1 - z0)) above z0, plus rate_lat cos^2(pi/2 d/width)
+// within width of the nearer lateral boundary (d its distance); 1/s in the non-dimensional units
+__device__ __forceinline__ double sponge_rate(const RhsParams& prm, const PointGeo& pg) {
+  const double half_pi = 1.5707963267948966;
+  double tau = 0.0;
+  if (pg.X[1] > prm.sp_z0) {
+    const double s = sin(half_pi * (pg.X[1] - prm.sp_z0) / (prm.sp_z1 - prm.sp_z0));
+    tau += prm.sp_rate * s * s;
+  }
+  const double d = fmin(pg.X[0] - prm.sp_x0, prm.sp_x1 - pg.X[0]);
+  if (d < prm.sp_width) {
+    const double c = cos(half_pi * d / prm.sp_width);
+    tau += prm.sp_rate_lat * c * c;
+  }
+  return tau;
+}
 
 __device__ __forceinline__ void gravity_dir(const RhsParams& prm, const PointGeo& pg, double& e0, double& e1,
                                             double& fac) {
@@ -148,6 +171,11 @@ struct RhsPhys {
           } else {
             val[O_U + 1] -= cg * prm.invFr2 * rho;
           }
+          if (prm.sponge) {  // -dt a_j tau rho_j (u_j - u_ref)
+            const T ct_ = ca * sponge_rate(prm, pg) * rho;
+            val[O_U] -= ct_ * (ux - prm.sp_u);
+            val[O_U + 1] -= ct_ * uz;
+          }
           const T cr = ca * rho, pt = ct * prm.invMa2 * p;
           gr[O_U][0] += cr * ux * ux + pt;
           gr[O_U][1] += cr * ux * uz;
@@ -230,6 +258,11 @@ struct RhsPhys {
             fv[O_U + 1] -= gfac * e1;
           } else {
             fv[O_U + 1] -= cg * prm.invFr2 * rdw;
+          }
+          if (prm.sponge) {  // -dt a_j tau rho_j (u_j - u_ref)
+            const double ct_ = ca * sponge_rate(prm, pg) * rdw;
+            fv[O_U] -= ct_ * (ux - prm.sp_u);
+            fv[O_U + 1] -= ct_ * uz;
           }
           const double pt = ct * prm.invMa2 * p;
           const double cx = cr * ux, cz = cr * uz;

@@ -98,6 +98,13 @@ class IMEXStepper:
     def step(self, n=1):
         check(_bind().af_imex_step(self._h, n))
 
+    def set_sponge(self, z_start, z_top, rate_top, x_left, x_right, width_lateral, rate_lateral, u_ref):
+        """Rayleigh damping of the momentum (af_set_sponge on the stepper's operator)."""
+        from atmospheric_flows_b200.operator import lib as oplib
+        L = oplib()
+        check(L.af_set_sponge(_bind().af_imex_operator(self._h), z_start, z_top, rate_top, x_left, x_right,
+                              width_lateral, rate_lateral, u_ref))
+
     def _triple(self):
         import torch
         return (torch.empty(self.n_scalar, dtype=torch.float64, device="cuda"),

@@ -67,6 +67,7 @@ def lib():
         L.af_compute_diagnostics.argtypes = [vp, dp, dp, dp, dp, ctypes.POINTER(Diagnostics)]
         L.af_l2_norm.argtypes = [vp, ip, dp, ctypes.POINTER(ctypes.c_double)]
         L.af_set_stage_wait_test.argtypes = [vp, ip]
+        L.af_set_sponge.argtypes = [vp] + [ctypes.c_double] * 8
         L.af_error_string.restype = ctypes.c_char_p
         L.af_error_string.argtypes = [ip]
         L.af_last_error_message.restype = ctypes.c_char_p
@@ -273,6 +274,13 @@ class EULEROperator:
         out = ctypes.c_double()
         check(lib().af_l2_norm(self._h, ncomp, _ptr(v), ctypes.byref(out)))
         return out.value
+
+    def set_sponge(self, z_start, z_top, rate_top, x_left, x_right, width_lateral, rate_lateral, u_ref):
+        """Rayleigh damping of the momentum towards (u_ref, 0): an upper sponge above z_start and
+        relaxation zones of width_lateral at x_left and x_right (no counterpart in the reference;
+        the 2D hill configuration's damping layers).  Rates 0 switch it off."""
+        check(lib().af_set_sponge(self._h, z_start, z_top, rate_top, x_left, x_right, width_lateral, rate_lateral,
+                                  u_ref))
 
     def set_stage_wait_test(self, polls):
         """Test hook: polls > 0 makes the handle's cell kernels give up a bounded wait (before any

@@ -145,6 +145,17 @@ int af_n_dofs(const af_operator* op, int space, long long* n);
 /* Number of kernels this library launched on the handle since creation. */
 int af_launch_count(const af_operator* op, long long* n);
 
+/* Rayleigh damping of the momentum towards (u_ref, 0), added to the explicit momentum rhs of
+ * every stage with the stage's explicit weights: -dt sum_j a_j tau rho_j (u_j - u_ref), with
+ * tau(x, z) = rate_top sin^2(pi/2 (z - z_start)/(z_top - z_start)) above z_start (an upper
+ * sponge) plus rate_lateral cos^2(pi/2 d/width_lateral) within width_lateral of the nearer of
+ * x_left and x_right (relaxation zones; d the distance).  Rates in 1/s of the non-dimensional
+ * units; both 0 (the default) switch it off.  No counterpart in the reference: the damping
+ * layers of the 2D hill configuration.  The stage-1 tangent and adjoint kernels have no sponge
+ * term (AF_UNSUPPORTED while it is on). */
+int af_set_sponge(af_operator* op, double z_start, double z_top, double rate_top, double x_left, double x_right,
+                  double width_lateral, double rate_lateral, double u_ref);
+
 /* Failure detection (no counterpart in the reference, whose deal.II loops have no waits):
  * the cell kernels wait for their bulk copies with a bounded number of polls.  A kernel that
  * gives up leaves a code in the handle's status word and returns without writing its

@@ -181,6 +181,10 @@ struct Op {
   // configuration); factors of M and of A(rho_for_fixed), rebuilt when emptied
   int exact_inverse = 0;
   std::vector<N> M_chol, A_chol;
+  // Rayleigh damping of the momentum (the 2D hill configuration's upper sponge and lateral
+  // relaxation zones; no counterpart in the reference, see sponge_rate)
+  int sponge = 0;
+  N sp_z0 = 0, sp_z1 = 1, sp_rate = 0, sp_x0 = 0, sp_x1 = 1, sp_width = 1, sp_rate_lat = 0, sp_u = 0;
   int ncell() const { return nx * nz; }
   int nd() const { return (P + 1) * (P + 1); }
   long nscalar() const { return (long)ncell() * nd(); }
@@ -467,6 +471,26 @@ struct CellSubmit {
   }
 };
 
+/* Damping rate tau(x, z) of the sponge (1/s in the non-dimensional units L_ref = u_ref = 1):
+ * rate sin^2(pi/2 (z - z0)/(z1 - z0)) above z0 (Klemp-Lilly upper layer), plus
+ * rate_lat cos^2(pi/2 d/width) within width of the lateral boundaries x0 and x1 (d the distance
+ * to the nearer one).  Documented extension of the 2D hill case; the reference has none. */
+template <typename N>
+static N sponge_rate(const Op<N>& o, const N X[2]) {
+  const N half_pi = (N)1.5707963267948966192313216916397514L;
+  N tau = 0;
+  if (X[1] > o.sp_z0) {
+    const N s = std::sin(half_pi * (X[1] - o.sp_z0) / (o.sp_z1 - o.sp_z0));
+    tau += o.sp_rate * s * s;
+  }
+  const N d = std::min(X[0] - o.sp_x0, o.sp_x1 - X[0]);
+  if (d < o.sp_width) {
+    const N c = std::cos(half_pi * d / o.sp_width);
+    tau += o.sp_rate_lat * c * c;
+  }
+  return tau;
+}
+
 /* ========================================================================= */
 /* Explicit right-hand sides                                                  */
 /* ========================================================================= */
@@ -685,9 +709,17 @@ static void rhs_velocity(const Op<N>& o, N* dst, const N* const* src, int nsrc) 
       N X[2] = {cq.X[2 * q], cq.X[2 * q + 1]}, e[2], fac;
       gravity_at(o, X, e, fac);
       N u0[2] = {ux[0][q], uz[0][q]};
+      // sponge: -dt sum_j a_j tau rho_j (u_j - u_ref), u_ref = (sp_u, 0), with the explicit
+      // weights of the stage (no counterpart in the reference)
+      const N tau = o.sponge ? sponge_rate(o, X) : (N)0;
       for (int d = 0; d < 2; ++d) {
         N v = rho[0][q] * u0[d];
         for (int k = 0; k < ng; ++k) v -= cg[k] * o.dt / Fr2 * rg[k][q] * e[d] * fac;
+        if (o.sponge)
+          for (int j = 0; j < nj; ++j) {
+            const N uj = d == 0 ? ux[j][q] - o.sp_u : uz[j][q];
+            v -= ca[j] * o.dt * tau * rho[j][q] * uj;
+          }
         sub.value(d, q, v);
       }
       N T[2][2] = {{0, 0}, {0, 0}};
@@ -1354,6 +1386,14 @@ int orc_get_num_threads(void) {
 
 void orc_set_params(void* h, double Ma, double Fr, double dt) {
   ORC_DISPATCH(h, (o.Ma = Ma, o.Fr = Fr, o.dt = dt), (o.Ma = Ma, o.Fr = Fr, o.dt = dt));
+}
+void orc_set_sponge(void* h, int on, double z0, double z1, double rate, double x0, double x1, double width,
+                    double rate_lat, double u_ref) {
+  ORC_DISPATCH(h,
+               (o.sponge = on, o.sp_z0 = z0, o.sp_z1 = z1, o.sp_rate = rate, o.sp_x0 = x0, o.sp_x1 = x1,
+                o.sp_width = width, o.sp_rate_lat = rate_lat, o.sp_u = u_ref),
+               (o.sponge = on, o.sp_z0 = z0, o.sp_z1 = z1, o.sp_rate = rate, o.sp_x0 = x0, o.sp_x1 = x1,
+                o.sp_width = width, o.sp_rate_lat = rate_lat, o.sp_u = u_ref));
 }
 void orc_set_stages(void* h, int hyperbolic, int ns) {
   ORC_DISPATCH(h, (o.hyperbolic_stage = hyperbolic, o.ns_stage = ns), (o.hyperbolic_stage = hyperbolic, o.ns_stage = ns));

@@ -40,6 +40,7 @@ def lib():
         L.orc_destroy.argtypes = [ctypes.c_void_p]
         L.orc_set_params.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.orc_set_stages.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_set_sponge.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 8
         L.orc_set_fixed.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         L.orc_rhs.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, ctypes.POINTER(dp), ctypes.c_int]
         L.orc_vmult.restype = ctypes.c_int
@@ -117,6 +118,13 @@ class OracleOperator:
 
     def set_Froude(self, Fr):
         self.Fr = Fr; self._push()
+
+    def set_sponge(self, z_start, z_top, rate_top, x_left, x_right, width_lateral, rate_lateral, u_ref):
+        """Rayleigh damping of the momentum towards (u_ref, 0) (the hill case's upper sponge and
+        lateral relaxation zones, no counterpart in the reference); rates 0 switch it off."""
+        on = int(rate_top > 0 or rate_lateral > 0)
+        lib().orc_set_sponge(self._h, on, z_start, z_top, rate_top, x_left, x_right, width_lateral, rate_lateral,
+                             u_ref)
 
     def set_HYPERBOLIC_stage(self, s):
         assert 1 <= s <= 3

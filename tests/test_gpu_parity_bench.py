@@ -159,3 +159,73 @@ def test_imex_100_steps_on_the_40x16_hill():
 def test_imex_10_accurate_steps_on_the_40x16_hill():
     for k, e in _imex_40x16(10, 1e-12, True).items():
         assert e < 1e-9, (k, e)
+
+
+# Rayleigh damping layers of the 2D hill case (no counterpart in the reference): the upper
+# sponge above 10 km and relaxation zones 4 km wide at the lateral boundaries, towards the
+# inflow velocity (10 m/s, 0).
+SPONGE = dict(z_start=10000.0, z_top=16000.0, rate_top=0.05, x_left=-20000.0, x_right=20000.0,
+              width_lateral=4000.0, rate_lateral=0.02, u_ref=10.0)
+
+
+@pytest.mark.parametrize("P", [2, 4])
+def test_rhs_parity_with_sponge(P):
+    from atmospheric_flows_b200.operator import EULEROperator
+    from oracle.oracle import OracleOperator
+    m = M.jitter_mesh(M.hill_mesh(10, 5, periodic_x=True), 0.1, seed=4)
+    sc = M.Scaling()
+    g = EULEROperator(m, P, sc.Ma, sc.Fr, 3.0)
+    o = OracleOperator(m, P, sc.Ma, sc.Fr, 3.0)
+    g.set_sponge(**SPONGE)
+    o.set_sponge(**SPONGE)
+    states = [M.hill_state(m, P, seed=5 + k, amplitude=0.05) for k in range(3)]
+    ns = m.n_cells * (P + 1) ** 2
+    o0 = OracleOperator(m, P, sc.Ma, sc.Fr, 3.0)  # without the sponge: the term must matter
+    for stage in (1, 2, 3):
+        g.set_HYPERBOLIC_stage(stage)
+        o.set_HYPERBOLIC_stage(stage)
+        o0.set_HYPERBOLIC_stage(stage)
+        src = _stage_sources(tuple(states), stage)
+        vel_src = src[:3 * stage] + ([src[3 * stage]] if stage < 3 else [])
+        want = o.vmult_rhs_velocity_fixed(vel_src)
+        assert rel(want, o0.vmult_rhs_velocity_fixed(vel_src)) > 1e-6
+        dst = torch.full((2 * ns,), np.nan, dtype=torch.float64, device="cuda")
+        g.vmult_rhs_velocity_fixed(dst, [_d(a) for a in vel_src])
+        assert rel(_h(dst), want) < TOL, ("separate", stage)
+        dr, du, dp = (torch.zeros(k * ns, dtype=torch.float64, device="cuda") for k in (1, 2, 1))
+        g.vmult_rhs_fused(dr, du, dp, [_d(a) for a in src])
+        assert rel(_h(du), want) < TOL, ("fused", stage)
+        assert rel(_h(dp), o.vmult_rhs_pressure(src)) < TOL, ("pressure unaffected", stage)
+
+
+def _imex_40x16_sponge(nsteps, accurate):
+    from atmospheric_flows_b200.imex import IMEXStepper
+    from oracle.oracle import OracleOperator, imex_steps
+    P, dt, eps = 4, 2.0, 1e-12
+    m = M.hill_mesh(40, 16, periodic_x=True)
+    sc = M.Scaling()
+    st = M.hill_state(m, P, amplitude=1e-3)
+    o = OracleOperator(m, P, sc.Ma, sc.Fr, dt)
+    o.set_sponge(**SPONGE)
+    ref = imex_steps(o, st.rho, st.u, st.p, nsteps, eps=eps, exact_inverse=True, true_residual=accurate)
+    g = IMEXStepper(m, P, sc.Ma, sc.Fr, dt, eps=eps, schur_preconditioner="jacobi" if accurate else None)
+    g.set_sponge(**SPONGE)
+    g.set_state(_d(st.rho), _d(st.u), _d(st.p))
+    g.step(nsteps)
+    got = [t.cpu().numpy() for t in g.get_state()]
+    errs = {k: rel(a, b) for k, a, b in zip(("rho", "u", "p"), got, ref[:3])}
+    print(f"imex 40x16 p=4 with sponge, {nsteps} steps, accurate solves {accurate}: state errors vs oracle {errs}")
+    return errs
+
+
+def test_imex_100_steps_with_sponge_on_the_40x16_hill():
+    """The plain FP64 hill case with its damping layers: Rayleigh sponge above 10 km and
+    lateral relaxation zones (periodic lateral boundaries), 100 steps at the reference's
+    criterion (stated tolerance 1e-6, as above)."""
+    for k, e in _imex_40x16_sponge(100, False).items():
+        assert e < 1e-6, (k, e)
+
+
+def test_imex_10_accurate_steps_with_sponge_on_the_40x16_hill():
+    for k, e in _imex_40x16_sponge(10, True).items():
+        assert e < 1e-9, (k, e)

@@ -537,3 +537,32 @@ def test_hydrostatic_balance(case):
         res.append(np.linalg.norm(resid) / np.linalg.norm(grav))
     assert res[1] < res[0] / 4
     assert res[1] < (1e-4 if case == "hill" else 1e-3)
+
+
+def test_sponge_vanishes_at_the_reference_velocity_and_outside_its_layers():
+    """The oracle's Rayleigh damping term (no counterpart in the reference) is zero where the
+    velocity equals the reference velocity, and zero on cells below the sponge and away from the
+    lateral zones; elsewhere it changes the momentum rhs."""
+    import numpy as np
+    from atmospheric_flows_b200 import mesh as M
+    from oracle.oracle import OracleOperator
+    P = 2
+    m = M.hill_mesh(10, 8, periodic_x=True)
+    sc = M.Scaling()
+    st = M.hill_state(m, P, seed=3, amplitude=0.05)
+    ns = m.n_cells * (P + 1) ** 2
+    kw = dict(z_start=10000.0, z_top=16000.0, rate_top=0.05, x_left=-20000.0, x_right=20000.0,
+              width_lateral=4000.0, rate_lateral=0.02, u_ref=10.0)
+    a = OracleOperator(m, P, sc.Ma, sc.Fr, 2.0)
+    b = OracleOperator(m, P, sc.Ma, sc.Fr, 2.0)
+    b.set_sponge(**kw)
+    uref = np.zeros(2 * ns)
+    uref.reshape(m.n_cells, 2, -1)[:, 0, :] = 10.0
+    src = [st.rho, uref, st.p, st.rho]
+    assert np.array_equal(a.vmult_rhs_velocity_fixed(src), b.vmult_rhs_velocity_fixed(src))
+    src = [st.rho, st.u, st.p, st.rho]
+    d = (b.vmult_rhs_velocity_fixed(src) - a.vmult_rhs_velocity_fixed(src)).reshape(m.n_cells, -1)
+    cz = M.dof_coordinates(m, P).reshape(m.n_cells, -1, 2)
+    inside = (cz[..., 1].max(axis=1) > 10000.0) | (np.abs(cz[..., 0]).max(axis=1) > 16000.0)
+    assert np.abs(d[~inside]).max() == 0.0
+    assert np.abs(d[inside]).max() > 0.0
