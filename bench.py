@@ -702,6 +702,64 @@ def run_timeline():
     print(json.dumps(out))
 
 
+def run_production_full(nsteps=1000, adjoint_steps=100, every=10):
+    """The production-size hill run in full (opt-in: about half an hour on one B200): periodic
+    hill 2048x512, degree 4 (104.9 M DoFs), dt 0.125 s, eps 1e-8; nsteps mixed-precision steps
+    and nsteps plain FP64 steps from the same state, the field error between them, and the
+    adjoint gradient of J = |w|^2/2 over z < 8 km at the final step with respect to the state
+    adjoint_steps steps earlier, by checkpointed recomputation (a checkpoint every `every`
+    steps).  Device time by CUDA events for the steps; wall clock for the gradient."""
+    import torch
+    from atmospheric_flows_b200 import mesh as M
+    from atmospheric_flows_b200.imex import IMEXStepper
+    sc = M.Scaling()
+    P = DEGREE
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    m = M.hill_mesh(2048, 512, periodic_x=True)
+    st = M.hill_state(m, P, seed=SEED, modes=4)
+    out = {"config": f"periodic hill 2048x512, degree {P} ({4 * m.n_cells * (P + 1) ** 2} DoFs), dt=0.125 s, eps=1e-8, "
+                     f"{nsteps} steps per precision from the same state; gradient of J = |w|^2/2 over z < 8 km at step "
+                     f"{nsteps} with respect to the state at step {nsteps - adjoint_steps}, a checkpoint every {every}"}
+    finals = {}
+    for name, pc in (("mixed", "cheb_fp32"), ("fp64", "jacobi")):
+        g = IMEXStepper(m, P, sc.Ma, sc.Fr, 0.125, eps=1e-8, schur_preconditioner=pc)
+        g.set_state(d(st.rho), d(st.u), d(st.p))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start_state = None
+        e0.record()
+        g.step(nsteps - adjoint_steps)
+        if name == "mixed":
+            start_state = [t.clone() for t in g.get_state()]
+        g.step(adjoint_steps)
+        e1.record()
+        e1.synchronize()
+        finals[name] = [t.clone() for t in g.get_state()]
+        out[name] = {"s_per_step": e0.elapsed_time(e1) * 1e-3 / nsteps, "stats_last_step": g.stats()}
+        if name == "mixed":
+            zc = M.dof_coordinates(m, P)[..., 1].reshape(-1)
+            low = d((zc < 8000.0).astype(np.float64))
+            uN = finals[name][1]
+            ns = m.n_cells * (P + 1) ** 2
+            wbar = torch.zeros(2 * ns, dtype=torch.float64, device="cuda")
+            wbar.view(m.n_cells, 2, -1)[:, 1, :] = uN.view(m.n_cells, 2, -1)[:, 1, :] * low.view(m.n_cells, -1)
+            zr = torch.zeros(ns, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            gb = g.gradient(*start_state, adjoint_steps, every, zr, wbar, zr, rel_tol=1e-10)
+            torch.cuda.synchronize()
+            out["gradient"] = {"seconds": time.perf_counter() - t0, "steps": adjoint_steps, "checkpoint_every": every,
+                               "grad_norms": [float(torch.linalg.norm(v)) for v in gb],
+                               "finite": all(bool(torch.isfinite(v).all()) for v in gb)}
+            del gb, start_state
+        del g
+        torch.cuda.synchronize()
+    out["field_error_mixed_vs_fp64"] = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+                                           for a, b in zip(finals["mixed"], finals["fp64"]))
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["s_per_step"] / out["mixed"]["s_per_step"]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -712,6 +770,9 @@ def main():
     ap.add_argument("--no-solvers", action="store_true", help="skip the Schur-solve and IMEX-step measurements")
     ap.add_argument("--profile", choices=["rhs", "adjoint", "schur", "imex"],
                     help="run one workload briefly for an ncu capture and exit (no measurement)")
+    ap.add_argument("--production-full", action="store_true",
+                    help="the 2048x512 hill run in full: 1000 mixed and 1000 FP64 steps, the gradient over the last "
+                         "100 (about half an hour); prints one JSON object")
     ap.add_argument("--timeline", action="store_true",
                     help="trace one warm IMEX step (mixed and FP64) and print its kernel timeline summary")
     args = ap.parse_args()
@@ -720,6 +781,9 @@ def main():
         return
     if args.timeline:
         run_timeline()
+        return
+    if args.production_full:
+        run_production_full()
         return
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
