@@ -1184,10 +1184,10 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       }
     }
     __syncthreads();
-    // pass 3 (along x): x[iz][ix] = sum_qx Vi[ix][qx] v[iz][qx], then the store or update
+    // pass 3 (along x): x[iz][ix] = sum_qx Vi[ix][qx] v[iz][qx], in place of the row
     for (int e = tid; e < NC * ncb * P1; e += NT) {
       const int o = e / (ncb * P1), cc = (e / P1) % ncb, iz = e % P1;
-      const R* row = ubase(o, cc) + iz * P1;
+      R* row = ubase(o, cc) + iz * P1;
       R v[P1];
 #pragma unroll
       for (int qx = 0; qx < P1; ++qx) v[qx] = row[qx];
@@ -1196,25 +1196,33 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         R y = R(0);
 #pragma unroll
         for (int qx = 0; qx < P1; ++qx) y = fmaR(cb.Vi[ix][qx], v[qx], y);
-        if constexpr (L::EPI == 1) {
-          // one output array, NOUT components, [cell][comp][node]
-          ptr.out[0][((size_t)(c0 + cc) * NOUT + o) * ND + iz * P1 + ix] = prm.scale * y;
-        } else if constexpr (L::EPI == 3) {  // z, din and x come from the prefetched chunks
-          const int l = cc * ND + iz * P1 + ix;
-          const size_t g = (size_t)c0 * ND + l;
-          const R dl = s_minv[2 * CB * ND + l];
-          const R zn = s_minv[CB * ND + l] + prm.g * y - dl;
-          const R nd = prm.alpha * dl + prm.s * zn;
-          prm.r[g] = zn;
-          prm.dout[g] = nd;
-          prm.x[g] = prm.first ? nd : s_minv[3 * CB * ND + l] + nd;
-        } else {  // din and x come from the prefetched chunks
-          const int l = cc * ND + iz * P1 + ix;
-          const size_t g = (size_t)c0 * ND + l;
-          const R nd = (prm.alpha != R(0) ? prm.alpha * s_minv[2 * CB * ND + l] : R(0)) + prm.s * y;
-          prm.dout[g] = nd;
-          prm.x[g] = prm.first ? nd : s_minv[3 * CB * ND + l] + nd;
-        }
+        row[ix] = y;
+      }
+    }
+    __syncthreads();
+    // the store or the update, one element per thread in global order (coalesced)
+    for (int e = tid; e < NC * ncb * ND; e += NT) {
+      if constexpr (L::EPI == 1) {
+        // one output array, NOUT components, [cell][comp][node]: e is the offset from the CTA's first
+        const int cc = e / (NOUT * ND), o = (e / ND) % NOUT, k = e % ND;
+        ptr.out[0][(size_t)c0 * NOUT * ND + e] = prm.scale * ubase(o, cc)[k];
+      } else if constexpr (L::EPI == 3) {  // z, din and x come from the prefetched chunks
+        const int cc = e / ND, k = e % ND;
+        const size_t g = (size_t)c0 * ND + e;
+        const R y = ubase(0, cc)[k];
+        const R dl = s_minv[2 * CB * ND + e];
+        const R zn = s_minv[CB * ND + e] + prm.g * y - dl;
+        const R nd = prm.alpha * dl + prm.s * zn;
+        prm.r[g] = zn;
+        prm.dout[g] = nd;
+        prm.x[g] = prm.first ? nd : s_minv[3 * CB * ND + e] + nd;
+      } else {  // din and x come from the prefetched chunks
+        const int cc = e / ND, k = e % ND;
+        const size_t g = (size_t)c0 * ND + e;
+        const R y = ubase(0, cc)[k];
+        const R nd = (prm.alpha != R(0) ? prm.alpha * s_minv[2 * CB * ND + e] : R(0)) + prm.s * y;
+        prm.dout[g] = nd;
+        prm.x[g] = prm.first ? nd : s_minv[3 * CB * ND + e] + nd;
       }
     }
   }

@@ -57,6 +57,12 @@ class EulerOperator {
   void set_dt(double v) { check(af_set_dt(h_, v), "set_dt"); }
   void set_Mach(double v) { check(af_set_Mach(h_, v), "set_Mach"); }
   void set_Froude(double v) { check(af_set_Froude(h_, v), "set_Froude"); }
+  // Rayleigh damping layers of the 2D hill case (no counterpart in the reference)
+  void set_sponge(double z_start, double z_top, double rate_top, double x_left, double x_right, double width_lateral,
+                  double rate_lateral, double u_ref) {
+    check(af_set_sponge(h_, z_start, z_top, rate_top, x_left, x_right, width_lateral, rate_lateral, u_ref),
+          "set_sponge");
+  }
   void set_HYPERBOLIC_stage(int s) { check(af_set_HYPERBOLIC_stage(h_, s), "set_HYPERBOLIC_stage"); }
   void set_NS_stage(int s) { check(af_set_NS_stage(h_, s), "set_NS_stage"); }
   void set_rho_for_fixed(const double* v) { check(af_set_rho_for_fixed(h_, v), "set_rho_for_fixed"); }
