@@ -79,26 +79,76 @@ def profile_numbers():
     return out
 
 
-class Clocks:
-    """nvidia-smi sampling (every 100 ms, with timestamps) around the timed region; mark() the
-    region's start and end, and the summary keeps the samples taken inside it (all samples,
-    flagged, when the region was too short to hold one)."""
+def gpu_pci_id(dev):
+    """The PCI bus id of a torch CUDA device in NVML's and nvidia-smi's form, or None."""
+    try:
+        import torch
+        pr = torch.cuda.get_device_properties(dev)
+        return f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+    except Exception:
+        return None
 
-    def __init__(self, index):
-        self.index = index
+
+_REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+            ("sw_power_cap", 0x4))
+
+
+class Clocks:
+    """SM clocks and throttle reasons around the timed region: nvidia-smi every 100 ms with
+    timestamps, and NVML read every 2 ms by a thread (the timed region of a short run is a few
+    ms).  mark() the region's start and end; the summary keeps the samples inside it (NVML's
+    when there are any, else nvidia-smi's, else all samples, flagged).  `gpu` is the device's
+    PCI bus id (or an index); `nvml` a module with pynvml's interface (tests pass a fake)."""
+
+    def __init__(self, gpu, nvml=None):
+        self.gpu = gpu
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
         self.t0 = self.t1 = None
+        self.nv_rows = []
+        self._nv = nvml
+        self._stop = None
+        self._thread = None
+
+    def _nvml_handle(self):
+        nv = self._nv
+        if nv is None:
+            import pynvml as nv
+            self._nv = nv
+        nv.nvmlInit()
+        if isinstance(self.gpu, str):
+            return nv.nvmlDeviceGetHandleByPciBusId(self.gpu)
+        return nv.nvmlDeviceGetHandleByIndex(int(self.gpu))
+
+    def _poll(self, h):
+        nv = self._nv
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                break
+            self.nv_rows.append((time.time(), float(sm), float(mx), {n for n, b in _REASONS if bits & b}))
+            self._stop.wait(0.002)
 
     def __enter__(self):
+        import threading
         q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
                                        "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.p = None
+        try:
+            h = self._nvml_handle()
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._poll, args=(h,), daemon=True)
+            self._thread.start()
+        except Exception:
+            self._thread = None
         time.sleep(0.3)
         return self
 
@@ -114,31 +164,40 @@ class Clocks:
             time.sleep(0.15)  # one more sample after the region
             self.p.terminate()
             self.p.wait()
+        if self._thread:
+            self._stop.set()
+            self._thread.join()
 
     def summary(self):
         import datetime
-        self.f.flush()
-        self.f.seek(0)
-        rows = []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 10:
-                continue
-            try:
-                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                rows.append((ts, float(parts[2]), float(parts[3]),
-                             {n for n, v in zip(names, parts[6:10]) if v.lower() == "active"}))
-            except ValueError:
-                continue
-        inside = [r for r in rows if self.t0 is not None and self.t1 is not None and self.t0 <= r[0] <= self.t1]
-        use = inside or rows
+        inside = lambda rows: [r for r in rows if self.t0 is not None and self.t1 is not None and
+                               self.t0 <= r[0] <= self.t1]
+        nv_in = inside(self.nv_rows)
+        if nv_in:
+            use, window = nv_in, "timed region (NVML every 2 ms)"
+        else:
+            self.f.flush()
+            self.f.seek(0)
+            rows = []
+            names = [n for n, _ in _REASONS]
+            for line in self.f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                try:
+                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    rows.append((ts, float(parts[2]), float(parts[3]),
+                                 {n for n, v in zip(names, parts[6:10]) if v.lower() == "active"}))
+                except ValueError:
+                    continue
+            smi_in = inside(rows)
+            use = smi_in or rows
+            window = "timed region" if smi_in else "around the timed region (shorter than the sampling interval)"
         sm = [r[1] for r in use]
         reasons = set().union(*(r[3] for r in use)) if use else set()
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max((r[2] for r in use), default=None),
-                "reasons": sorted(reasons), "samples": len(sm),
-                "window": "timed region" if inside else "around the timed region (shorter than the sampling interval)"}
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 CPU_ROWS = 32  # the CPU sample: a 512x32 strip of the workload mesh, 1/8 of its cells
@@ -463,7 +522,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     launches0 = op.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local_rank) as clk:
+    with Clocks(gpu_pci_id(dev) or local_rank) as clk:
         clk.mark()
         e0.record(stream)
         for _ in range(args.steps):

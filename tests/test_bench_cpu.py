@@ -79,3 +79,39 @@ def test_clock_summary_keeps_the_samples_inside_the_timed_region():
     s = c.summary()
     assert s["samples"] == 12 and s["window"].startswith("around")
     assert s["reasons"] == ["sw_power_cap"]
+
+
+def test_clock_summary_prefers_nvml_samples_inside_the_region():
+    """With a (fake) NVML, the polling thread's samples inside the timed region give the clock
+    and the reasons, at a rate that fits a region of a few milliseconds."""
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class FakeNVML:
+        NVML_CLOCK_SM = 1
+
+        def nvmlInit(self):
+            pass
+
+        def nvmlDeviceGetHandleByPciBusId(self, bus):
+            return bus
+
+        def nvmlDeviceGetMaxClockInfo(self, h, kind):
+            return 1965
+
+        def nvmlDeviceGetClockInfo(self, h, kind):
+            return 1950
+
+        def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+            return 0x4  # sw_power_cap
+
+    c = bench.Clocks("00000000:1b:00.0", nvml=FakeNVML())
+    with c:
+        c.mark()
+        time.sleep(0.05)
+        c.mark()
+    s = c.summary()
+    assert s["window"].startswith("timed region (NVML")
+    assert s["samples"] >= 5 and s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
