@@ -26,6 +26,7 @@ namespace af {
 struct RhsAdj1Phys {
   static constexpr int NG = 1;
   static constexpr bool FACES = true, NEED_X = true, ACCUMULATE = false;
+  static constexpr bool FOLD = true;  // z-face folding measured faster (1.53 -> 1.43 ms, 0.97 -> 0.90 ms)
   static constexpr int NOUT_ARR = 5, NOUT = 7;
   using Params = RhsParams;
   using real = double;
@@ -163,6 +164,7 @@ struct RhsAdj1Phys {
 struct RhsTlm1Phys {
   static constexpr int NG = 1;
   static constexpr bool FACES = true, NEED_X = true, ACCUMULATE = false;
+  static constexpr bool FOLD = true;  // z-face folding measured faster (1.53 -> 1.43 ms, 0.97 -> 0.90 ms)
   static constexpr int NOUT_ARR = 3, NOUT = 4;
   using Params = RhsParams;
   using real = double;

@@ -82,6 +82,20 @@ struct MappedOf<Phys, std::void_t<decltype(Phys::MAPPED)>> {
   static constexpr bool value = Phys::MAPPED;
 };
 
+// Policies opt in to z-face folding (Layout::FOLD_Z) with Phys::FOLD = true.  Measured at
+// 512x256, p = 4: the fused rhs 439 -> 399 us with it, its stage-1 backward 1.53 -> 1.43 ms;
+// C (the enthalpy operator) 125 -> 153 us and the FP64 IMEX step 265 -> 275 ms, where the
+// z-faces evaluated after the z pass serialise behind it; the FP32 smoother kernels are
+// indifferent (mixed step 77.1 vs 77.4 ms).
+template <class Phys, class = void>
+struct FoldOf {
+  static constexpr bool value = false;
+};
+template <class Phys>
+struct FoldOf<Phys, std::void_t<decltype(Phys::FOLD)>> {
+  static constexpr bool value = Phys::FOLD;
+};
+
 // Whether a policy's point functions read the physical position: Phys::NEED_X, and for
 // parameters that say so (needs_position()) only when they do (the vertical gravity of the hill
 // needs no position, radial gravity and the sponge do).
@@ -350,8 +364,9 @@ struct Layout {
   // x-transpose pass then has no edge rows with extra work
   // (two input buffers: FACE_G + 2 >= NG; one buffer: FACE_G is the last group)
   static constexpr int FACE_G = PhysInfo<Phys>::FACE_G;
-  static constexpr bool FOLD_2BUF = Phys::FACES && PhysInfo<Phys>::NFACEG == 1 && FACE_G + 2 >= Phys::NG;
-  static constexpr bool FOLD_1BUF = Phys::FACES && PhysInfo<Phys>::NFACEG == 1 && FACE_G == Phys::NG - 1;
+  static constexpr bool FOLD_OK = FoldOf<Phys>::value && Phys::FACES && PhysInfo<Phys>::NFACEG == 1;
+  static constexpr bool FOLD_2BUF = FOLD_OK && FACE_G + 2 >= Phys::NG;
+  static constexpr bool FOLD_1BUF = FOLD_OK && FACE_G == Phys::NG - 1;
   static constexpr int flux_size(bool fold) { return Phys::FACES ? (fold ? 2 : 4) * NOUT * CB * NQ : 0; }
 
   // per cell: A,B,C,v0 (8) + 4 faces x (nx,nz,len) (12) + 4 nb; an odd stride, so that a warp

@@ -102,6 +102,7 @@ struct RhsPhys {
   static constexpr bool HAS_I = STAGE < 3 ? (VEL || PRES) : PRES;
   static constexpr int NG = STAGE + (HAS_I ? 1 : 0);
   static constexpr bool FACES = true, NEED_X = true, ACCUMULATE = false;
+  static constexpr bool FOLD = true;  // z-face folding (Layout::FOLD_Z) measured faster here
   static constexpr int NOUT_ARR = (RHO ? 1 : 0) + (VEL ? 1 : 0) + (PRES ? 1 : 0);
   static constexpr int NOUT = (RHO ? 1 : 0) + (VEL ? 2 : 0) + (PRES ? 1 : 0);
   static constexpr int O_RHO = 0, O_U = RHO ? 1 : 0, O_P = (RHO ? 1 : 0) + (VEL ? 2 : 0);
