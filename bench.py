@@ -722,14 +722,14 @@ def run_timeline():
     m = M.hill_mesh(512, 256, periodic_x=True)
     st = M.hill_state(m, DEGREE, seed=SEED, modes=4)
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-    out = {"config": "periodic hill 512x256, degree 4, dt=0.5 s, eps=1e-8, one warm step after one warm-up step"}
-    for label, pc in (("mixed", "cheb_fp32"), ("fp64", "jacobi")):
-        g = IMEXStepper(m, DEGREE, sc.Ma, sc.Fr, 0.5, eps=1e-8, schur_preconditioner=pc)
-        g.set_state(d(st.rho), d(st.u), d(st.p))
-        g.step(1)
+    out = {"config": "periodic hill 512x256, degree 4, dt=0.5 s, eps=1e-8, one warm step after one warm-up step; "
+                     "step_backward: the adjoint of one mixed-precision step (eps 1e-10, as in the gradient) at its "
+                     "recorded forward, after one warm-up adjoint"}
+
+    def trace(fn):
         torch.cuda.synchronize()
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
-            g.step(1)
+            fn()
             torch.cuda.synchronize()
         iv = sorted((e.time_range.start, e.time_range.end, e.name) for e in prof.events()
                     if e.device_type == torch.autograd.DeviceType.CUDA)
@@ -749,15 +749,29 @@ def run_timeline():
             a[1] += e0 - s0
         span = iv[-1][1] - iv[0][0]
         top = sorted(agg.items(), key=lambda kv: -kv[1][1])[:12]
-        out[label] = {
+        return {
             "device_events": len(iv), "span_ms": span / 1e3, "busy_ms": busy / 1e3,
             "idle_ms": float(gaps[gaps > 0].sum()) / 1e3, "gap_median_us": float(np.median(gaps)),
             "gaps_over_20us": int((gaps > 20).sum()),
             "top": [{"kernel": k[:160], "launches": v[0], "total_ms": round(v[1] / 1e3, 3),
                      "per_launch_us": round(v[1] / v[0], 1), "share": round(v[1] / busy, 4)} for k, v in top],
         }
+
+    for label, pc in (("mixed", "cheb_fp32"), ("fp64", "jacobi")):
+        g = IMEXStepper(m, DEGREE, sc.Ma, sc.Fr, 0.5, eps=1e-8, schur_preconditioner=pc)
+        g.set_state(d(st.rho), d(st.u), d(st.p))
+        g.step(1)
+        out[label] = trace(lambda: g.step(1))
         del g
         torch.cuda.synchronize()
+    g = IMEXStepper(m, DEGREE, sc.Ma, sc.Fr, 0.5, eps=1e-10, schur_preconditioner="cheb_fp32")
+    x = (d(st.rho), d(st.u), d(st.p))
+    g.step_forward(*x)
+    yb = tuple(torch.ones_like(v) for v in x)
+    g.step_backward(*yb, rel_tol=1e-10)
+    out["step_backward"] = trace(lambda: g.step_backward(*yb, rel_tol=1e-10))
+    del g
+    torch.cuda.synchronize()
     print(json.dumps(out))
 
 
