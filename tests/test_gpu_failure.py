@@ -98,3 +98,27 @@ def test_calls_that_synchronize_return_the_timeout_themselves():
     op.vmult(dst, p_f)
     op.synchronize()
     assert bool(torch.isfinite(dst).all())
+
+
+def test_imex_step_reports_the_timeout():
+    """A time step whose kernels give up their waits returns AF_TIMEOUT from af_imex_step (the
+    stepper synchronises inside its solves), and the next steps run normally."""
+    import ctypes
+    from atmospheric_flows_b200.imex import IMEXStepper, _bind
+    from atmospheric_flows_b200.operator import AFError, AF_TIMEOUT, lib
+    m = M.hill_mesh(8, 4, periodic_x=True)
+    sc = M.Scaling()
+    st = M.hill_state(m, P)
+    g = IMEXStepper(m, P, sc.Ma, sc.Fr, 2.0)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    g.set_state(d(st.rho), d(st.u), d(st.p))
+    op = ctypes.c_void_p(_bind().af_imex_operator(g._h))
+    assert lib().af_set_stage_wait_test(op, POLLS) == 0
+    with pytest.raises(AFError) as e:
+        g.step(1)
+    assert e.value.status == AF_TIMEOUT
+    assert lib().af_set_stage_wait_test(op, 0) == 0
+    g.set_state(d(st.rho), d(st.u), d(st.p))
+    g.step(2)
+    r, u, p = g.get_state()
+    assert bool(torch.isfinite(u).all())
