@@ -253,20 +253,24 @@ static int pressure_fixed_point(af_imex* h, int stage, int iter) {
   const long ns = h->ns;
   IM_AF(af_set_pres_fixed(o, h->pfix_old));
   IM_AF(af_set_u_fixed(o, h->ufix));
+  // rhs_u and tmp_1 = A^{-1} rhs_u depend only on the stage's explicit fields and on A (the
+  // stage's rho_for_fixed), not on pres_fixed or u_fixed: the reference forms them at every
+  // fixed-point iteration (Atmospheric_Flow.cc:558-571), here at the first iteration of a stage
+  // only (the same values; update_velocity leaves rhs_u as it is)
   if (stage == 1) {
     const double* sp[] = {h->rho0, h->u0, h->p0, h->rho2, h->ufix};
     IM_AF(af_vmult_rhs_pressure(o, h->rhs_p, sp, 5));
     const double* su[] = {h->rho0, h->u0, h->p0, h->rho2};
-    IM_AF(af_vmult_rhs_velocity_fixed(o, h->rhs_u, su, 4));
+    if (iter == 0) IM_AF(af_vmult_rhs_velocity_fixed(o, h->rhs_u, su, 4));
   } else {
     const double* sp[] = {h->rho0, h->u0, h->p0, h->rho2, h->u2, h->p2, h->rho3, h->ufix};
     IM_AF(af_vmult_rhs_pressure(o, h->rhs_p, sp, 8));
     const double* su[] = {h->rho0, h->u0, h->p0, h->rho2, h->u2, h->p2, h->rho3};
-    IM_AF(af_vmult_rhs_velocity_fixed(o, h->rhs_u, su, 7));
+    if (iter == 0) IM_AF(af_vmult_rhs_velocity_fixed(o, h->rhs_u, su, 7));
   }
   // tmp_1 = A^{-1} rhs_u, CG to 1e-12 |rhs_u| (Atmospheric_Flow.cc:571, 642); tmp_1 persists
   IM_AF(af_set_NS_stage(o, 3));
-  IM_AF(mass_solve(h, h->invd_u, h->tmp1, h->rhs_u, 2 * ns, 1e-12));
+  if (iter == 0) IM_AF(mass_solve(h, h->invd_u, h->tmp1, h->rhs_u, 2 * ns, 1e-12));
   IM_AF(af_vmult_enthalpy(o, h->tmpp, h->tmp1));
   IM_CU(axpby(-1.0, h->tmpp, 1.0, h->rhs_p, ns, o->stream));
   o->launches += 1;
@@ -291,21 +295,24 @@ static int pressure_fixed_point(af_imex* h, int stage, int iter) {
 static int update_velocity(af_imex* h, int stage) {
   af_operator* o = h->op;
   const long ns = h->ns;
-  double* x;
+  double *x, *b;
   if (stage < 3) {
+    // b = rhs_u - B p, in tmpu (rhs_u is kept for the next fixed-point iteration)
     IM_AF(af_set_NS_stage(o, 3));
     IM_AF(af_vmult_pressure(o, h->tmpu, h->pfix));
-    IM_CU(axpby(-1.0, h->tmpu, 1.0, h->rhs_u, 2 * ns, o->stream));
+    IM_CU(axpby(1.0, h->rhs_u, -1.0, h->tmpu, 2 * ns, o->stream));
     o->launches += 1;
     x = h->ufix;
+    b = h->tmpu;
   } else {
     IM_AF(af_set_NS_stage(o, 5));
     const double* su[] = {h->rho0, h->u0, h->p0, h->rho2, h->u2, h->p2, h->rho3, h->u3, h->p3};
     IM_AF(af_vmult_rhs_velocity_fixed(o, h->rhs_u, su, 9));
     x = h->uc;
+    b = h->rhs_u;
     IM_CU(cudaMemcpyAsync(x, h->u3, 2 * ns * 8, cudaMemcpyDeviceToDevice, o->stream));
   }
-  return mass_solve(h, h->invd_u, x, h->rhs_u, 2 * ns, h->opt.eps);
+  return mass_solve(h, h->invd_u, x, b, 2 * ns, h->opt.eps);
 }
 
 static int update_pressure(af_imex* h) {

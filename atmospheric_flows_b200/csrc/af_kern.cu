@@ -449,9 +449,11 @@ cudaError_t launch_mass_solve(const R* L, int ncomp, const R* b, R scale, R* x, 
 // kernel above (instruction-bound: about 11.5 k warp instructions per cell at p = 4):
 //   rows: M[i][j] = sum_qz S[qz][iz] S[qz][jz] T(qz)[ix][jx], T as above (full, not packed);
 //   in-place Gauss-Jordan without pivoting (M is symmetric positive definite): for each
-//   pivot k, row k is scaled by 1/M_kk and broadcast by warp shuffles, every other row r
-//   takes a_rj -= a_rk a_kj and a_rk = -a_rk / M_kk, leaving M^{-1} in the rows;
-//   the lower triangle is staged in shared memory and stored coalesced.
+//   pivot k, row k is scaled by 1/M_kk and broadcast through shared memory (one of two row
+//   buffers, so one warp barrier per pivot), every other row r takes a_rj -= a_rk a_kj and
+//   a_rk = -a_rk / M_kk, leaving M^{-1} in the rows; the lower triangle is staged in shared
+//   memory and stored coalesced.  (Broadcasting the row by warp shuffles instead, two per
+//   double and element, made the kernel shuffle-bound: 1.19 ms per launch at 131072 cells.)
 constexpr int kGJWarps = 4;
 template <int ND_ = kND>
 __global__ void __launch_bounds__(32 * kGJWarps)
@@ -464,6 +466,8 @@ __global__ void __launch_bounds__(32 * kGJWarps)
   __shared__ double sF[kGJWarps][NQ * NQ];
   __shared__ double sT[kGJWarps][NQ * P1 * P1];
   __shared__ double sO[kGJWarps][NPK];
+  constexpr int NDE = (ND + 1) / 2 * 2;  // a row padded to whole double2
+  __shared__ __align__(16) double sR[kGJWarps][2][NDE];
   const Tab<P>& tb = c_tab;
   for (int k = threadIdx.x; k < NQ * P1; k += blockDim.x) sS[k] = tb.S[k / P1][k % P1];
   __syncthreads();  // the only block-wide barrier; warps past the last cell leave after it
@@ -513,7 +517,7 @@ __global__ void __launch_bounds__(32 * kGJWarps)
   double siz[NQ];
 #pragma unroll
   for (int qz = 0; qz < NQ; ++qz) siz[qz] = sS[qz * P1 + rz];
-  double a[ND];
+  double a[NDE];
 #pragma unroll
   for (int jj = 0; jj < ND; ++jj) {
     const int jz = jj / P1, jx = jj % P1;
@@ -522,19 +526,28 @@ __global__ void __launch_bounds__(32 * kGJWarps)
     for (int qz = 0; qz < NQ; ++qz) s = fma(siz[qz] * tb.S[qz][jz], Tm[qz * P1 * P1 + rx * P1 + jx], s);
     a[jj] = s;
   }
+  if (NDE > ND) a[NDE - 1] = 0.0;
   // Gauss-Jordan in place
 #pragma unroll
   for (int k = 0; k < ND; ++k) {
-    const double piv = 1.0 / __shfl_sync(0xffffffffu, a[k], k);
+    double2* row = reinterpret_cast<double2*>(sR[warp][k & 1]);
     if (lane == k) {
+      const double piv = 1.0 / a[k];
 #pragma unroll
       for (int jj = 0; jj < ND; ++jj) a[jj] = jj == k ? piv : a[jj] * piv;
-    }
-    const double f = a[k];
 #pragma unroll
-    for (int jj = 0; jj < ND; ++jj) {
-      const double rkj = __shfl_sync(0xffffffffu, a[jj], k);
-      if (lane != k) a[jj] = jj == k ? -f * rkj : fma(-f, rkj, a[jj]);
+      for (int jj = 0; jj < NDE / 2; ++jj) row[jj] = make_double2(a[2 * jj], a[2 * jj + 1]);
+    }
+    // the other buffer was last read before the previous pivot's barrier
+    __syncwarp();
+    const double f = a[k];
+    if (lane != k) {
+#pragma unroll
+      for (int jj = 0; jj < NDE / 2; ++jj) {
+        const double2 rk = row[jj];
+        a[2 * jj] = 2 * jj == k ? -f * rk.x : fma(-f, rk.x, a[2 * jj]);
+        if (2 * jj + 1 < ND) a[2 * jj + 1] = 2 * jj + 1 == k ? -f * rk.y : fma(-f, rk.y, a[2 * jj + 1]);
+      }
     }
   }
   // lower triangle of row r, packed row-major, then coalesced

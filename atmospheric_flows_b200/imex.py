@@ -76,12 +76,13 @@ class IMEXStepper:
         h = ctypes.c_void_p()
         check(L.af_imex_create(ctypes.byref(desc), degree, Ma, Fr, dt, ctypes.byref(opt), ctypes.byref(h)))
         self._h = h
+        self._destroy = L.af_imex_destroy  # kept: module globals may be gone when __del__ runs at exit
         self.n_scalar = mesh.n_cells * (degree + 1) ** 2
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            _bind().af_imex_destroy(h)
+            self._destroy(h)
             self._h = None
 
     def set_state(self, rho, u, p):

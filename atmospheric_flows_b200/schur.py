@@ -67,13 +67,14 @@ class SchurSolver:
         h = ctypes.c_void_p()
         check(L.af_schur_solver_create(op._h, ctypes.byref(opt), ctypes.byref(h)))
         self._h = h
+        self._destroy = L.af_schur_solver_destroy  # kept: module globals may be gone at exit
         self.op = op  # keeps the operator alive
         self.options = opt
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().af_schur_solver_destroy(h)
+            self._destroy(h)
             self._h = None
 
     def setup(self, estimate_eigenvalues=False):
