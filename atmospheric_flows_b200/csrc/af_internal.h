@@ -129,6 +129,22 @@ struct DegreeOps {
   cudaError_t (*res_chebz_f)(const MeshDev&, const float* w, const float* pf, const float* din,
                              const CParamsT<float>&, const float* WM, float g, float alpha, float s, float* z,
                              float* dout, float* x, int first, int reduced, int ncell, cudaStream_t);
+  // ---- the same smoother in the Gauss-point basis (af_gauss.cuh): vectors hold values at the
+  // (P+1)^2 Gauss points, face traces tr[face][comp][cell][P+1] go with them
+  //   entry: d = x = sc WM (Vi x Vi)^T v (v FP64 nodal), z = theta d, dtr = traces of d
+  cudaError_t (*gs_entry)(const double* v, const float* WM, float sc, float theta, float* z, float* d, float* x,
+                          float* dtr, int ncell, cudaStream_t);
+  //   w = scale diag(WA) B_g d (two components) and its traces
+  cudaError_t (*gs_binv)(const MeshDev&, const float* d, const float* dtr, float c, const float* WA, float scale,
+                         float* w, float* wtr, int ncell, cudaStream_t);
+  //   z += g WM C0_g(w; pg) - d;  d = alpha d + s z (in place);  x += d;  dtr = traces of d
+  cudaError_t (*gs_zstep)(const MeshDev&, const float* w, const float* wtr, const float* pg, const float* ptr,
+                          float cdt, float gg, const float* WM, float g, float alpha, float s, float* z, float* d,
+                          float* x, float* dtr, int ncell, cudaStream_t);
+  //   out = (Vi x Vi) x (FP64 nodal)
+  cudaError_t (*gs_exit)(const float* x, double* out, int ncell, cudaStream_t);
+  //   a coefficient at the Gauss points and its traces: pg = (V x V) p
+  cudaError_t (*gs_values)(const double* p, float* pg, float* ptr, int ncell, cudaStream_t);
 };
 
 const DegreeOps* degree_ops(int P);  // null if the degree was not compiled

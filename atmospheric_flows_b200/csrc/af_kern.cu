@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "af_adjoint.cuh"
+#include "af_gauss.cuh"
 #include "af_internal.h"
 
 #ifndef AF_P
@@ -447,13 +448,19 @@ cudaError_t launch_mass_solve(const R* L, int ncomp, const R* b, R scale, R* x, 
 // Degrees <= 4 ((P+1)^2 <= 32 rows): the same cell matrix and its inverse with lane i owning
 // row i in registers, which removes the shared-memory traffic and index decoding of the
 // kernel above (instruction-bound: about 11.5 k warp instructions per cell at p = 4):
-//   rows: M[i][j] = sum_qz S[qz][iz] S[qz][jz] T(qz)[ix][jx], T as above (full, not packed);
-//   in-place Gauss-Jordan without pivoting (M is symmetric positive definite): for each
-//   pivot k, row k is scaled by 1/M_kk and broadcast through shared memory (one of two row
-//   buffers, so one warp barrier per pivot), every other row r takes a_rj -= a_rk a_kj and
-//   a_rk = -a_rk / M_kk, leaving M^{-1} in the rows; the lower triangle is staged in shared
-//   memory and stored coalesced.  (Broadcasting the row by warp shuffles instead, two per
-//   double and element, made the kernel shuffle-bound: 1.19 ms per launch at 131072 cells.)
+//   rows: M[i][j] = sum_qz S[qz][iz] S[qz][jz] T(qz)[ix][jx], T as above (full, not packed),
+//   as sum_qz S[qz][jz] U[qz][jx] with U[qz][jx] = S[qz][iz] T(qz)[ix][jx] formed first;
+//   the inverse by the symmetric sweep operator (M is symmetric positive definite, no
+//   pivoting): sweeping pivot k maps a_kk -> -1/a_kk, a_rk = a_kr -> a_rk/a_kk and, for
+//   r, j != k, a_rj -> a_rj - (a_rk/a_kk) a_kj; it keeps the matrix symmetric, and sweeping
+//   every pivot leaves -M^{-1}.  By symmetry the pivot row is the column k of the lanes'
+//   registers: each lane stores its a_rk (one shared-memory store for the warp) and reads
+//   the row back as broadcasts, every row but k updates itself, and row k takes the new
+//   column k (the a_rk/a_kk of the other lanes) through shared memory.  (Gauss-Jordan with
+//   the pivot lane scaling its row alone, 24 multiplies with one lane active per pivot, and
+//   the row broadcast by warp shuffles took 1.19 ms per launch at 131072 cells; with the row
+//   broadcast through shared memory 1.0 ms.)  The lower triangle is staged in shared memory
+//   and stored coalesced.
 constexpr int kGJWarps = 4;
 template <int ND_ = kND>
 __global__ void __launch_bounds__(32 * kGJWarps)
@@ -467,7 +474,9 @@ __global__ void __launch_bounds__(32 * kGJWarps)
   __shared__ double sT[kGJWarps][NQ * P1 * P1];
   __shared__ double sO[kGJWarps][NPK];
   constexpr int NDE = (ND + 1) / 2 * 2;  // a row padded to whole double2
-  __shared__ __align__(16) double sR[kGJWarps][2][NDE];
+  // per warp: the pivot row (column k) and the new column k, one slot per lane
+  __shared__ __align__(16) double sR[kGJWarps][32];
+  __shared__ __align__(16) double sG[kGJWarps][32];
   const Tab<P>& tb = c_tab;
   for (int k = threadIdx.x; k < NQ * P1; k += blockDim.x) sS[k] = tb.S[k / P1][k % P1];
   __syncthreads();  // the only block-wide barrier; warps past the last cell leave after it
@@ -514,42 +523,54 @@ __global__ void __launch_bounds__(32 * kGJWarps)
   __syncwarp();
   // row r = lane of the cell matrix (lanes >= ND duplicate the last row and store nothing)
   const int r = lane < ND ? lane : ND - 1, rz = r / P1, rx = r % P1;
-  double siz[NQ];
-#pragma unroll
-  for (int qz = 0; qz < NQ; ++qz) siz[qz] = sS[qz * P1 + rz];
+  // U[qz][jx] = S[qz][rz] T(qz)[rx][jx], then a[jz P1 + jx] = sum_qz S[qz][jz] U[qz][jx]
+  // (qz outermost: one U row live at a time)
   double a[NDE];
 #pragma unroll
-  for (int jj = 0; jj < ND; ++jj) {
-    const int jz = jj / P1, jx = jj % P1;
-    double s = 0.0;
+  for (int jj = 0; jj < NDE; ++jj) a[jj] = 0.0;
 #pragma unroll
-    for (int qz = 0; qz < NQ; ++qz) s = fma(siz[qz] * tb.S[qz][jz], Tm[qz * P1 * P1 + rx * P1 + jx], s);
-    a[jj] = s;
+  for (int qz = 0; qz < NQ; ++qz) {
+    const double sz = sS[qz * P1 + rz];
+    double u[P1];
+#pragma unroll
+    for (int jx = 0; jx < P1; ++jx) u[jx] = sz * Tm[qz * P1 * P1 + rx * P1 + jx];
+#pragma unroll
+    for (int jj = 0; jj < ND; ++jj) a[jj] = fma(tb.S[qz][jj / P1], u[jj % P1], a[jj]);
   }
-  if (NDE > ND) a[NDE - 1] = 0.0;
-  // Gauss-Jordan in place
+  // sweep every pivot; rows r = lane (lanes >= ND repeat the last row and are not stored)
 #pragma unroll
   for (int k = 0; k < ND; ++k) {
-    double2* row = reinterpret_cast<double2*>(sR[warp][k & 1]);
-    if (lane == k) {
-      const double piv = 1.0 / a[k];
-#pragma unroll
-      for (int jj = 0; jj < ND; ++jj) a[jj] = jj == k ? piv : a[jj] * piv;
-#pragma unroll
-      for (int jj = 0; jj < NDE / 2; ++jj) row[jj] = make_double2(a[2 * jj], a[2 * jj + 1]);
-    }
-    // the other buffer was last read before the previous pivot's barrier
+    // (the previous pivot's barriers order its reads of R and G before these writes)
+    double* R = sR[warp];
+    double* G = sG[warp];
+    R[lane] = a[k];  // a_rk = a_kr: the pivot row, one element per lane
     __syncwarp();
-    const double f = a[k];
+    const double id = 1.0 / R[k];
+    const double g = a[k] * id;  // the new a_rk
     if (lane != k) {
 #pragma unroll
       for (int jj = 0; jj < NDE / 2; ++jj) {
-        const double2 rk = row[jj];
-        a[2 * jj] = 2 * jj == k ? -f * rk.x : fma(-f, rk.x, a[2 * jj]);
-        if (2 * jj + 1 < ND) a[2 * jj + 1] = 2 * jj + 1 == k ? -f * rk.y : fma(-f, rk.y, a[2 * jj + 1]);
+        const double2 v = reinterpret_cast<const double2*>(R)[jj];
+        if (2 * jj != k) a[2 * jj] = fma(-g, v.x, a[2 * jj]);
+        if (2 * jj + 1 != k && 2 * jj + 1 < ND) a[2 * jj + 1] = fma(-g, v.y, a[2 * jj + 1]);
       }
+      a[k] = g;
+    }
+    G[lane] = g;
+    __syncwarp();
+    if (lane == k) {  // row k = the new column k
+#pragma unroll
+      for (int jj = 0; jj < NDE / 2; ++jj) {
+        const double2 v = reinterpret_cast<const double2*>(G)[jj];
+        a[2 * jj] = v.x;
+        a[2 * jj + 1] = v.y;
+      }
+      a[k] = -id;
+      if (NDE > ND) a[NDE - 1] = 0.0;
     }
   }
+#pragma unroll
+  for (int jj = 0; jj < ND; ++jj) a[jj] = -a[jj];  // the sweeps leave -M^{-1}
   // lower triangle of row r, packed row-major, then coalesced
 #pragma unroll
   for (int jj = 0; jj < ND; ++jj)
@@ -1038,6 +1059,46 @@ cudaError_t res_chebz_f(const MeshDev& mesh, const float* w, const float* pf, co
                                                          ncell, st);
 }
 
+// ------------------------------------------------------------------ Gauss-point smoother
+template <class K, class... A>
+cudaError_t launch_gs(K kernel, int ncell, cudaStream_t st, bool pdl, A... args) {
+  using S = GsShape<P>;
+  const int nblk = (ncell + S::CB - 1) / S::CB;
+  if (ncell <= 0) return cudaSuccess;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)nblk);
+  cfg.blockDim = dim3((unsigned)S::NT);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = (kPDL && pdl) ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+cudaError_t gs_entry(const double* v, const float* WM, float sc, float theta, float* z, float* d, float* x,
+                     float* dtr, int ncell, cudaStream_t st) {
+  return launch_gs(k_gs_entry<P>, ncell, st, true, v, WM, sc, theta, z, d, x, dtr, ncell);
+}
+cudaError_t gs_binv(const MeshDev& mesh, const float* d, const float* dtr, float c, const float* WA, float scale,
+                    float* w, float* wtr, int ncell, cudaStream_t st) {
+  if (mesh.cell0 != 0) return cudaErrorInvalidValue;
+  return launch_gs(k_gs_binv<P>, ncell, st, true, mesh, d, dtr, c, WA, scale, w, wtr, ncell);
+}
+cudaError_t gs_zstep(const MeshDev& mesh, const float* w, const float* wtr, const float* pg, const float* ptr,
+                     float cdt, float gg, const float* WM, float g, float alpha, float s, float* z, float* d,
+                     float* x, float* dtr, int ncell, cudaStream_t st) {
+  if (mesh.cell0 != 0) return cudaErrorInvalidValue;
+  return launch_gs(k_gs_zstep<P>, ncell, st, true, mesh, w, wtr, pg, ptr, cdt, gg, WM, g, alpha, s, z, d, x, 0, dtr,
+                   ncell);
+}
+cudaError_t gs_exit(const float* x, double* out, int ncell, cudaStream_t st) {
+  return launch_gs(k_gs_exit<P>, ncell, st, true, x, out, ncell);
+}
+cudaError_t gs_values(const double* p, float* pg, float* ptr, int ncell, cudaStream_t st) {
+  return launch_gs(k_gs_values<P>, ncell, st, false, p, pg, ptr, ncell);
+}
+
 cudaError_t op_A_rho_T(const MeshDev& mesh, const double* x, const double* y, double* rhobar, int ncell,
                        cudaStream_t st) {
   ArgPtrs<2, 1> a{{x, y}, {rhobar}};
@@ -1088,7 +1149,9 @@ const DegreeOps kOps = {upload_tables,     rhs,
                         b_inv_fr,          res_cheb_fr,
                         op_A_rho_T,        op_C_pf_T,
                         rhs_tangent,       rhs_adjoint,
-                        res_chebz_f};
+                        res_chebz_f,       gs_entry,
+                        gs_binv,           gs_zstep,
+                        gs_exit,           gs_values};
 
 }  // namespace
 

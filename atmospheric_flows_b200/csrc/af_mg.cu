@@ -161,6 +161,9 @@ struct Level {
   void* LA = nullptr;
   void* LM = nullptr;
   void *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *u = nullptr, *w = nullptr;
+  // the Gauss-point smoother (af_gauss.cuh): face traces of d and w, p_fixed at the Gauss
+  // points and its traces
+  float *gdtr = nullptr, *gwtr = nullptr, *gpg = nullptr, *gptr = nullptr;
   double lmax = 0.0;
 };
 
@@ -173,6 +176,7 @@ struct af_schur_solver {
   int nact = 0;                 // levels in use (the coarsest has lmax <= coarse_lmax)
   bool fp32 = false;
   bool rq = false;              // FP32 levels with the reduced quadrature (P+1 Gauss points)
+  bool gauss = false;           // the single-level FP32 Chebyshev in the Gauss-point basis
   bool setup_done = false, eig_done = false;
   double cB = 0, cdt = 0;       // B and C coefficients of the last setup
   double* part = nullptr;       // reductions
@@ -420,6 +424,7 @@ int setup_levels(af_schur_solver* s, bool estimate) {
       o->launches += 2;
     }
     k_convert<double, R><<<nblocks(L.ns), kThreads, 0, o->stream>>>(L.pf, (R*)L.pfR, L.ns);
+    if (s->gauss) MG_CU(k->gs_values(L.pf, L.gpg, L.gptr, L.ncell, o->stream));
     if (sizeof(R) == sizeof(float)) {  // Gauss-point inverse weights of A
       MG_CU(k->cob_weights_f(L.mesh, L.rho, (float*)L.LA, L.ncell, o->stream));
     } else if (l == 0) {  // the operator's own inverse of A (built once per rho_for_fixed)
@@ -459,6 +464,40 @@ int build_mass_inverses(af_schur_solver* s) {
   return AF_OK;
 }
 
+// z = the single-level FP32 Chebyshev polynomial in the Gauss-point basis applied to v (FP64 in
+// and out): the iteration of chebyshev() on z = D^{-1} r (zero start, no final residual), with
+// the basis changed at entry and exit (af_gauss.cuh)
+int apply_gauss(af_schur_solver* s, double* z, const double* v) {
+  af_operator* o = s->op;
+  const DegreeOps* k = o->ops;
+  Level& L = s->lv[0];
+  const double hi = 1.2 * L.lmax, lo = std::fmin(0.9, hi / s->opt.smoothing_range);
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  const double ginv = 1.0 / kG1;  // D^{-1} = (gamma-1) M^{-1}
+  float* zg = (float*)L.r;
+  float* d = (float*)L.d;
+  float* x = (float*)L.x;
+  const float* WM = (const float*)L.LM;
+  // d = x = D^{-1} v / theta;  z = D^{-1} v = theta d
+  MG_CU(k->gs_entry(v, WM, (float)(ginv / theta), (float)theta, zg, d, x, L.gdtr, L.ncell, o->stream));
+  o->launches += 1;
+  double rho_old = 1.0 / sigma;
+  for (int it = 1; it < s->opt.coarse_degree; ++it) {
+    const double rho = 1.0 / (2.0 * sigma - rho_old);
+    const double a = rho * rho_old, sc = 2.0 * rho / delta;
+    // w = A^{-1} B d;  z += D^{-1} C0 w - d;  d = a d + sc z;  x += d  (two launches)
+    MG_CU(k->gs_binv(L.mesh, d, L.gdtr, (float)s->cB, (const float*)L.LA, 1.0f, (float*)L.w, L.gwtr, L.ncell,
+                     o->stream));
+    MG_CU(k->gs_zstep(L.mesh, (const float*)L.w, L.gwtr, L.gpg, L.gptr, (float)s->cdt, (float)kGG, WM, (float)ginv,
+                      (float)a, (float)sc, zg, d, x, L.gdtr, L.ncell, o->stream));
+    o->launches += 2;
+    rho_old = rho;
+  }
+  MG_CU(k->gs_exit(x, z, L.ncell, o->stream));
+  o->launches += 1;
+  return AF_OK;
+}
+
 // z = V-cycle(v): FP64 in and out, level precision inside
 template <class R>
 int apply_vcycle(af_schur_solver* s, double* z, const double* v) {
@@ -483,6 +522,7 @@ int precondition(af_schur_solver* s, double* z, const double* v) {
     o->launches += 1;
     return AF_OK;
   }
+  if (s->gauss) return apply_gauss(s, z, v);
   return s->fp32 ? apply_vcycle<float>(s, z, v) : apply_vcycle<double>(s, z, v);
 }
 
@@ -502,7 +542,7 @@ int af_schur_default_options(af_schur_options* opt) {
   opt->min_coarse_cells = 16;
   opt->eig_iterations = 20;
   opt->restart = 30;
-  opt->reduced_quadrature = 1;
+  opt->reduced_quadrature = 2;
   return AF_OK;
 }
 
@@ -516,7 +556,7 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
     return merr(AF_BAD_ARG, "af_schur_solver_create: unknown preconditioner");
   if (o.smoother_degree < 1 || o.coarse_degree < 1 || o.smoothing_range <= 1.0 || o.eig_iterations < 1 ||
       o.restart < 1 || o.restart > 64 || !(o.coarse_lmax >= 0.0) || o.poly_degree < 1 || o.reduced_quadrature < 0 ||
-      o.reduced_quadrature > 1)
+      o.reduced_quadrature > 2)
     return merr(AF_BAD_ARG, "af_schur_solver_create: invalid options");
   if (o.preconditioner == AF_SCHUR_CHEB_FP64 || o.preconditioner == AF_SCHUR_CHEB_FP32) {
     // single level: the "coarse solve" on the operator's own mesh is the polynomial
@@ -529,6 +569,7 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
   s->opt = o;
   s->fp32 = o.preconditioner == AF_SCHUR_MG_FP32 || o.preconditioner == AF_SCHUR_CHEB_FP32;
   s->rq = s->fp32 && o.reduced_quadrature != 0;
+  s->gauss = o.preconditioner == AF_SCHUR_CHEB_FP32 && o.reduced_quadrature == 2;
   const size_t rs = s->fp32 ? sizeof(float) : sizeof(double);
   const long ns0 = op->n_scalar();
   auto cleanup = [&](int code) {
@@ -587,6 +628,13 @@ int af_schur_solver_create(af_operator* op, const af_schur_options* opt, af_schu
       if ((r = alloc(s, p, rs * L.ns)) != AF_OK) return cleanup(r);
     for (void** p : {&L.u, &L.w})
       if ((r = alloc(s, p, rs * 2 * L.ns)) != AF_OK) return cleanup(r);
+    if (s->gauss) {
+      const size_t nt = sizeof(float) * 4 * (size_t)L.ncell * (op->P + 1);
+      if ((r = alloc(s, (void**)&L.gdtr, nt)) != AF_OK) return cleanup(r);
+      if ((r = alloc(s, (void**)&L.gwtr, 2 * nt)) != AF_OK) return cleanup(r);
+      if ((r = alloc(s, (void**)&L.gptr, nt)) != AF_OK) return cleanup(r);
+      if ((r = alloc(s, (void**)&L.gpg, sizeof(float) * L.ns)) != AF_OK) return cleanup(r);
+    }
   }
   s->nact = (int)s->lv.size();
   r = s->fp32 ? build_mass_inverses<float>(s) : build_mass_inverses<double>(s);

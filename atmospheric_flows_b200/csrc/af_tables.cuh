@@ -66,6 +66,10 @@ struct CobT {
   R Vi[P + 1][P + 1];  // Vi[i][q] = (V^{-1})[i][q]
   R V[P + 1][P + 1];   // V[q][i] = l_i(g_q)
   R g[P + 1], w[P + 1];  // Gauss points and weights on [0, 1]
+  // the Lagrange basis L_i of the Gauss points (the collocated basis of the Gauss-point
+  // smoother): Dg[q][i] = L_i'(g_q), lo[i] = L_i(0), hi[i] = L_i(1)
+  R Dg[P + 1][P + 1];
+  R lo[P + 1], hi[P + 1];
 };
 
 namespace host {
@@ -208,6 +212,11 @@ inline CobT<P, R> make_cob() {
   for (int q = 0; q < P1; ++q) {
     t.g[q] = (R)x[q];
     t.w[q] = (R)w[q];
+  }
+  for (int i = 0; i < P1; ++i) {
+    for (int q = 0; q < P1; ++q) t.Dg[q][i] = (R)dlag(x, i, x[q]);
+    t.lo[i] = (R)lag(x, i, 0);
+    t.hi[i] = (R)lag(x, i, 1);
   }
   return t;
 }

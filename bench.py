@@ -752,7 +752,7 @@ def run_timeline():
             a[0] += 1
             a[1] += e0 - s0
         span = iv[-1][1] - iv[0][0]
-        top = sorted(agg.items(), key=lambda kv: -kv[1][1])[:12]
+        top = sorted(agg.items(), key=lambda kv: -kv[1][1])[:16]
         return {
             "device_events": len(iv), "span_ms": span / 1e3, "busy_ms": busy / 1e3,
             "idle_ms": float(gaps[gaps > 0].sum()) / 1e3, "gap_median_us": float(np.median(gaps)),

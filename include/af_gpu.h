@@ -198,7 +198,11 @@ typedef struct {
   int poly_degree;          /* degree of the AF_SCHUR_CHEB_* polynomial preconditioner (16)    */
   int reduced_quadrature;   /* FP32 levels: B, C0 with P+1 Gauss points per direction instead  */
                             /* of 2P+1 (exact for B and D on bilinear cells, approximate for   */
-                            /* C0 and A; the outer FGMRES keeps the exact operator) (1)        */
+                            /* C0 and A; the outer FGMRES keeps the exact operator): 1; 2: the */
+                            /* same, and AF_SCHUR_CHEB_FP32 iterates in the basis of the       */
+                            /* Lagrange polynomials of those Gauss points, where the cell      */
+                            /* inverses are diagonal (the same polynomial; multigrid levels    */
+                            /* stay nodal); 0: 2P+1 points (2)                                 */
 } af_schur_options;
 typedef struct {
   int iterations;           /* FGMRES iterations of the last solve                             */

@@ -154,9 +154,10 @@ def test_schur_solve_all_preconditioners():
     o.set_NS_stage(2)
     its = {}
     cases = {"jacobi": {}, "mg_fp64": {}, "mg_fp32": {}, "cheb_fp64": {}, "cheb_fp32": {},
-             "cheb_fp32_full_quadrature": {"reduced_quadrature": 0}}
+             "cheb_fp32_full_quadrature": {"reduced_quadrature": 0},
+             "cheb_fp32_nodal": {"reduced_quadrature": 1}}
     for pc, kw in cases.items():
-        s = SchurSolver(op, pc.replace("_full_quadrature", ""), **kw)
+        s = SchurSolver(op, pc.replace("_full_quadrature", "").replace("_nodal", ""), **kw)
         s.setup()
         x = torch.zeros_like(b)
         out = s.solve(x, b, rel_tol=1e-10, max_iterations=5000)
@@ -167,8 +168,10 @@ def test_schur_solve_all_preconditioners():
         assert rel(xh, xt) < 1e-8, pc
         assert rel(o.vmult(xh), bh) < 1e-9, pc
     # the multigrid and polynomial preconditioners take far fewer iterations than Jacobi
-    for pc in ("mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32", "cheb_fp32_full_quadrature"):
+    for pc in ("mg_fp64", "mg_fp32", "cheb_fp64", "cheb_fp32", "cheb_fp32_full_quadrature", "cheb_fp32_nodal"):
         assert its[pc] * 2 < its["jacobi"], its
+    # the Gauss-point smoother (the default) is the nodal reduced-quadrature one in another basis
+    assert abs(its["cheb_fp32"] - its["cheb_fp32_nodal"]) <= 1, its
 
 
 def test_reduced_quadrature_preconditioner_is_exact_on_affine_cells():
@@ -244,3 +247,39 @@ def test_fp32_chebyshev_on_the_preconditioned_residual_matches_fp64(P):
         errs[degree] = rel(z["cheb_fp32"].cpu().numpy(), z["cheb_fp64"].cpu().numpy())
         assert errs[degree] < tol, errs
     print("fp32 z-form vs fp64 r-form, relative difference by degree:", errs)
+
+
+@pytest.mark.parametrize("P,periodic", [(1, False), (2, True), (3, False), (4, False), (4, True), (5, True), (6, False)])
+def test_gauss_point_smoother_matches_the_nodal_one(P, periodic):
+    """reduced_quadrature = 2 runs the FP32 Chebyshev polynomial in the basis of the Lagrange
+    polynomials of the P+1 Gauss points, where the cell inverses of A and D are diagonal; it is
+    the same polynomial in D^{-1} S0 as the nodal reduced-quadrature smoother
+    (reduced_quadrature = 1), so the two preconditioner outputs agree to FP32 rounding amplified
+    by the recurrence (degree 2: one step; degree 16).  Hill state coefficients, walled and
+    x-periodic meshes, every compiled degree."""
+    from atmospheric_flows_b200.operator import EULEROperator
+    from atmospheric_flows_b200.schur import SchurSolver
+    dt = 2.0
+    sc = M.Scaling()
+    m = M.hill_mesh(16, 8, periodic_x=periodic)
+    n = m.n_cells * (P + 1) ** 2
+    op = EULEROperator(m, P, sc.Ma, sc.Fr, dt)
+    op.set_stream(torch.cuda.current_stream())
+    op.set_HYPERBOLIC_stage(1)
+    st = M.hill_state(m, P, modes=4)
+    op.set_rho_for_fixed(torch.from_numpy(st.rho).cuda())
+    op.set_pres_fixed(torch.from_numpy(st.p).cuda())
+    op.set_NS_stage(2)
+    b = torch.from_numpy(np.random.default_rng(11).standard_normal(n)).cuda()
+    errs = {}
+    for degree, tol in ((2, 2e-5), (16, 1e-3)):
+        z = {}
+        for rq in (1, 2):
+            s = SchurSolver(op, "cheb_fp32", poly_degree=degree, reduced_quadrature=rq)
+            s.setup()
+            z[rq] = torch.zeros(n, dtype=torch.float64, device="cuda")
+            s.precondition(z[rq], b)
+        torch.cuda.synchronize()
+        errs[degree] = rel(z[2].cpu().numpy(), z[1].cpu().numpy())
+        assert errs[degree] < tol, errs
+    print(f"P={P} periodic={periodic}: Gauss-point vs nodal smoother, relative difference by degree:", errs)
