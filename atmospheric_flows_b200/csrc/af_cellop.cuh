@@ -380,12 +380,19 @@ struct Layout {
   // chunk sizes are multiples of 16 bytes (CB even).  Without padding an even ND puts the same
   // node of consecutive cells on few banks: at degree 3 (ND 16, every cell on the same bank)
   // bulk staging measured 414 us against 245 us with the padded per-element copies, at degree 5
-  // (ND 36 doubles, a 4-way conflict) 748 us against 836 us; so even ND stages in bulk only at
-  // degree 5 in FP64.
+  // (ND 36 doubles, a 4-way conflict) 748 us against 836 us, and 707 us with the padded slots
+  // below; so even ND stages in bulk only at degree 5 in FP64.
   static constexpr bool BULK =
       kBulkStaging && (CB % 2 == 0) && ((ND % 2 == 1) || (P == 5 && sizeof(R) == 8));
+  // Padded bulk layout (even ND, i.e. degree 5 in FP64): each cell's chunk of an array arrives
+  // by its own bulk copy into a slot 16 bytes longer than the chunk (38 doubles for a scalar
+  // field, 74 for a velocity), so that the same node of the CTA's 8 cells lies on 8 different
+  // bank pairs instead of 4 (36 doubles = 8 banks apart).  The copies are spread over warp 0.
+  static constexpr int PADB = (BULK && ND % 2 == 0) ? ALIGN : 0;
+  static constexpr int slot(int nc) { return nc * ND + PADB; }  // one cell of an array
+  static constexpr int ISSUE_LANES = PADB ? 32 : 1;             // threads that issue the copies
   // region B: one group's nodal values and neighbour face nodes, later the outputs
-  static constexpr int R_IN = NF * CB * NDP;
+  static constexpr int R_IN = NF * CB * (NDP > ND + PADB ? NDP : ND + PADB);
   static constexpr int R_NB = Phys::FACES ? 4 * NF * CB * P1P : 0;
   static constexpr int R_OUT = NOUT * CB * NDP;
   static constexpr int RB = (R_IN + R_NB) > R_OUT ? (R_IN + R_NB) : R_OUT;
@@ -551,28 +558,57 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   // own cells of a group: the contiguous chunk of each array, by one bulk copy per array (TMA)
   // when the layout allows (uniform per CTA), otherwise by coalesced per-element copies
   const bool bulk = L::BULK && ((size_t)ncb * ND * sizeof(R)) % 16 == 0;
-  // issued by thread 0: group G's chunks into input buffer G % 2 (buffer 0 without prefetch)
+  // issued by warp 0 (lane 0 alone without padding): group G's chunks into input buffer G % 2
+  // (buffer 0 without prefetch)
   auto issue_group = [&](auto gc) {
     constexpr int G = decltype(gc)::value;
     using Gi = GroupInfo<Phys, G>;
     using Gr = typename Phys::template Grp<G>;
     R* buf = (L::PREFETCH && (G & 1)) ? s_in2 : s_in0;
     const unsigned gbar = (L::PREFETCH && (G & 1)) ? bar2 : bar;
-    unsigned bytes = 0;
-    sfor<Gi::NARR>([&](auto ac) { bytes += (unsigned)(ncb * Gr::ncomp(decltype(ac)::value) * ND * sizeof(R)); });
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(gbar), "r"(bytes) : "memory");
-    sfor<Gi::NARR>([&](auto ac) {
-      constexpr int A = decltype(ac)::value;
-      constexpr int NC = Gr::ncomp(A);
-      constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
-      const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
-      const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + fb * CB * ND);
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-          "l"(src), "r"((unsigned)(ncb * NC * ND * sizeof(R))), "r"(gbar)
-          : "memory");
-    });
+    const int lane = threadIdx.x;
+    if (lane == 0) {
+      unsigned bytes = 0;
+      sfor<Gi::NARR>([&](auto ac) { bytes += (unsigned)(ncb * Gr::ncomp(decltype(ac)::value) * ND * sizeof(R)); });
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(gbar), "r"(bytes) : "memory");
+    }
+    if constexpr (L::PADB == 0) {
+      if (lane == 0) {
+        sfor<Gi::NARR>([&](auto ac) {
+          constexpr int A = decltype(ac)::value;
+          constexpr int NC = Gr::ncomp(A);
+          constexpr int fb = [] { int b = 0; for (int a = 0; a < A; ++a) b += Gr::ncomp(a); return b; }();
+          const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + fb * CB * ND);
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                  dst),
+              "l"(src), "r"((unsigned)(ncb * NC * ND * sizeof(R))), "r"(gbar)
+              : "memory");
+        });
+      }
+    } else {
+      // one copy per (array, cell), spread over the lanes of warp 0; every chunk and slot is a
+      // multiple of 16 bytes (ND * 8 = 288 bytes, slots of 304 and 592), so both addresses stay
+      // 16-byte aligned
+      __syncwarp();
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      sfor<Gi::NARR>([&](auto ac) {
+        constexpr int A = decltype(ac)::value;
+        constexpr int NC = Gr::ncomp(A);
+        constexpr int ab = [] { int b = 0; for (int a = 0; a < A; ++a) b += CB * L::slot(Gr::ncomp(a)); return b; }();
+        const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
+        for (int cc = lane; cc < ncb; cc += 32) {
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + ab + cc * L::slot(NC));
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                  dst),
+              "l"(src + (size_t)cc * NC * ND), "r"((unsigned)(NC * ND * sizeof(R))), "r"(gbar)
+              : "memory");
+        }
+      });
+    }
   };
   // neighbours' face nodes of a face group (L2-resident), ordered along the face parameter, by
   // per-element asynchronous copies; one element per thread for each (face, field):
@@ -616,12 +652,13 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
     if constexpr (!L::BULK) {
       return (fi * CB + cl_) * L::NDP;
     } else {
-      int off = 0, fb = 0;
+      int off = 0, fb = 0, ab = 0;
 #pragma unroll
       for (int a = 0; a < Gi::NARR; ++a) {
         const int nc = Gr::ncomp(a);
-        if (fi >= fb && fi < fb + nc) off = fb * CB * ND + cl_ * nc * ND + (fi - fb) * ND;
+        if (fi >= fb && fi < fb + nc) off = ab + cl_ * L::slot(nc) + (fi - fb) * ND;
         fb += nc;
+        ab += CB * L::slot(nc);
       }
       return off;
     }
@@ -704,7 +741,7 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
   // and the epilogue's chunks
   auto issue_inputs = [&]() {
     if constexpr (L::BULK) {
-      if (threadIdx.x == 0 && bulk) issue_group(std::integral_constant<int, 0>{});
+      if (threadIdx.x < L::ISSUE_LANES && bulk) issue_group(std::integral_constant<int, 0>{});
     }
     if constexpr (L::EPI != 0) {
       if (epi_bulk) {
@@ -801,11 +838,11 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
       // now (group G-1 has finished reading it), otherwise group G is issued here
       if constexpr (L::PREFETCH) {
         if constexpr (G + 1 < Phys::NG) {
-          if (tid == 0) issue_group(std::integral_constant<int, G + 1>{});
+          if (tid < L::ISSUE_LANES) issue_group(std::integral_constant<int, G + 1>{});
           pending[B ^ 1] = true;
         }
       } else if constexpr (G > 0) {
-        if (tid == 0) issue_group(std::integral_constant<int, G>{});
+        if (tid < L::ISSUE_LANES) issue_group(std::integral_constant<int, G>{});
         pending[0] = true;
       }
     } else {
@@ -816,7 +853,9 @@ __global__ void __launch_bounds__(Layout<P, Phys, CB_>::NT, MINB)
         const R* src = ptr.in[Gi::arr_base() + A] + (size_t)c0 * NC * ND;
         for (int e = tid; e < ncb * NC * ND; e += NT) {
           if constexpr (L::BULK) {
-            cp_async_el(&s_in[fb * CB * ND + e], src + e);  // [cell][comp][node], as the bulk copy
+            // [cell][comp][node] in the slots of the bulk layout
+            constexpr int ab = [] { int b = 0; for (int a = 0; a < A; ++a) b += CB * L::slot(Gr::ncomp(a)); return b; }();
+            cp_async_el(&s_in[ab + (e / (NC * ND)) * L::slot(NC) + e % (NC * ND)], src + e);
           } else {
             const int cc = e / (NC * ND), r = e % (NC * ND);
             cp_async_el(&s_in[((fb + r / ND) * CB + cc) * L::NDP + r % ND], src + e);
