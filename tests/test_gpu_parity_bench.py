@@ -3,8 +3,9 @@
 * The explicit apply on the benchmark's 512x256 hill mesh (the 2D terrain-following
   operator microbenchmark: hydrostatic background plus the seeded 16x16-mode perturbation,
   seed 20261203), at degree 4 and at the odd degree 3: the fused stage-1 triple that
-  bench.py times and the three separate right-hand sides of every stage; at degree 5 (the
-  layout with padded per-cell bulk slots) the stage-1 launches.  1e-12 relative L2.
+  bench.py times and the three separate right-hand sides of every stage; at degrees 2, 5 (the
+  layout with padded per-cell bulk slots) and 6, the rest of the benchmark's degree sweep, the
+  stage-1 launches.  1e-12 relative L2.
 * The implicit operators on the same mesh at degree 4: the mass-type operators, B
   (vmult_pressure), C (vmult_enthalpy), the inverse diagonals, and the NS-stage-2 Schur apply
   D p - C A^{-1} B p with the nested CG to 1e-12 on both sides (1e-10).
@@ -66,7 +67,7 @@ def _stage_sources(states, stage):
     return src + [cur.rho, cur.u]
 
 
-@pytest.mark.parametrize("P", [4, 3, 5])
+@pytest.mark.parametrize("P", [4, 3, 5, 2, 6])
 def test_rhs_parity_on_the_bench_mesh(P):
     m, g, o, states = _bench_setup(P)
     ns = m.n_cells * (P + 1) ** 2
