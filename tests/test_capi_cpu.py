@@ -107,3 +107,47 @@ def test_imex_options_are_checked_on_the_host_and_no_device_fails_loudly():
     op = ctypes.c_void_p()
     assert L.af_create(ctypes.byref(desc), 4, 9, *args, ctypes.byref(op)) == O.AF_NO_DEVICE
     assert op.value is None
+
+
+def test_noalloc_schur_apply_checks_arguments_on_the_host():
+    """af_schur_apply_noalloc validates its arguments before it touches a device: null or
+    unaligned pointers, the stage, the degree and the static scratch limit (65536 pressure
+    DoFs) are rejected on the host; with valid arguments and no CUDA device it returns
+    AF_NO_DEVICE.  No pointer is dereferenced on these paths."""
+    from atmospheric_flows_b200 import operator as O
+    from atmospheric_flows_b200 import mesh as M
+    L = O.lib()
+    vp = ctypes.c_void_p
+    L.af_schur_apply_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, vp, vp, vp, vp, vp,
+                                         ctypes.POINTER(ctypes.c_int)]
+    L.af_schur_apply_noalloc.restype = ctypes.c_int
+    m = M.hill_mesh(4, 2)
+    buf = np.zeros(4096, dtype=np.float64)  # stands in for device memory: never read here
+    base = buf.ctypes.data + (-buf.ctypes.data) % 16
+    p = vp(base)
+    it = ctypes.c_int(-1)
+
+    def call(nx=4, nz=2, degree=4, stage=1, ptrs=None, mach=1.0, dt=1.0):
+        a = ptrs or [p] * 5
+        return L.af_schur_apply_noalloc(nx, nz, 0, a[0], degree, mach, dt, stage, a[1], a[2], a[3], a[4], None,
+                                        ctypes.byref(it))
+
+    assert call(ptrs=[p, p, None, p, p]) == O.AF_BAD_ARG
+    assert b"null pointer" in L.af_last_error_message()
+    assert call(stage=3) == O.AF_BAD_ARG
+    assert call(mach=0.0) == O.AF_BAD_ARG
+    assert call(degree=9) == O.AF_UNSUPPORTED
+    assert call(nx=64, nz=64) == O.AF_BAD_ARG  # 4096 cells x 25 = 102400 pressure DoFs
+    assert b"static scratch limit" in L.af_last_error_message()
+    assert call(ptrs=[p, p, p, vp(base + 8), p]) == O.AF_BAD_ARG
+    assert b"16-byte aligned" in L.af_last_error_message()
+    assert m.n_cells * 25 <= 65536
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return  # a CUDA device is present: the no-device path is not reachable
+    except ImportError:
+        pass
+    assert call() == O.AF_NO_DEVICE
+    assert it.value == -1
